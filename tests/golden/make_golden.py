@@ -1,0 +1,427 @@
+"""Generate the golden fixtures under tests/golden/ from the reference itself.
+
+Run in a container that holds the reference checkout (``python tests/golden/make_golden.py
+/path/to/reference``).  It imports the reference's own float64 array formulation
+(src/pysurf/sphSolver.py), its numba neighbour list (src/pysurf/sphCompiled.py), its boundaries
+(src/pysurf/sphBoundaries.py), its refinement (src/pysurf/sphRefinement.py) and its scenario
+builders, runs them on the inputs its own tests use (tests/testSphGpu.py:32-63 and the sloshing
+tank of tests/testSphGpu.py:441-457), and saves inputs and outputs as compressed .npz files.
+
+The reference's package __init__ pulls plotting and unit libraries that the sums do not need, so
+the package object, ``pysurf.constants`` (g = 9.80665, src/pysurf/constants.py:29-38) and
+``pysurf.figures`` are stubbed; every module used below is the reference's, unmodified.
+
+Nothing at test time imports the reference: the tests read these files only.
+"""
+from __future__ import annotations
+
+import math
+import os
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def loadReference(root: str):
+    package = types.ModuleType('pysurf')
+    package.__path__ = [os.path.join(root, 'src', 'pysurf')]
+    sys.modules['pysurf'] = package
+    constants = types.ModuleType('pysurf.constants')
+    constants.gravity = 9.80665
+    constants.freshwaterDensity = 998.2
+    constants.freshwaterKinematicViscosity = 1.0034e-6
+    constants.seawaterDensity = 1025.0
+    sys.modules['pysurf.constants'] = constants
+    package.constants = constants
+    figures = types.ModuleType('pysurf.figures')
+    sys.modules['pysurf.figures'] = figures
+    package.figures = figures
+
+
+rho0, c0, alpha, epsilon = 1000.0, 20.0, 0.1, 0.5
+
+
+def cloud(dimensions, periodic, seed=3, kernelType='cubicSpline'):
+    """The random cloud of tests/testSphGpu.py:32-63 (offset 25 m from the origin)."""
+    from pysurf.sphKernels import createKernel
+    from pysurf.sphNeighbors import neighborPairs
+    from pysurf.sphSolver import taitEquationOfState
+    rng = np.random.default_rng(seed)
+    count, spacing = (600, 0.04) if dimensions == 2 else (900, 0.045)
+    extent = np.full(dimensions, spacing * count ** (1.0 / dimensions))
+    positions = 25.0 + rng.uniform(0.0, 1.0, size=(count, dimensions)) * extent
+    period = None
+    if periodic:
+        positions[:, 1] -= 25.0
+        period = float(extent[1])
+    h = (2.0 if kernelType == 'wendlandC2' else 1.3) * spacing
+    velocities = rng.normal(0.0, 1.0, size=(count, dimensions))
+    densities = rho0 * (1.0 + rng.uniform(-0.01, 0.01, size=count))
+    masses = rho0 * spacing ** dimensions * (1.0 + rng.uniform(-0.05, 0.05, size=count))
+    isFluid = rng.uniform(size=count) < 0.8
+    pressures = taitEquationOfState(densities, rho0, c0)
+    i, j = neighborPairs(positions, 2.0 * h, period)
+    separation = positions[i] - positions[j]
+    if period is not None:
+        separation[:, 1] -= period * np.round(separation[:, 1] / period)
+    distance = np.linalg.norm(separation, axis=1)
+    kernel = createKernel(kernelType, dimensions)
+    return dict(kernelType=kernelType, positions=positions, period=period, h=h, velocities=velocities,
+                densities=densities, masses=masses, isFluid=isFluid, pressures=pressures, i=i, j=j,
+                separation=separation, distance=distance, values=kernel.evaluateBatch(distance, h),
+                gradients=kernel.gradientBatch(separation, distance, h), kernel=kernel)
+
+
+def strainedFlow(case):
+    """tests/testSphGpu.py:199-206: a linear flow under noise."""
+    positions = case['positions']
+    dimensions = positions.shape[1]
+    return (positions - positions.mean(axis=0)) @ np.random.default_rng(11).normal(
+        size=(dimensions, dimensions)).T + 0.3 * case['velocities']
+
+
+def makeClouds():
+    from pysurf import sphCompiled
+    from pysurf.sphSolver import (artificialViscosity, continuityRate, correctionMatrices, densityDiffusionRate,
+                                  extrapolatedWallPressure, limitedVelocityDifference, pairAccelerations,
+                                  renormalizedDensityGradient, shepardDensity, taitDensity, velocityGradients,
+                                  xsphVelocity)
+    out = {}
+    for dimensions, periodic in [(2, False), (3, False), (3, True)]:
+        for kernelType in ('cubicSpline', 'wendlandC2'):
+            tag = f'{dimensions}d_{"p" if periodic else "o"}_{kernelType}'
+            case = cloud(dimensions, periodic, kernelType=kernelType)
+            i, j, fluid = case['i'], case['j'], case['isFluid']
+            n = len(fluid)
+            gravity = np.zeros(dimensions)
+            gravity[-1] = -9.81
+            factor = 0.3
+            rec = dict(positions=case['positions'], velocities=case['velocities'], densities=case['densities'],
+                       masses=case['masses'], isFluid=fluid, pressures=case['pressures'], h=case['h'],
+                       period=case['period'] or 0.0, kernel=1 if kernelType == 'wendlandC2' else 0)
+            # Plain accelerations (tests/testSphGpu.py:79-99)
+            viscosity = artificialViscosity(case['velocities'][i] - case['velocities'][j], case['separation'],
+                                            case['distance'], 0.5 * (case['densities'][i] + case['densities'][j]),
+                                            case['h'], c0, alpha)
+            viscosity[~(fluid[i] & fluid[j])] *= factor
+            acc = pairAccelerations(case['masses'], case['densities'], case['pressures'], i, j, case['gradients'],
+                                    viscosity, n)
+            acc[fluid] += gravity
+            acc[~fluid] = 0.0
+            rec['accelerations'] = acc
+            # Limited accelerations and velocity gradients (tests/testSphGpu.py:101-133)
+            strained = strainedFlow(case)
+            G = velocityGradients(case['masses'], case['densities'], strained, i, j, case['separation'],
+                                  case['gradients'], fluid)
+            relative = strained[i] - strained[j]
+            rec_ = limitedVelocityDifference(relative, case['separation'], case['distance'], case['h'], G[i], G[j])
+            boundaryPairs = ~(fluid[i] & fluid[j])
+            rec_[boundaryPairs] = relative[boundaryPairs]
+            viscosity = artificialViscosity(relative, case['separation'], case['distance'],
+                                            0.5 * (case['densities'][i] + case['densities'][j]), case['h'], c0,
+                                            alpha, rec_)
+            viscosity[boundaryPairs] *= factor
+            accL = pairAccelerations(case['masses'], case['densities'], case['pressures'], i, j, case['gradients'],
+                                     viscosity, n)
+            accL[fluid] += gravity
+            accL[~fluid] = 0.0
+            rec['strained'] = strained
+            rec['velocityGradients'] = G
+            rec['limitedAccelerations'] = accL
+            # Continuity, plain and corrected (tests/testSphGpu.py:135-168)
+            rec['continuity'] = continuityRate(case['masses'], case['velocities'], i, j, case['gradients'], n,
+                                               fluid[i] | fluid[j])
+            L = correctionMatrices(case['masses'], case['densities'], i, j, case['separation'], case['gradients'],
+                                   fluid)
+            rec['corrections'] = L
+            rec['correctedContinuity'] = continuityRate(case['masses'], case['velocities'], i, j, case['gradients'],
+                                                        n, fluid[i] | fluid[j], L)
+            # Diffusive continuity (tests/testSphGpu.py:170-187)
+            plain = rec['continuity']
+            for mode in ('molteni', 'hydrostatic'):
+                gravityMagnitude = 9.81 if mode == 'hydrostatic' else None
+                rec[f'diffusive_{mode}'] = plain + densityDiffusionRate(
+                    case['masses'], case['densities'], i, j, case['separation'], case['distance'],
+                    case['gradients'], n, case['h'], c0, 0.1, rho0, gravityMagnitude, fluid[i] & fluid[j])
+            # Antuono (tests/testSphGpu.py:189-208)
+            gradients = renormalizedDensityGradient(case['masses'], case['densities'], i, j, case['gradients'], L,
+                                                    fluid)
+            rec['densityGradients'] = gradients
+            rec['diffusive_antuono'] = plain + densityDiffusionRate(
+                case['masses'], case['densities'], i, j, case['separation'], case['distance'], case['gradients'], n,
+                case['h'], c0, 0.1, rho0, None, fluid[i] & fluid[j], gradients)
+            # Wall pressure (tests/testSphGpu.py:306-318) and the boundary's density from it
+            wall = extrapolatedWallPressure(case['densities'], case['pressures'], i, j, case['separation'],
+                                            case['values'], fluid, gravity)
+            rec['wallPressure'] = wall
+            rec['wallDensity'] = np.where(fluid, case['densities'], taitDensity(wall, rho0, c0))
+            # XSPH and Shepard (tests/testSphGpu.py:368-388)
+            pairs = fluid[i] & fluid[j]
+            rec['xsph'] = xsphVelocity(case['velocities'], case['masses'], case['densities'], i[pairs], j[pairs],
+                                       case['values'][pairs], epsilon)
+            rec['shepard'] = shepardDensity(case['masses'], case['densities'], i, j, case['values'],
+                                            case['kernel'].evaluate(0.0, case['h']))
+            # The reference's compiled neighbour rows at the support (src/pysurf/sphCompiled.py:133-234)
+            offsets, neighbors = sphCompiled.neighborList(case['positions'], 2.0 * case['h'], case['period'] or 0.0)
+            rec['offsets'] = np.asarray(offsets, dtype=np.int64)
+            rec['neighbors'] = np.asarray(neighbors, dtype=np.int32)
+            # The cKDTree pair set (src/pysurf/sphNeighbors.py:28-78)
+            rec['pairCount'] = np.array(len(i))
+            for key, value in rec.items():
+                out[f'{tag}/{key}'] = np.asarray(value)
+    np.savez_compressed(os.path.join(HERE, 'clouds.npz'), **out)
+
+
+def makeCellKeys():
+    from pysurf.sphSolver import cellOrderKey
+    positions = np.array([[0.5, 0.5, 0.5], [1.5, 0.5, 0.5], [0.5, 1.5, 0.5], [0.5, 0.5, 1.5], [4.5, 0.5, 0.5],
+                          [-0.5, 0.5, 0.5]])
+    rng = np.random.default_rng(5)
+    random3 = rng.uniform(-3.0, 40.0, size=(2000, 3))
+    random2 = rng.uniform(-3.0, 60.0, size=(2000, 2))
+    np.savez_compressed(os.path.join(HERE, 'cellkeys.npz'),
+                        known3=positions, keys3=cellOrderKey(positions, 1.0, (4, 3, 2)),
+                        known2=positions[:3, :2], keys2=cellOrderKey(positions[:3, :2], 1.0, (4, 3, 1)),
+                        random3=random3, randomKeys3=cellOrderKey(random3, 0.37, (57, 23, 9)),
+                        random2=random2, randomKeys2=cellOrderKey(random2, 0.09375, (700, 40, 1)))
+
+
+def makeEnforcement():
+    """tests/testSphGpu.py:645-712: host enforcement of a reef bed (2D, 3D) and a ridge height field."""
+    from pysurf.bathymetry import Bathymetry, HeightField
+    from pysurf.sphBoundaries import BedBoundary, HeightFieldBoundary
+    from pysurf.sphParticles import ParticleSystem
+    out = {}
+    for dimensions in (2, 3):
+        rng = np.random.default_rng(7)
+        bed = Bathymetry.reefBreak(depth=1.0, toeX=2.0, faceSlope=0.2, reefDepth=0.3, reefLength=2.0)
+        s, width = 0.05, (0.6 if dimensions == 3 else None)
+        boundary = BedBoundary(bed, s, nLayers=3, wallTop=1.5, width=width,
+                               endWallTop=1.5 if dimensions == 2 else None)
+        count = 4000
+        fluid = np.column_stack([rng.uniform(bed.startX - 0.2, bed.endX + 0.2, count)]
+                                + ([rng.uniform(-0.1, 0.7, count)] if dimensions == 3 else [])
+                                + [rng.uniform(-1.2, 1.2, count)])
+        host = ParticleSystem.assemble(fluid, boundary.positions(), s, 1000.0, rng.normal(0.0, 1.0, (count, dimensions)))
+        boundary.attachPiston(host)
+        boundary.movePiston(host, bed.startX + 0.03, 0.4)
+        tag = f'bed{dimensions}d'
+        keep = host.isFluid.copy()
+        out[f'{tag}/positions'] = host.positions[keep].copy()
+        out[f'{tag}/velocities'] = host.velocities[keep].copy()
+        out[f'{tag}/bedX'] = bed.x.copy()
+        out[f'{tag}/bedZ'] = bed.z.copy()
+        clearance = 0.25 * boundary.spacing
+        sideWalls = boundary.width is not None and not boundary.periodic
+        endLimit = bed.endX - clearance if boundary.endWallTop is not None else bed.endX
+        mask = boundary._pistonMask
+        pistonSpeed = float(host.velocities[mask, 0][0])
+        out[f'{tag}/params'] = np.array([clearance, float(sideWalls), float(boundary.width or 0.0),
+                                         float(boundary.wallTop is not None), float(boundary.wallX), pistonSpeed,
+                                         float(endLimit)])
+        boundary.enforce(host)
+        out[f'{tag}/enforcedPositions'] = host.positions[keep].copy()
+        out[f'{tag}/enforcedVelocities'] = host.velocities[keep].copy()
+    rng = np.random.default_rng(11)
+    field = HeightField.ridge(0.5, endX=8.0, halfWidth=2.0, gridSpacing=1.0 / 16.0)
+    s = 0.125
+    boundary = HeightFieldBoundary(field, s, nLayers=3, wallTop=1.5)
+    count = 6000
+    fluid = np.column_stack([rng.uniform(-0.2, 8.2, count), rng.uniform(-0.2, 2.2, count), rng.uniform(-0.1, 1.2, count)])
+    host = ParticleSystem.assemble(fluid, boundary.positions(), s, 1000.0, rng.normal(0.0, 1.0, (count, 3)))
+    keep = host.isFluid.copy()
+    out['field/positions'] = host.positions[keep].copy()
+    out['field/velocities'] = host.velocities[keep].copy()
+    out['field/table'] = field.z.copy()
+    clearance = 0.25 * s
+    startX, endX, startY, endY = field.bounds
+    out['field/params'] = np.array([float(field.x[0]), float(field.y[0]), field.spacingX, field.spacingY, clearance,
+                                    startY + clearance, endY - clearance, float(boundary.offshoreWall),
+                                    startX + clearance, endX - clearance if boundary.endWall else endX])
+    boundary.enforce(host)
+    out['field/enforcedPositions'] = host.positions[keep].copy()
+    out['field/enforcedVelocities'] = host.velocities[keep].copy()
+    np.savez_compressed(os.path.join(HERE, 'enforce.npz'), **out)
+
+
+def sloshing(backend='numpy', tilt=10.0, **options):
+    """tests/testSphGpu.py:441-457: a 0.2 x 0.15 m tank half full at 5 mm spacing."""
+    from pysurf.sphSolver import WcsphSolver
+    from pysurf.WaterSim.scenarios.sloshingTank import SloshingTankConfig, createSloshingTank
+    tank = SloshingTankConfig(tankWidth=0.2, tankHeight=0.15, fillRatio=0.5, initialTiltDeg=tilt,
+                              particleSpacing=0.005)
+    config, particles, boundary = createSloshingTank(tank)
+    config.backend = backend
+    config.maxTimeStep = 1e-3
+    for name, value in options.items():
+        setattr(config, name, value)
+    solver = WcsphSolver(config, boundary=boundary)
+    solver.initialize(particles)
+    return solver, particles, boundary
+
+
+deltaContinuity = dict(densityFilterInterval=0, xsphEpsilon=0.0, wallPressure='extrapolated',
+                       continuityCorrection=True, densityFloor=0.9)
+
+
+def recordRun(out, tag, solver, particles, steps, boundaryRecord):
+    config = solver.config
+    out[f'{tag}/positions'] = particles.positions.copy()
+    out[f'{tag}/velocities'] = particles.velocities.copy()
+    out[f'{tag}/densities'] = particles.densities.copy()
+    out[f'{tag}/masses'] = particles.masses.copy()
+    out[f'{tag}/isFluid'] = particles.isFluid.copy()
+    modes = {'none': 0, 'molteni': 1, 'hydrostatic': 2, 'antuono': 3}
+    out[f'{tag}/config'] = np.array([
+        config.dimensions, 1.0 if config.kernelType == 'wendlandC2' else 0.0, config.smoothingLength,
+        config.referenceDensity, solver.speedOfSound, config.alphaViscosity, config.boundaryViscosityFactor,
+        config.xsphEpsilon, config.densityFloor * config.referenceDensity, modes[config.densityDiffusion],
+        config.diffusionDelta, float(config.wallPressure == 'extrapolated'), float(config.negativePressure),
+        float(config.continuityCorrection), float(config.viscosityLimiter), config.cflNumber, config.maxTimeStep,
+        float(config.densityFilterInterval), float(config.periodicWidth or 0.0)])
+    out[f'{tag}/gravity'] = np.asarray(config.gravity, dtype=float)
+    out[f'{tag}/domain'] = np.array([list(config.domainMin), list(config.domainMax)], dtype=float)
+    for key, value in boundaryRecord.items():
+        out[f'{tag}/boundary_{key}'] = np.asarray(value)
+    dts = []
+    for _ in range(steps):
+        state = solver.step()
+        dts.append(state.dt)
+    out[f'{tag}/steps'] = np.array(steps)
+    out[f'{tag}/dts'] = np.array(dts)
+    out[f'{tag}/finalPositions'] = particles.positions.copy()
+    out[f'{tag}/finalVelocities'] = particles.velocities.copy()
+    out[f'{tag}/finalDensities'] = particles.densities.copy()
+    out[f'{tag}/finalPressures'] = particles.pressures.copy()
+    out[f'{tag}/finalAccelerations'] = particles.accelerations.copy()
+
+
+def containerRecord(boundary):
+    return dict(kind=1, lower=boundary.containerMin, upper=boundary.containerMax, openTop=int(boundary.openTop))
+
+
+def makeRuns():
+    """Host steps of the reference's float64 numpy solver, the runs its GPU tests compare against."""
+    out = {}
+    runs = {
+        'plain': dict(),                                                  # Shepard filter and XSPH
+        'limited': dict(viscosityLimiter=True),
+        'deltaHydrostatic': dict(densityDiffusion='hydrostatic', **deltaContinuity),
+        'deltaAntuono': dict(deltaContinuity, continuityCorrection=False, densityDiffusion='antuono'),
+        'tension': dict(negativePressure=True),
+        'deltaWendland': dict(kernelType='wendlandC2', smoothingLengthRatio=2.0, densityDiffusion='hydrostatic',
+                              viscosityLimiter=True, **deltaContinuity),
+    }
+    for tag, options in runs.items():
+        solver, particles, boundary = sloshing(**options)
+        if tag == 'tension':
+            particles.densities[particles.isFluid] *= 0.998
+        steps = 30 if tag != 'plain' else 40
+        recordRun(out, tag, solver, particles, steps, containerRecord(boundary))
+    # A solitary wave over a flat channel bed, the deltaSph scheme at h = 3 dx (tests/testSphGpu.py:714-750)
+    from pysurf import constants, waveTheory
+    from pysurf.bathymetry import Bathymetry
+    from pysurf.sphBoundaries import BedBoundary
+    from pysurf.sphParticles import ParticleSystem
+    from pysurf.sphSolver import SimulationConfig, WcsphSolver
+    from pysurf.waveMakers import solitaryWaveFluid
+    depth, height, spacing = 1.0, 0.3, 1.0 / 8.0
+    crestX = waveTheory.solitaryWaveHalfLength(height, depth, 0.01)
+    channel = Bathymetry([0.0, 12.0], [0.0, 0.0], stillWaterLevel=depth)
+    boundary = BedBoundary(channel, spacing, nLayers=6, wallTop=1.9, endWallTop=1.9)
+    fluid, velocities = solitaryWaveFluid(channel, height, crestX, spacing)
+    particles = ParticleSystem.assemble(fluid, boundary.positions(), spacing, constants.freshwaterDensity, velocities)
+    config = SimulationConfig(domainMin=np.array([-0.5, -0.5]), domainMax=np.array([12.5, 1.9]),
+                              particleSpacing=spacing, maxTimeStep=1.0, smoothingLengthRatio=3.0,
+                              kernelType='wendlandC2', densityDiffusion='hydrostatic', viscosityLimiter=True,
+                              speedOfSound=10.0 * waveTheory.solitaryWaveSpeed(height, depth), alphaViscosity=0.01,
+                              backend='numpy', initialSurface=lambda x: depth + waveTheory.solitaryWaveProfile(
+                                  x, height, depth, crestX), **deltaContinuity)
+    solver = WcsphSolver(config, boundary=boundary)
+    solver.initialize(particles)
+    clearance = 0.25 * spacing
+    bedRecord = dict(kind=2, bedX=channel.x, bedZ=channel.z,
+                     params=[clearance, 0.0, 0.0, 1.0, float(boundary.wallX), 0.0, channel.endX - clearance])
+    recordRun(out, 'bedDelta', solver, particles, 40, bedRecord)
+    np.savez_compressed(os.path.join(HERE, 'runs.npz'), **out)
+
+
+def makeSplit():
+    """src/pysurf/sphRefinement.py:136-190 on a small 2D and 3D set, h kept and h halved."""
+    from pysurf.sphParticles import ParticleSystem
+    from pysurf.sphRefinement import splitParticles
+    out = {}
+    for dimensions in (2, 3):
+        for ratio in (1.0, 0.5):
+            rng = np.random.default_rng(21 + dimensions)
+            s = 0.05
+            fluid = 3.0 + rng.uniform(0.0, 1.0, (300, dimensions))
+            wall = rng.uniform(0.0, 1.0, (60, dimensions))
+            particles = ParticleSystem.assemble(fluid, wall, s, 1000.0, rng.normal(0.0, 1.0, (300, dimensions)))
+            particles.densities = 1000.0 + rng.uniform(-5, 5, len(particles.densities))
+            particles.pressures = rng.uniform(0, 10, len(particles.densities))
+            mask = rng.uniform(size=len(particles.densities)) < 0.3
+            tag = f'split{dimensions}d_{ratio}'
+            for name in ('positions', 'velocities', 'accelerations', 'densities', 'pressures', 'masses', 'isFluid'):
+                out[f'{tag}/{name}'] = getattr(particles, name).copy()
+            out[f'{tag}/mask'] = mask
+            count = splitParticles(particles, mask, 1000.0, 1.3 * s, ratio)
+            out[f'{tag}/count'] = np.array(count)
+            for name in ('positions', 'velocities', 'accelerations', 'densities', 'pressures', 'masses', 'isFluid',
+                         'lengths'):
+                out[f'{tag}/split_{name}'] = getattr(particles, name).copy()
+    np.savez_compressed(os.path.join(HERE, 'split.npz'), **out)
+
+
+def makeBeach():
+    """The solitary-wave-on-a-plane-beach start at 8 particles per depth, as the reference builds it."""
+    from pysurf import constants, waveTheory
+    from pysurf.bathymetry import Bathymetry
+    from pysurf.sphBoundaries import BedBoundary, ContainerBoundary
+    from pysurf.sphParticles import ParticleSystem, latticePoints
+    from pysurf.sphSolver import hydrostaticDensity
+    from pysurf.waveMakers import solitaryWaveFluid
+    out = {}
+    depth, height, ppd = 1.0, 0.45, 8
+    s = depth / ppd
+    beach = Bathymetry.planeBeach(depth=depth, toeX=15.0, slope=1.0 / 15.0, endX=60.0)
+    layers = 6
+    boundary = BedBoundary(beach, s, nLayers=layers, wallTop=depth + 3.0 * height, endWallTop=None)
+    fluid, velocities = solitaryWaveFluid(beach, height, 10.0, s)
+    particles = ParticleSystem.assemble(fluid, boundary.positions(), s, constants.freshwaterDensity, velocities)
+    c0 = 10.0 * waveTheory.solitaryWaveSpeed(height, depth)
+    surface = depth + waveTheory.solitaryWaveProfile(particles.positions[:, 0], height, depth, 10.0)
+    densities = hydrostaticDensity(surface - particles.positions[:, -1], constants.freshwaterDensity, c0)
+    out['beach/positions'] = particles.positions
+    out['beach/velocities'] = particles.velocities
+    out['beach/isFluid'] = particles.isFluid
+    out['beach/masses'] = particles.masses
+    out['beach/densities'] = densities
+    # The dam break's tank: a 1 x 2 m column in a 4 x 3 m container, 3 layers, at 0.1 m
+    tank = ContainerBoundary(np.zeros(2), np.array([4.0, 3.0]), 0.1, nLayers=3, openTop=True)
+    out['dam/boundary'] = tank.positions()
+    out['dam/column'] = latticePoints([0.0, 0.0], [1.0, 2.0], 0.1)
+    np.savez_compressed(os.path.join(HERE, 'beach.npz'), **out)
+
+
+def main():
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('PYSURF_REFERENCE', '')
+    if not root or not os.path.isdir(root):
+        raise SystemExit('Give the reference checkout: make_golden.py /path/to/reference')
+    loadReference(root)
+    makeCellKeys()
+    makeClouds()
+    makeEnforcement()
+    makeSplit()
+    makeBeach()
+    makeRuns()
+    for name in sorted(os.listdir(HERE)):
+        if name.endswith('.npz'):
+            print(name, os.path.getsize(os.path.join(HERE, name)))
+
+
+if __name__ == '__main__':
+    main()
