@@ -1,0 +1,315 @@
+"""Benchmark: fluid particle-updates/s of the deltaSph step on the 2D solitary wave over a 1:15 beach.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--ppd 64]
+
+Workload: the first-order solitary wave of H/d = 0.45 at x0 = 10 d over a 1:15 beach from
+x = 15 d, 60 d long, 64 particles per depth (pysurf_b200.cases.solitaryBeach), stepped by the
+deltaSph scheme (Wendland C2 at h = 3 dx, hydrostatic delta-SPH diffusion, the continuity
+correction, extrapolated walls, the viscosity limiter, density floor 0.9 rho0).  A step is one
+full device-resident step: cell list, wall pressure, gradients, momentum, time step, kick,
+continuity, density update, drift and bed enforcement.
+
+value      fluid particles x steps / device time of exactly K steps (CUDA events on the stream the
+           kernels run on, an L2 flush of 256 MiB between steps outside the timed spans), max over
+           ranks; with N GPUs each rank runs its own replica of the case (independent cases need
+           no collective), so the value is the sum over replicas ("scaling": "weak").
+e2e        the same metric through the public API with host buffers: each step pushes the whole
+           state from pinned host memory, steps once and pulls the state back.
+roofline   the dominant kernel (momentum) against the measured HBM copy bandwidth, with the
+           step's algorithmic bytes per fluid particle-update (53 B in 2D) per launch.
+--impl reference   the float64 C restatement of the reference's step (oracle/, OpenMP over every
+           host core) on the same workload, timed per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import re
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+ALGORITHMIC_BYTES_2D = 53       # per fluid particle-update: x 8+4, v 8, rho 4, m 4, kind 1 read; x, v, rho written
+METRIC = 'particle-updates/s'
+
+
+def parseArgs():
+    p = argparse.ArgumentParser()
+    p.add_argument('--gpus', type=int, default=1)
+    p.add_argument('--steps', type=int, default=40)
+    p.add_argument('--warmup', type=int, default=5)
+    p.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    p.add_argument('--ppd', type=int, default=64)
+    p.add_argument('--cells', type=int, default=None, help='cells per kernel support in the device cell list')
+    p.add_argument('--no-e2e', action='store_true')
+    p.add_argument('--no-cpu', action='store_true')
+    return p.parse_args()
+
+
+def config(case, flush: bool = True) -> dict:
+    info = dict(case.info)
+    return {'workload': 'solitary wave H/d 0.45 on a 1:15 plane beach, 2D, deltaSph scheme (Wendland C2 h=3dx, '
+                        'hydrostatic delta-SPH 0.1, continuity correction, extrapolated walls, viscosity limiter)',
+            'particles_per_depth': info['ppd'], 'fluid_particles': case.fluidCount,
+            'boundary_particles': int(case.state.nParticles - case.fluidCount), 'bed_layers': info['layers'],
+            'smoothing_length_over_dx': round(case.smoothingLength / case.spacing, 6), 'domain_length_d': info['length'],
+            'l2': 'flushed (256 MiB write) between timed steps' if flush else 'resident'}
+
+
+def clockSampler(device: int):
+    """nvidia-smi clocks and throttle reasons every 200 ms while the timed region runs."""
+    samples, stop = [], threading.Event()
+
+    def run():
+        query = ('clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,'
+                 'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
+                 'clocks_event_reasons.sw_power_cap')
+        while not stop.is_set():
+            try:
+                out = subprocess.run(['nvidia-smi', '-i', str(device), f'--query-gpu={query}',
+                                      '--format=csv,noheader,nounits'], capture_output=True, text=True, timeout=5)
+                fields = [f.strip() for f in out.stdout.strip().split(',')]
+                if len(fields) == 7:
+                    samples.append(fields)
+            except Exception:
+                pass
+            stop.wait(0.2)
+
+    thread = threading.Thread(target=run, daemon=True)
+    thread.start()
+
+    def finish():
+        stop.set()
+        thread.join(timeout=10)
+        if not samples:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['unsampled']}
+        sm = sorted(float(s[0]) for s in samples if s[0].replace('.', '').isdigit())
+        reasons = set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for s in samples:
+            for name, value in zip(names, s[3:]):
+                if value.lower().startswith('active'):
+                    reasons.add(name)
+        return {'sm_mhz': sm[len(sm) // 2] if sm else None, 'sm_max_mhz': float(samples[0][1]),
+                'reasons': sorted(reasons), 'samples': len(samples)}
+
+    return finish
+
+
+def measuredPeaks() -> dict:
+    path = os.path.join(ROOT, 'MEASURED_PEAKS.json')
+    if os.path.exists(path):
+        with open(path) as f:
+            data = json.load(f)
+        return {'hbm_gbs': float(data['hbm_gbs']), 'source': 'measured'}
+    return {'hbm_gbs': 6650.0, 'source': 'fallback'}
+
+
+def profiledTraffic() -> float | None:
+    """dram bytes per momentum launch from the committed ncu summary, if one is there."""
+    path = os.path.join(ROOT, 'profiles', 'momentum_solitaryBeach64.md')
+    if not os.path.exists(path):
+        return None
+    match = re.search(r'traffic_bytes_per_launch:\s*([0-9.eE+]+)', open(path).read())
+    return float(match.group(1)) if match else None
+
+
+def cpuBaseline(case, seconds: float = 12.0) -> dict:
+    """The float64 oracle's step on the same workload, on every host core, for about `seconds`."""
+    import numpy as np
+    from oracle import oracle
+    bed = case.boundary.bathymetry
+    stepper = oracle.Stepper(2, case.kernelType, case.smoothingLength, case.referenceDensity, case.soundSpeed,
+                             case.alpha, case.gravity, 0.0, 0.0, case.densityFloor, case.densityDiffusion,
+                             case.diffusionDelta, True, False, True, True, case.cflNumber, case.maxTimeStep, 0.0, 0,
+                             ('bed', oracle.bedParams(bed.x, bed.z, 0.25 * case.spacing, False, 0.0, True, bed.startX,
+                                                      0.0, bed.endX)))
+    state = {k: np.array(getattr(case.state, k), copy=True) for k in ('positions', 'velocities', 'densities',
+                                                                       'masses', 'isFluid')}
+    stepper(state)                          # warm-up: page in, first neighbour list
+    steps, start = 0, time.perf_counter()
+    while True:
+        stepper(state)
+        steps += 1
+        elapsed = time.perf_counter() - start
+        if elapsed > seconds or steps >= 200:
+            break
+    cores = os.cpu_count()
+    return {'value': case.fluidCount * steps / elapsed, 'unit': METRIC, 'cores': cores, 'kind': 'port',
+            'sample': f'{steps} full steps of the same case ({case.state.nParticles} particles) in float64, '
+                      f'OpenMP over {cores} threads, {elapsed:.1f} s'}
+
+
+def referenceArm(args) -> None:
+    """The reference's algorithm on the host cores: the float64 C restatement (oracle/), timed per step."""
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return
+    from pysurf_b200 import cases
+    case = cases.solitaryBeach(args.ppd)
+    import numpy as np
+    from oracle import oracle
+    bed = case.boundary.bathymetry
+    stepper = oracle.Stepper(2, case.kernelType, case.smoothingLength, case.referenceDensity, case.soundSpeed,
+                             case.alpha, case.gravity, 0.0, 0.0, case.densityFloor, case.densityDiffusion,
+                             case.diffusionDelta, True, False, True, True, case.cflNumber, case.maxTimeStep, 0.0, 0,
+                             ('bed', oracle.bedParams(bed.x, bed.z, 0.25 * case.spacing, False, 0.0, True, bed.startX,
+                                                      0.0, bed.endX)))
+    state = {k: np.array(getattr(case.state, k), copy=True) for k in ('positions', 'velocities', 'densities',
+                                                                       'masses', 'isFluid')}
+    for _ in range(args.warmup):
+        stepper(state)
+    start = time.perf_counter()
+    for _ in range(args.steps):
+        stepper(state)
+    elapsed = time.perf_counter() - start
+    value = case.fluidCount * args.steps / elapsed
+    cores = os.cpu_count()
+    line = {'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': METRIC, 'n_gpus': args.gpus,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 * elapsed / args.steps,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+            'config': config(case, flush=False),
+            'cpu_baseline': {'value': value, 'unit': METRIC, 'cores': cores, 'kind': 'port',
+                             'sample': f'{args.steps} full steps of the whole case in float64 on {cores} threads'},
+            'e2e': {'value': value, 'unit': METRIC, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    args = parseArgs()
+    if args.impl == 'reference':
+        referenceArm(args)
+        return
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+
+    from pysurf_b200 import cases
+    from pysurf_b200._lib import C
+
+    rank = int(os.environ.get('RANK', '0'))
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group('nccl', timeout=timedelta(seconds=300), device_id=torch.device('cuda', local))
+
+    case = cases.solitaryBeach(args.ppd)
+    sums = cases.pairSumsFor(case, args.cells, device=local)
+    stream = torch.cuda.Stream()
+    sums.setStream(stream.cuda_stream)
+    state = case.state.copy()
+    sums.push(state)
+    sums.setBoundary(case.boundary, state)
+    h, cfl, maxdt = case.smoothingLength, case.cflNumber, case.maxTimeStep
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device='cuda')     # 256 MiB, twice the L2
+
+    # warm-up steps (untimed), then exactly K timed steps
+    sums.beginSteps(0.0, 0, math.inf, 1 << 62, h, cfl, maxdt)
+    sums.enqueueSteps(args.warmup)
+    t, s, dt = sums.finishSteps()
+    sums.beginSteps(t, s, math.inf, 1 << 62, h, cfl, maxdt, lastTimeStep=dt)
+    launchesPerStep = sums.stepLaunches()
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    stageMs = []
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = clockSampler(local)
+    for k in range(args.steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            starts[k].record(stream)
+            sums.enqueueSteps(1)
+            stops[k].record(stream)
+        stream.synchronize()
+        stageMs.append(sums.stageTimes())
+    torch.cuda.synchronize()
+    clocks = sampler()
+    t, s, dt = sums.finishSteps()
+    stepMs = [a.elapsed_time(b) for a, b in zip(starts, stops)]
+    totalMs = float(sum(stepMs))
+    if world > 1:
+        worst = torch.tensor([totalMs], device='cuda', dtype=torch.float64)
+        dist.all_reduce(worst, op=dist.ReduceOp.MAX)
+        totalMs = float(worst.item())
+        dist.barrier()
+    value = world * case.fluidCount * args.steps / (totalMs / 1e3)
+
+    names = sums.stageNames()
+    stages = {name: float(np.mean([m[i] for m in stageMs])) for i, name in enumerate(names)}
+    dominant = max(stages, key=stages.get)
+    peaks = measuredPeaks()
+    kernelMs = stages[dominant]
+    achieved = ALGORITHMIC_BYTES_2D * case.fluidCount / (kernelMs / 1e3) / 1e9
+    roofline = {'bound': 'hbm', 'kernel': dominant, 'achieved': achieved, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
+                'frac': achieved / peaks['hbm_gbs'], 'traffic': profiledTraffic(), 'peak_source': peaks['source'],
+                'kernel_ms': kernelMs, 'step_hbm_frac': ALGORITHMIC_BYTES_2D * case.fluidCount /
+                (totalMs / args.steps / 1e3) / 1e9 / peaks['hbm_gbs']}
+
+    # end to end through the public API with host buffers: push, one step, pull, every step
+    e2e = None
+    if not args.no_e2e:
+        n, dim = case.state.nParticles, 2
+        pinned = {name: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
+                  for name, shape in (('positions', (n, dim)), ('velocities', (n, dim)), ('densities', (n,)),
+                                      ('masses', (n,)), ('pressures', (n,)), ('accelerations', (n, dim)))}
+        sums.pull(state)
+        host = type(state)(pinned['positions'], pinned['velocities'], pinned['accelerations'], pinned['densities'],
+                           pinned['pressures'], pinned['masses'], torch.empty(n, dtype=torch.bool, pin_memory=True).numpy())
+        for name in ('positions', 'velocities', 'densities', 'masses', 'pressures', 'accelerations'):
+            getattr(host, name)[:] = getattr(state, name)
+        host.isFluid[:] = state.isFluid
+        bytesIn = n * (dim * 8 * 2 + 8 + 8 + 1)
+        bytesOut = n * (dim * 8 * 2 + 8 + 8 + dim * 8)
+        e2eSteps = max(5, min(args.steps, 20))
+        torch.cuda.synchronize()
+        begin = torch.cuda.Event(enable_timing=True)
+        end = torch.cuda.Event(enable_timing=True)
+        clockT, clockS, clockDt = t, s, dt
+        wall = time.perf_counter()
+        begin.record(stream)
+        for k in range(e2eSteps):
+            sums.push(host)
+            clockT, clockS, clockDt = sums.advance(clockT, clockS, math.inf, clockS + 1, h, cfl, maxdt, 0, clockDt)
+            sums.pull(host)
+        end.record(stream)
+        end.synchronize()
+        e2eMs = max(begin.elapsed_time(end), 0.0)
+        wallMs = (time.perf_counter() - wall) * 1e3
+        e2eMs = max(e2eMs, wallMs)
+        if world > 1:
+            worst = torch.tensor([e2eMs], device='cuda', dtype=torch.float64)
+            dist.all_reduce(worst, op=dist.ReduceOp.MAX)
+            e2eMs = float(worst.item())
+        e2e = {'value': world * case.fluidCount * e2eSteps / (e2eMs / 1e3), 'unit': METRIC,
+               'h2d_bytes_per_step': bytesIn, 'd2h_bytes_per_step': bytesOut, 'steps': e2eSteps,
+               'ms_per_step': e2eMs / e2eSteps}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpuBaseline(case)
+
+    if rank == 0:
+        line = {'metric': METRIC, 'value': value, 'unit': METRIC, 'n_gpus': world, 'steps': args.steps,
+                'warmup': args.warmup, 'ms_per_step': totalMs / args.steps, 'higher_is_better': True,
+                'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32 sums, f64 state', 'data': 'synthetic',
+                'config': dict(config(case), parallelism=f'replicas{world}' if world > 1 else 'single'),
+                'clocks': clocks, 'e2e': e2e, 'gpu_launches': launchesPerStep * args.steps,
+                'roofline': roofline, 'stages_ms': stages, 'cpu_baseline': cpu,
+                'simulated_time_s': t}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    main()

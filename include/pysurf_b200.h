@@ -1,0 +1,183 @@
+/*
+ * pysurf_b200.h -- C-ABI of the B200 delta-SPH backend (libpysurf_b200.so).
+ *
+ * The drop-in boundary is the solver-backend interface pySurf's WcsphSolver drives,
+ * `pysurf.sphGpu.PairSums` (src/pysurf/sphGpu.py:1482-2323).  Each entry point below replaces one
+ * method of it; the citation on each names the method.  A Python `PairSums` over this ABI lives in
+ * pysurf_b200/sphGpu.py; a ctypes or cffi binding needs nothing but these declarations.
+ *
+ * Conventions
+ *   - Plain pointers and sizes only.  Unless a name ends in _device, array arguments are HOST
+ *     memory, row-major float64 as numpy lays them out: vectors (n, dim), matrices (n, dim, dim),
+ *     scalars (n,); fluid flags one byte per particle.  The library copies inputs in and results
+ *     out through its own pinned staging; the caller keeps ownership of every array it passes.
+ *   - Every call returns 0 (SPH_OK) or a negative status; sph_last_error() describes the last
+ *     failure on the calling thread.
+ *   - A handle is one particle system on one device; calls on one handle must not overlap.
+ *     Work is ordered on the handle's stream (sph_set_stream; the device's default stream
+ *     otherwise).  Calls that return host results synchronize that stream.
+ *   - The library allocates its own device memory (float64 master state, float32 sweep frame,
+ *     sort scratch), about 300 bytes a particle in 2D, and frees it in sph_destroy.
+ */
+#ifndef PYSURF_B200_H
+#define PYSURF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SPH_OK 0
+#define SPH_ERR_INVALID (-1)     /* an argument is out of range; no state changed */
+#define SPH_ERR_NOMEM (-2)       /* device or pinned host memory ran out */
+#define SPH_ERR_CUDA (-3)        /* a CUDA call failed */
+#define SPH_ERR_NONFINITE (-4)   /* the state stopped being finite during a step */
+#define SPH_ERR_TIMESTEP (-5)    /* the time step collapsed (not positive and finite) */
+#define SPH_ERR_STATE (-6)       /* the call needs state the handle does not hold yet */
+#define SPH_ERR_CAPACITY (-7)    /* an output array is too small; the needed size is returned */
+#define SPH_ERR_UNSUPPORTED (-8) /* an option the backend does not carry */
+
+typedef struct SphSystem SphSystem;
+
+/* Construction: PairSums.__init__ (src/pysurf/sphGpu.py:1524-1569).
+ * kernel_type 0 cubic spline, 1 Wendland C2; period > 0 makes y periodic (3D only);
+ * precise 1 takes separations from the float64 positions' point and remainder, 0 from the
+ * float32 points alone (separationPrecision). */
+int sph_create(int dimensions, double smoothing_length, const double *domain_min, const double *domain_max,
+               double period, int precise, int kernel_type, int device, SphSystem **out);
+int sph_destroy(SphSystem *sys);
+const char *sph_last_error(void);
+int sph_version(void);
+
+/* The hash grid's shape the reference's sortParticles reads (PairSums.gridShape,
+ * src/pysurf/sphGpu.py:1466-1478 gridDimensions). */
+int sph_grid_shape(const SphSystem *sys, int64_t shape[3]);
+/* Cells per support of the internal cell list (1: cells 2h wide, 2: cells h wide). */
+int sph_set_cells_per_support(SphSystem *sys, int cells);
+/* The CUDA stream (a cudaStream_t) the handle's work goes on; NULL for the default stream. */
+int sph_set_stream(SphSystem *sys, void *stream);
+
+/* Setters: PairSums.setDiffusion (src/pysurf/sphGpu.py:1882), setWallPressure (1910),
+ * setNegativePressure (1921), setContinuityCorrection (1701), setViscosityLimiter (1744).
+ * mode 0 none, 1 molteni, 2 hydrostatic, 3 antuono. */
+int sph_set_diffusion(SphSystem *sys, int mode, double delta, double sound_speed, double reference_density,
+                      double gravity);
+int sph_set_wall_pressure(SphSystem *sys, int extrapolated);
+int sph_set_negative_pressure(SphSystem *sys, int enabled);
+int sph_set_continuity_correction(SphSystem *sys, int enabled);
+int sph_set_viscosity_limiter(SphSystem *sys, int enabled);
+/* PairSums.setPhysics (src/pysurf/sphGpu.py:2173-2205); density_floor in kg/m^3, 0 for none. */
+int sph_set_physics(SphSystem *sys, double reference_density, double sound_speed, double alpha,
+                    double boundary_viscosity_factor, const double *gravity, double xsph_epsilon,
+                    double density_floor);
+
+/* ---- Host steps (the state stays with the caller) ---------------------------------------- */
+
+/* PairSums.update (src/pysurf/sphGpu.py:1998-2042): positions, masses, flags and lengths
+ * (lengths may be NULL for the handle's h throughout); rebuilds the cell list.  Fails with
+ * SPH_ERR_INVALID when a length exceeds the handle's h. */
+int sph_update(SphSystem *sys, int64_t n, const double *positions, const double *masses, const uint8_t *is_fluid,
+               const double *lengths);
+/* PairSums.pairAccelerations (src/pysurf/sphGpu.py:2044-2059) -> out (n, dim). */
+int sph_pair_accelerations(SphSystem *sys, const double *velocities, const double *densities,
+                           const double *pressures, double sound_speed, double alpha, double boundary_factor,
+                           const double *gravity, double *out);
+/* PairSums.continuityRate (src/pysurf/sphGpu.py:2061-2078) -> out (n,); densities may be NULL
+ * only without diffusion and correction. */
+int sph_continuity_rate(SphSystem *sys, const double *velocities, const double *densities, double *out);
+/* PairSums.xsphVelocity (src/pysurf/sphGpu.py:2080-2088) -> out (n, dim). */
+int sph_xsph_velocity(SphSystem *sys, const double *velocities, const double *densities, double epsilon,
+                      double *out);
+/* PairSums.wallPressure (src/pysurf/sphGpu.py:2090-2102) -> out (n,), the boundary's replaced. */
+int sph_wall_pressure(SphSystem *sys, const double *densities, const double *pressures, const double *gravity,
+                      double reference_density, double sound_speed, double *out);
+/* PairSums.shepardDensity (src/pysurf/sphGpu.py:2104-2113) -> out (n,). */
+int sph_shepard_density(SphSystem *sys, const double *densities, double *out);
+/* PairSums.velocityGradients (src/pysurf/sphGpu.py:1827), correctionMatrices (1855),
+ * densityGradients (1868) -> (n, dim, dim), (n, dim, dim), (n, dim). */
+int sph_velocity_gradients(SphSystem *sys, const double *velocities, const double *densities, double *out);
+int sph_correction_matrices(SphSystem *sys, const double *densities, double *out);
+int sph_density_gradients(SphSystem *sys, const double *densities, double *out);
+
+/* ---- Device-resident steps (the state lives on the device between push and pull) --------- */
+
+/* PairSums.push (src/pysurf/sphGpu.py:2207-2221): the whole state, caller order. */
+int sph_push(SphSystem *sys, int64_t n, const double *positions, const double *velocities, const double *densities,
+             const double *masses, const uint8_t *is_fluid, const double *lengths);
+/* PairSums.pull (src/pysurf/sphGpu.py:2223-2235): any output may be NULL.  masses, lengths and
+ * is_fluid come back too, since a device split changes them. */
+int sph_pull(SphSystem *sys, double *positions, double *velocities, double *densities, double *pressures,
+             double *accelerations, double *masses, double *lengths, uint8_t *is_fluid);
+int sph_count(const SphSystem *sys, int64_t *n);
+
+/* PairSums.setBoundary (src/pysurf/sphGpu.py:2121-2171), one call per kind. */
+int sph_clear_boundary(SphSystem *sys);
+int sph_set_boundary_container(SphSystem *sys, const double *lower, const double *upper, int open_top);
+/* bed: the profile's vertices; clearance = spacing / 4; side walls in 3D at y = clearance and
+ * width - clearance; the offshore wall at wall_x with the piston's speed; end_limit the
+ * shoreward limit. */
+int sph_set_boundary_bed(SphSystem *sys, const double *bed_x, const double *bed_z, int64_t count, double clearance,
+                         int side_walls, double width, int offshore_wall, double wall_x, double piston_speed,
+                         double end_limit);
+/* height field: table (ny, nx) row-major, grid origin and steps, walls as HeightFieldBoundary. */
+int sph_set_boundary_height_field(SphSystem *sys, const double *table, int64_t nx, int64_t ny, double origin_x,
+                                  double origin_y, double step_x, double step_y, double clearance, double low_y,
+                                  double high_y, int offshore_wall, double low_x, double high_x);
+/* PairSums.enforceBoundary (src/pysurf/sphGpu.py:2317-2323). */
+int sph_enforce_boundary(SphSystem *sys);
+
+/* PairSums.residentRates (src/pysurf/sphGpu.py:2237-2273): the first half of a device step;
+ * returns the largest fluid speed and acceleration. */
+int sph_resident_rates(SphSystem *sys, int filter_density, double *max_speed, double *max_acceleration);
+/* PairSums.residentIntegrate (src/pysurf/sphGpu.py:2275-2315): the second half, with the host's dt. */
+int sph_resident_integrate(SphSystem *sys, double time_step);
+
+/* WcsphSolver.advance's device loop (src/pysurf/sphSolver.py:1941-1991) without a host round trip
+ * per step: steps while time < until_time and step < max_step, each step's dt taken on the
+ * device from its own maxima (cflTimeStep, src/pysurf/sphSolver.py:1410-1424); a Shepard filter
+ * step every filter_interval steps (0 for none).  On return *time, *step and *last_dt hold the
+ * clock.  Steps are captured once into a CUDA graph and replayed. */
+int sph_advance(SphSystem *sys, double *time, int64_t *step, double *last_dt, double until_time, int64_t max_step,
+                double shortest_length, double cfl, double max_time_step, int64_t filter_interval);
+
+/* ---- Utilities ----------------------------------------------------------------------------- */
+
+/* cellOrderKey (src/pysurf/sphSolver.py:1379-1408), float64, bit-exact: keys (n,). */
+int sph_cell_order_key(const double *positions, int64_t n, int dimensions, double cell_width, const int64_t *shape,
+                       int64_t *keys, int device);
+/* sphCompiled.neighborList (src/pysurf/sphCompiled.py:133-234) of the handle's current positions
+ * (after sph_update or sph_push): every particle's neighbours closer than radius, itself
+ * excluded, by the same float64 test, so each row holds the reference's set bit for bit; rows in
+ * the walk's order.  offsets has n + 1 entries; when capacity < the total, SPH_ERR_CAPACITY and
+ * *total set. */
+int sph_neighbor_list(SphSystem *sys, double radius, int64_t *offsets, int32_t *neighbors, int64_t capacity,
+                      int64_t *total);
+/* splitParticles (src/pysurf/sphRefinement.py:136-190) on the device-resident state: the fluid
+ * particles mask (caller order, n bytes) selects each become 2^dim daughters, the first in place
+ * and the rest appended in the caller's order.  *split returns how many split. */
+int sph_split(SphSystem *sys, const uint8_t *mask, double reference_density, double length_ratio, int64_t *split);
+
+/* The same loop in three calls, for callers that overlap their own work with the steps:
+ * sph_begin_steps sets the clock and the limits on the device; sph_enqueue_steps queues `count`
+ * steps on the handle's stream and returns at once (steps past the limits do nothing);
+ * sph_finish_steps waits and reads the clock back. */
+int sph_begin_steps(SphSystem *sys, double time, int64_t step, double last_dt, double until_time, int64_t max_step,
+                    double shortest_length, double cfl, double max_time_step, int64_t filter_interval);
+int sph_enqueue_steps(SphSystem *sys, int64_t count);
+int sph_finish_steps(SphSystem *sys, double *time, int64_t *step, double *last_dt);
+
+/* Timing of the last sph_advance call (milliseconds, device events), and of each stage of the
+ * last step that ran (cells, filter, wall, gradients, momentum, kick, continuity: *count of them,
+ * named by sph_stage_name), and the kernels one step launches. */
+int sph_last_advance_ms(const SphSystem *sys, double *ms);
+int sph_stage_times(SphSystem *sys, double *ms, int64_t capacity, int64_t *count);
+const char *sph_stage_name(int64_t stage);
+int sph_step_launches(SphSystem *sys, int64_t *kernels);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PYSURF_B200_H */

@@ -1,0 +1,272 @@
+"""Workload builders: the benchmark cases laid out as the reference lays them out.
+
+Set-up only (nothing here runs per step).  Each builder restates the reference's seeding so the
+benchmarks and GPU tests run without it; tests/test_cases.py checks them against starts the
+reference itself built (tests/golden/beach.npz).
+
+    damBreak            a 1 x 2 m column in a 4 x 3 m tank, 3 wall layers, jittered lattice
+    solitaryBeach       a first-order solitary wave over a plane beach, the deltaSph scheme
+                        (src/pysurf/BreakingWave.py:658-760 with src/pysurf/waveMakers.py:282-329)
+
+Each returns a ``Case``: the particle state, the boundary, and the solver configuration the
+reference's ``SimulationConfig``/``WcsphSolver`` would hold for it.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from pysurf_b200.state import BedBoundary, ContainerBoundary, ParticleState, Profile
+
+GRAVITY = 9.80665            # src/pysurf/constants.py:29
+FRESHWATER = 998.2           # src/pysurf/constants.py:33
+
+
+@dataclass
+class Case:
+    """A particle system, its boundary and the scheme it runs (the fields of SimulationConfig it uses)."""
+    name: str
+    state: ParticleState
+    boundary: object
+    dimensions: int
+    spacing: float
+    smoothingLength: float
+    kernelType: str
+    domainMin: np.ndarray
+    domainMax: np.ndarray
+    referenceDensity: float
+    soundSpeed: float
+    gravity: np.ndarray
+    alpha: float = 0.01
+    boundaryViscosityFactor: float = 0.0
+    xsphEpsilon: float = 0.0
+    densityFloor: float = 0.0         # kg/m^3
+    densityDiffusion: str = 'none'
+    diffusionDelta: float = 0.1
+    wallExtrapolated: bool = False
+    negativePressure: bool = False
+    continuityCorrection: bool = False
+    viscosityLimiter: bool = False
+    cflNumber: float = 0.25
+    maxTimeStep: float = 1.0
+    densityFilterInterval: int = 0
+    period: float = 0.0
+    info: dict = field(default_factory=dict)
+
+    @property
+    def fluidCount(self) -> int:
+        return int(np.count_nonzero(self.state.isFluid))
+
+
+def latticePoints(lower, upper, spacing: float) -> np.ndarray:
+    """Cell centres of a square lattice filling [lower, upper] (src/pysurf/sphParticles.py:289-312)."""
+    axes = [np.arange(low + spacing / 2.0, high, spacing) for low, high in zip(lower, upper)]
+    grids = np.meshgrid(*axes, indexing='xy')
+    return np.column_stack([grid.ravel() for grid in grids])
+
+
+def containerPositions(lower, upper, spacing: float, layers: int, openTop: bool) -> np.ndarray:
+    """The wall shell of src/pysurf/sphBoundaries.py:96-124 (ContainerBoundary.positions)."""
+    lower, upper = np.asarray(lower, dtype=float), np.asarray(upper, dtype=float)
+    dim = len(lower)
+    offsets = (np.arange(layers) + 0.5) * spacing
+    axes = []
+    for axis, (low, high) in enumerate(zip(lower, upper)):
+        pieces = [low - offsets[::-1], np.arange(low + spacing / 2.0, high, spacing)]
+        if not (openTop and axis == dim - 1):
+            pieces.append(high + offsets)
+        axes.append(np.concatenate(pieces))
+    grids = np.meshgrid(*axes, indexing='xy')
+    points = np.column_stack([grid.ravel() for grid in grids])
+    interior = np.all((points > lower) & (points < upper), axis=1)
+    if openTop:
+        between = np.all((points[:, :-1] > lower[:-1]) & (points[:, :-1] < upper[:-1]), axis=1)
+        interior = between & (points[:, -1] > lower[-1])
+    return points[~interior]
+
+
+def taitDensity(pressure, rho0: float, c0: float) -> np.ndarray:
+    """src/pysurf/sphSolver.py:560-566."""
+    stiffness = rho0 * c0 ** 2 / 7.0
+    return rho0 * (1.0 + np.asarray(pressure) / stiffness) ** (1.0 / 7.0)
+
+
+def hydrostaticDensity(depth, rho0: float, c0: float, g: float = GRAVITY) -> np.ndarray:
+    """src/pysurf/sphSolver.py:1106-1120: the density carrying rho0 g z below the surface."""
+    return taitDensity(rho0 * g * np.maximum(np.asarray(depth, dtype=float), 0.0), rho0, c0)
+
+
+def damBreak(spacing: float = 0.02, seed: int = 0, kernelType: str = 'wendlandC2', diffusion: str = 'hydrostatic',
+             smoothingRatio: float = 1.3) -> Case:
+    """A 1.0 x 2.0 m water column in a 4.0 x 3.0 m tank, three layers of wall particles, the lattice
+    jittered by U(-0.01, 0.01) spacings from a seed: 5,000 fluid particles at 0.02 m."""
+    rng = np.random.default_rng(seed)
+    fluid = latticePoints([0.0, 0.0], [1.0, 2.0], spacing)
+    fluid = fluid + rng.uniform(-0.01 * spacing, 0.01 * spacing, size=fluid.shape)
+    lower, upper = np.zeros(2), np.array([4.0, 3.0])
+    wall = containerPositions(lower, upper, spacing, 3, True)
+    rho0 = 1000.0
+    height = 2.0
+    c0 = 10.0 * math.sqrt(GRAVITY * height)
+    state = ParticleState.assemble(fluid, wall, spacing, rho0)
+    state.densities = hydrostaticDensity(height - state.positions[:, 1], rho0, c0)
+    return Case('damBreak', state, ContainerBoundary(lower, upper, spacing, 3, True), 2, spacing,
+                smoothingRatio * spacing, kernelType, lower, upper, rho0, c0, np.array([0.0, -GRAVITY]), alpha=0.01,
+                densityDiffusion=diffusion, cflNumber=0.2, maxTimeStep=1.0,
+                info={'tank': [4.0, 3.0], 'column': [1.0, 2.0], 'layers': 3})
+
+
+def sloshingTank(tilt: float = 10.0, width: float = 0.2, height: float = 0.15, fill: float = 0.5,
+                 spacing: float = 0.005, **scheme) -> Case:
+    """The sloshing tank of the reference's GPU tests (tests/testSphGpu.py:441-457, built by
+    src/pysurf/WaterSim/scenarios/sloshingTank.py:108-157): water below a surface tilted `tilt` degrees
+    in a container with three wall layers, the default scheme (cubic spline at h = 1.3 dx, Shepard every
+    30 steps, XSPH 0.5, alpha 0.1) with `scheme` overriding any Case field, and a step no longer than 1 ms."""
+    slope = math.tan(math.radians(tilt))
+    fillHeight = fill * height
+    lower, upper = np.zeros(2), np.array([width, height])
+    points = latticePoints(lower, upper, spacing)
+    fluid = points[points[:, 1] < fillHeight + slope * (points[:, 0] - width / 2.0)]
+    wall = containerPositions(lower, upper, spacing, 3, True)
+    rho0 = FRESHWATER
+    c0 = 10.0 * math.sqrt(GRAVITY * height)
+    state = ParticleState.assemble(fluid, wall, spacing, rho0)
+    surface = fillHeight + slope * (state.positions[:, 0] - width / 2.0)
+    state.densities = hydrostaticDensity(surface - state.positions[:, 1], rho0, c0)
+    ratio = scheme.pop('smoothingLengthRatio', 1.3)
+    fields = dict(kernelType='cubicSpline', alpha=0.1, xsphEpsilon=0.5, cflNumber=0.25, maxTimeStep=1e-3,
+                  densityFilterInterval=30)
+    fields.update(scheme)
+    kernelType = fields.pop('kernelType')
+    if 'densityFloor' in fields:
+        fields['densityFloor'] = fields['densityFloor'] * rho0    # given as a share of rho0
+    return Case('sloshingTank', state, ContainerBoundary(lower, upper, spacing, 3, True), 2, spacing, ratio * spacing,
+                kernelType, lower, upper, rho0, c0, np.array([0.0, -GRAVITY]), **fields,
+                info={'tilt': tilt, 'fillHeight': fillHeight})
+
+
+# -- the solitary wave over a plane beach -- #
+
+def planeBeach(depth: float, toeX: float, slope: float, endX: float, startX: float = 0.0) -> Profile:
+    """src/pysurf/bathymetry.py:115-140: flat to the toe, then a constant slope."""
+    return Profile(np.array([startX, toeX, endX]), np.array([0.0, 0.0, (endX - toeX) * slope]), depth)
+
+
+def profileSample(bed: Profile, spacing: float):
+    """Points along the bed at equal arc length, both ends included (src/pysurf/bathymetry.py:272-293)."""
+    lengths = np.hypot(np.diff(bed.x), np.diff(bed.z))
+    arc = np.concatenate([[0.0], np.cumsum(lengths)])
+    count = max(2, int(round(arc[-1] / spacing)) + 1)
+    targets = np.linspace(0.0, arc[-1], count)
+    return np.interp(targets, arc, bed.x), np.interp(targets, arc, bed.z)
+
+
+def profileNormal(bed: Profile, x) -> np.ndarray:
+    """The bed's upward unit normal (src/pysurf/bathymetry.py:233-250)."""
+    slopes = np.diff(bed.z) / np.diff(bed.x)
+    index = np.clip(np.searchsorted(bed.x, x, side='right') - 1, 0, slopes.size - 1)
+    slope = slopes[index]
+    length = np.sqrt(1.0 + slope ** 2)
+    return np.stack([-slope / length, 1.0 / length], axis=-1)
+
+
+def bedPositions(bed: Profile, spacing: float, layers: int, wallTop: float | None,
+                 endWallTop: float | None) -> np.ndarray:
+    """The 2D bed's layers and end walls (src/pysurf/sphBoundaries.py:196-215, BedBoundary._profilePositions)."""
+    bedX, bedZ = profileSample(bed, spacing)
+    normal = profileNormal(bed, bedX)
+    blocks = [np.column_stack([bedX, bedZ]) - (layer + 0.5) * spacing * normal for layer in range(layers)]
+    for wallX, top, side in ((bed.startX, wallTop, -1.0), (bed.endX, endWallTop, 1.0)):
+        if top is None:
+            continue
+        bottom = float(bed.elevation(wallX)) - layers * spacing
+        heights = np.arange(bottom + spacing / 2.0, top, spacing)
+        for layer in range(layers):
+            blocks.append(np.column_stack([np.full_like(heights, wallX + side * (layer + 0.5) * spacing), heights]))
+    return np.vstack(blocks)
+
+
+def solitaryWaveSpeed(height: float, depth: float) -> float:
+    """c = sqrt(g (d + H)) (src/pysurf/waveTheory.py:192-196)."""
+    return math.sqrt(GRAVITY * (depth + height))
+
+
+def solitaryWaveDecay(height: float, depth: float) -> float:
+    """kappa = sqrt(3 H / (4 d^3)) (src/pysurf/waveTheory.py:198-202)."""
+    return math.sqrt(3.0 * height / (4.0 * depth ** 3))
+
+
+def solitaryWaveProfile(x, height: float, depth: float, crestX: float) -> np.ndarray:
+    """eta = H sech^2(kappa (x - x0)) (src/pysurf/waveTheory.py:204-225)."""
+    argument = solitaryWaveDecay(height, depth) * (np.asarray(x, dtype=float) - crestX)
+    return height / np.cosh(argument) ** 2
+
+
+def solitaryWaveFluid(bed: Profile, height: float, crestX: float, spacing: float):
+    """The lattice below the first-order solitary wave and its velocities (src/pysurf/waveMakers.py:258-329)."""
+    depth = float(max(0.0, bed.stillWaterLevel - bed.elevation(crestX)))
+    swl = bed.stillWaterLevel
+    lower = [bed.startX, float(np.min(bed.z))]
+    upper = [bed.endX, swl + height + spacing]
+    points = latticePoints(lower, upper, spacing)
+    bedZ = bed.elevation(points[:, 0])
+    surface = swl + solitaryWaveProfile(points[:, 0], height, depth, crestX)
+    keep = (points[:, 1] >= bedZ + (0.5 - 1e-9) * spacing) & (points[:, 1] < surface)
+    positions = points[keep]
+    x, y = positions[:, 0], positions[:, 1]
+    celerity = solitaryWaveSpeed(height, depth)
+    kappa = solitaryWaveDecay(height, depth)
+    eta = solitaryWaveProfile(x, height, depth, crestX)
+    etaSlope = -2.0 * kappa * eta * np.tanh(kappa * (x - crestX))
+    u = celerity * eta / (depth + eta)
+    w = -(y - bed.elevation(x)) * celerity * depth * etaSlope / (depth + eta) ** 2
+    return positions, np.column_stack([u, w])
+
+
+def solitaryBeach(particlesPerDepth: int = 64, depth: float = 1.0, height: float = 0.45, crestX: float = 10.0,
+                  toeX: float = 15.0, slope: float = 1.0 / 15.0, length: float = 60.0, smoothingRatio: float = 3.0,
+                  layers: int | None = None) -> Case:
+    """A first-order (Boussinesq sech^2) solitary wave of H/d = 0.45 at x0 = 10 d over a 1:15 beach from
+    x = 15 d, 60 d long, run with the deltaSph scheme of src/pysurf/BreakingWave.py:722-725: Wendland C2 at
+    h = 3 dx, hydrostatic diffusion, the continuity correction, extrapolated walls, the viscosity limiter and a
+    density floor of 0.9 rho0, alpha = 0.01, c0 = 10 c.  Layers default to the facade's max(3, ceil(2h/dx))."""
+    s = depth / particlesPerDepth
+    layers = max(3, math.ceil(2.0 * smoothingRatio - 1e-9)) if layers is None else layers
+    bed = planeBeach(depth, toeX, slope, length)
+    wallTop = depth + 3.0 * height
+    boundary = BedBoundary(bed, s, nLayers=layers, wallTop=wallTop, endWallTop=None, wallX=bed.startX)
+    fluid, velocities = solitaryWaveFluid(bed, height, crestX, s)
+    rho0 = FRESHWATER
+    state = ParticleState.assemble(fluid, bedPositions(bed, s, layers, wallTop, None), s, rho0, velocities)
+    c0 = 10.0 * solitaryWaveSpeed(height, depth)
+    surface = depth + solitaryWaveProfile(state.positions[:, 0], height, depth, crestX)
+    state.densities = hydrostaticDensity(surface - state.positions[:, 1], rho0, c0)
+    margin = (layers + 1.0) * s
+    return Case('solitaryBeach', state, boundary, 2, s, smoothingRatio * s, 'wendlandC2',
+                np.array([-margin, -margin]), np.array([length + margin, wallTop]), rho0, c0,
+                np.array([0.0, -GRAVITY]), alpha=0.01, densityFloor=0.9 * rho0, densityDiffusion='hydrostatic',
+                wallExtrapolated=True, continuityCorrection=True, viscosityLimiter=True, cflNumber=0.25,
+                maxTimeStep=1.0,
+                info={'depth': depth, 'H/d': height / depth, 'crestX': crestX, 'toeX': toeX, 'slope': slope,
+                      'length': length, 'ppd': particlesPerDepth, 'layers': layers})
+
+
+def pairSumsFor(case: Case, cellsPerSupport: int | None = None, device: int = 0):
+    """A PairSums set up for a case: the switches WcsphSolver.__init__ sets (src/pysurf/sphSolver.py:1499-1518)
+    and the physics WcsphSolver.advance sets (src/pysurf/sphSolver.py:1970-1972)."""
+    from pysurf_b200.sphGpu import PairSums
+    sums = PairSums(case.dimensions, case.smoothingLength, case.domainMin, case.domainMax, case.period,
+                    device=device, kernelType=case.kernelType)
+    if cellsPerSupport is not None:
+        sums.setCellsPerSupport(cellsPerSupport)
+    sums.setDiffusion(case.densityDiffusion, case.diffusionDelta, case.soundSpeed, case.referenceDensity,
+                      abs(float(case.gravity[-1])))
+    sums.setWallPressure(case.wallExtrapolated)
+    sums.setNegativePressure(case.negativePressure)
+    sums.setContinuityCorrection(case.continuityCorrection)
+    sums.setViscosityLimiter(case.viscosityLimiter)
+    sums.setPhysics(case.referenceDensity, case.soundSpeed, case.alpha, case.boundaryViscosityFactor, case.gravity,
+                    case.xsphEpsilon, case.densityFloor)
+    return sums

@@ -1,0 +1,272 @@
+// sph_internal.cuh -- shared types and device helpers of the B200 delta-SPH backend.
+//
+// Layout in HBM (all arrays in the current sort order, slot s = 0..n-1):
+//   master float64 state, double-buffered so a re-sort is one gather:
+//     x[a], v[a] (a < dim), rho            integrated in float64, as the reference integrates
+//   per-particle constants carried through each re-sort:
+//     m, h (float64), fluid (uint8), orig (int32: the caller's index of the slot)
+//   the sweeps' float32 frame, rebuilt from the master each step:
+//     pa  float4  2D (hx, hy, lx, ly)      3D (hx, hy, hz, hs)
+//     pb  float4  2D (m, hs, dev, -)       3D (lx, ly, lz, m)
+//     kin float4  2D (vx, vy, rho, p)      3D (vx, vy, vz, rho)
+//     aux float2  3D (p, dev)
+//   hi + lo is each float64 coordinate split into a float32 point and its float32 remainder, so a
+//   separation (hi_i - hi_j) + (lo_i - lo_j) keeps the float64 positions' digits without float64
+//   arithmetic (src/pysurf/sphGpu.py:227-242 states the same split).  hs is +h for a fluid
+//   particle and -h for a boundary particle; dev is rho - rho0 in float32, taken in float64
+//   (src/pysurf/sphGpu.py:1031-1038), so neighbours' density differences keep their digits.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace sph {
+
+constexpr int kBlock = 128;                 // threads per sweep block
+constexpr float kViscositySoftening = 0.01f;   // mu_ij's r^2 + 0.01 h^2 (src/pysurf/sphSolver.py:213)
+constexpr float kCloseDistance = 0.3f;      // limiter fade (src/pysurf/sphSolver.py:220-221)
+constexpr float kFoldWidth = 0.2f;
+constexpr float kCandidateMargin = 1.0001f; // on r^2, as the reference's coarse test (src/pysurf/sphGpu.py:99)
+
+// Error flags the device raises; the host reads them after each call that syncs.
+enum DeviceError : int {
+    kErrNonFinite = 1,      // a position, velocity or density stopped being finite
+    kErrTimeStep = 2,       // the step collapsed (dt not positive and finite)
+};
+
+// Everything a sweep needs besides the arrays; passed by value.
+struct Params {
+    int n;                  // particles
+    int dim;
+    int kind;               // 0 cubic spline, 1 Wendland C2
+    int mixedH;             // particles carry different smoothing lengths
+    float hMax;             // longest smoothing length, sizes the cells
+    float sigmaUnit;        // kernel sigma at h = 1
+    // grid: cell c = (cz * ny + cy) * nx + cx, x fastest; coordinates clamped onto the grid
+    double origin[3];
+    double cellWidth;
+    int nc[3];
+    int ncs;                // cells per support: the stencil is +-ncs cells
+    int precise;            // separations from point + remainder (1) or the float32 points alone (0)
+    double period;          // periodic y axis length, 0 for none
+    float periodF;
+    // physics
+    float c0, alpha, boundaryFactor;
+    float g[3];
+    double rho0, stiffness, densityFloor;  // the equation of state's rho0 and B = rho0 c0^2 / 7
+    double devReference;    // the diffusion's rho0: deviations are rho - devReference
+    float rho0F;            // devReference in float32, for the hydrostatic subtraction
+    int tension;            // the fluid may carry negative pressure
+    int diffusion;          // 0 none, 1 molteni, 2 hydrostatic, 3 antuono
+    float diffusionFactor;  // 2 delta c0
+    float gravityOverSound; // g / c0^2, for the hydrostatic subtraction
+    int corrected;          // continuity takes L_i grad W
+    int limited;            // viscosity limiter
+    int wallExtrapolated;
+    float xsphEpsilon;
+    double gravity64[3];
+};
+
+// The float32 frame and the float64 master state, current buffers.
+struct Frame {
+    float4 *pa, *pb, *kin;
+    float2 *aux;
+    int *cell;              // sorted cell index of each slot
+    const int *cellStart;   // lower bound of each cell in the sorted order, numCells + 1 entries
+    float4 *G0, *G1, *G2;   // velocity gradient rows (2D: G0 = (G00, G01, G10, G11))
+    float4 *L0, *L1, *L2;   // correction matrix rows, same packing
+    float4 *gradRho;        // renormalized density gradient
+    float4 *acc;            // acceleration (w: unused)
+    float *rate;            // d rho / dt
+    float *scalar;          // scratch per particle (Shepard, wall pressure outputs)
+    float4 *vec;            // scratch per particle (XSPH transport velocity)
+    // master (current buffers)
+    double *x[3], *v[3], *rho, *m, *h;
+    uint8_t *fluid;
+    int *orig;
+};
+
+// Step control on the device: the time step is taken from the step's own maxima on the device,
+// so a run of steps needs no host round trip (src/pysurf/sphSolver.py:1410-1424, 1980-1989).
+struct Control {
+    double time, untilTime, dt;
+    long long step, lastStep;
+    double vmax, amax;          // this step's fluid maxima
+    double hMin, cfl, maxTimeStep;
+    int active;                 // this step runs
+    int hostDt;                 // dt comes from the host (residentIntegrate), not the maxima
+    int filterNow;              // host-driven steps: this step filters the density (Shepard)
+    long long filterInterval;   // device loop: filter every this many steps, 0 for none
+    unsigned int ticket;        // last-block-done counter of the maxima reduction
+    int error;                  // DeviceError flags
+};
+
+// ------------------------------------------------------------------------------------------
+// Kernels W and dW/dr / r: src/pysurf/sphKernels.py:108-648; src/pysurf/sphGpu.py:139-204.
+// ------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ float sigmaAt(float unit, float h, int dim)
+{
+    return dim == 2 ? unit / (h * h) : unit / (h * h * h);
+}
+
+template <int K>
+__device__ __forceinline__ float kernelValue(float q, float sigma)
+{
+    if (K == 1) {
+        if (q >= 2.0f) return 0.0f;
+        float rest = 1.0f - 0.5f * q, sq = rest * rest;
+        return sigma * sq * sq * (2.0f * q + 1.0f);
+    }
+    if (q < 1.0f) return sigma * (1.0f - 1.5f * q * q + 0.75f * q * q * q);
+    if (q < 2.0f) { float rest = 2.0f - q; return sigma * 0.25f * rest * rest * rest; }
+    return 0.0f;
+}
+
+// dW/dr at distance r = q h, for r < 2h.
+template <int K>
+__device__ __forceinline__ float kernelSlope(float q, float h, float sigma)
+{
+    if (K == 1) {
+        float rest = 1.0f - 0.5f * q;
+        return -5.0f * sigma * q * rest * rest * rest / h;
+    }
+    if (q < 1.0f) return sigma * (-3.0f * q + 2.25f * q * q) / h;
+    float rest = 2.0f - q;
+    return sigma * (-0.75f * rest * rest) / h;
+}
+
+__device__ __forceinline__ int clampi(int a, int lo, int hi) { return a < lo ? lo : (a > hi ? hi : a); }
+
+// Cell coordinate of a float64 coordinate along an axis, clamped onto the grid.  Clamping is
+// monotone and never parts two cells further than they were, so the +-ncs stencil still finds
+// every neighbour of a particle outside the grid; only its candidates grow.
+__device__ __forceinline__ int cellCoordinate(double value, double origin, double width, int count)
+{
+    double f = floor((value - origin) / width);
+    if (f < 0.0) return 0;
+    if (f > (double)(count - 1)) return count - 1;
+    return (int)f;
+}
+
+// ------------------------------------------------------------------------------------------
+// Frame access per dimension.
+// ------------------------------------------------------------------------------------------
+
+template <int D> struct Pos;
+template <> struct Pos<2> {
+    float hx, hy, lx, ly;
+};
+template <> struct Pos<3> {
+    float hx, hy, hz, lx, ly, lz;
+};
+
+// A particle's signed smoothing length and mass.
+template <int D> __device__ __forceinline__ float signedLength(const Frame &F, int j);
+template <> __device__ __forceinline__ float signedLength<2>(const Frame &F, int j) { return __ldg(&F.pb[j].y); }
+template <> __device__ __forceinline__ float signedLength<3>(const Frame &F, int j) { return __ldg(&F.pa[j].w); }
+
+template <int D> __device__ __forceinline__ float massOf(const Frame &F, int j);
+template <> __device__ __forceinline__ float massOf<2>(const Frame &F, int j) { return __ldg(&F.pb[j].x); }
+template <> __device__ __forceinline__ float massOf<3>(const Frame &F, int j) { return __ldg(&F.pb[j].w); }
+
+template <int D> __device__ __forceinline__ float pressureOf(const Frame &F, int j);
+template <> __device__ __forceinline__ float pressureOf<2>(const Frame &F, int j) { return __ldg(&F.kin[j].w); }
+template <> __device__ __forceinline__ float pressureOf<3>(const Frame &F, int j) { return __ldg(&F.aux[j].x); }
+
+template <int D> __device__ __forceinline__ float deviationOf(const Frame &F, int j);
+template <> __device__ __forceinline__ float deviationOf<2>(const Frame &F, int j) { return __ldg(&F.pb[j].z); }
+template <> __device__ __forceinline__ float deviationOf<3>(const Frame &F, int j) { return __ldg(&F.aux[j].y); }
+
+template <int D> __device__ __forceinline__ float densityOf(const Frame &F, int j);
+template <> __device__ __forceinline__ float densityOf<2>(const Frame &F, int j) { return __ldg(&F.kin[j].z); }
+template <> __device__ __forceinline__ float densityOf<3>(const Frame &F, int j) { return __ldg(&F.kin[j].w); }
+
+// Velocity (float32) of slot j.
+template <int D> __device__ __forceinline__ void velocityOf(const Frame &F, int j, float v[3])
+{
+    float4 k = __ldg(&F.kin[j]);
+    v[0] = k.x; v[1] = k.y; v[2] = D == 3 ? k.z : 0.0f;
+}
+
+// Candidate coordinates (the float32 points alone) and the precise separation.
+template <int D> __device__ __forceinline__ void pointOf(const Frame &F, int j, float p[3]);
+template <> __device__ __forceinline__ void pointOf<2>(const Frame &F, int j, float p[3])
+{
+    float4 a = __ldg(&F.pa[j]); p[0] = a.x; p[1] = a.y; p[2] = 0.0f;
+}
+template <> __device__ __forceinline__ void pointOf<3>(const Frame &F, int j, float p[3])
+{
+    float4 a = __ldg(&F.pa[j]); p[0] = a.x; p[1] = a.y; p[2] = a.z;
+}
+
+template <int D> __device__ __forceinline__ void remainderOf(const Frame &F, int j, float l[3]);
+template <> __device__ __forceinline__ void remainderOf<2>(const Frame &F, int j, float l[3])
+{
+    float4 a = __ldg(&F.pa[j]); l[0] = a.z; l[1] = a.w; l[2] = 0.0f;
+}
+template <> __device__ __forceinline__ void remainderOf<3>(const Frame &F, int j, float l[3])
+{
+    float4 b = __ldg(&F.pb[j]); l[0] = b.x; l[1] = b.y; l[2] = b.z;
+}
+
+// Matrix rows (dim x dim) packed in float4 rows.
+template <int D> __device__ __forceinline__ void loadMatrix(const float4 *R0, const float4 *R1, const float4 *R2,
+                                                            int j, float M[3][3]);
+template <> __device__ __forceinline__ void loadMatrix<2>(const float4 *R0, const float4 *, const float4 *, int j,
+                                                          float M[3][3])
+{
+    float4 a = __ldg(&R0[j]);
+    M[0][0] = a.x; M[0][1] = a.y; M[1][0] = a.z; M[1][1] = a.w;
+}
+template <> __device__ __forceinline__ void loadMatrix<3>(const float4 *R0, const float4 *R1, const float4 *R2, int j,
+                                                          float M[3][3])
+{
+    float4 a = __ldg(&R0[j]), b = __ldg(&R1[j]), c = __ldg(&R2[j]);
+    M[0][0] = a.x; M[0][1] = a.y; M[0][2] = a.z;
+    M[1][0] = b.x; M[1][1] = b.y; M[1][2] = b.z;
+    M[2][0] = c.x; M[2][1] = c.y; M[2][2] = c.z;
+}
+
+template <int D> __device__ __forceinline__ void storeMatrix(float4 *R0, float4 *R1, float4 *R2, int j,
+                                                             const float M[3][3]);
+template <> __device__ __forceinline__ void storeMatrix<2>(float4 *R0, float4 *, float4 *, int j, const float M[3][3])
+{
+    R0[j] = make_float4(M[0][0], M[0][1], M[1][0], M[1][1]);
+}
+template <> __device__ __forceinline__ void storeMatrix<3>(float4 *R0, float4 *R1, float4 *R2, int j,
+                                                           const float M[3][3])
+{
+    R0[j] = make_float4(M[0][0], M[0][1], M[0][2], 0.0f);
+    R1[j] = make_float4(M[1][0], M[1][1], M[1][2], 0.0f);
+    R2[j] = make_float4(M[2][0], M[2][1], M[2][2], 0.0f);
+}
+
+template <int D> __device__ __forceinline__ float determinant(const float M[3][3])
+{
+    if (D == 2) return M[0][0] * M[1][1] - M[0][1] * M[1][0];
+    return M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) - M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0])
+         + M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
+}
+
+template <int D> __device__ __forceinline__ void inverse(const float M[3][3], float out[3][3])
+{
+    float det = determinant<D>(M);
+    float s = 1.0f / det;
+    if (D == 2) {
+        out[0][0] = M[1][1] * s; out[0][1] = -M[0][1] * s;
+        out[1][0] = -M[1][0] * s; out[1][1] = M[0][0] * s;
+        return;
+    }
+    out[0][0] = (M[1][1] * M[2][2] - M[1][2] * M[2][1]) * s;
+    out[0][1] = (M[0][2] * M[2][1] - M[0][1] * M[2][2]) * s;
+    out[0][2] = (M[0][1] * M[1][2] - M[0][2] * M[1][1]) * s;
+    out[1][0] = (M[1][2] * M[2][0] - M[1][0] * M[2][2]) * s;
+    out[1][1] = (M[0][0] * M[2][2] - M[0][2] * M[2][0]) * s;
+    out[1][2] = (M[0][2] * M[1][0] - M[0][0] * M[1][2]) * s;
+    out[2][0] = (M[1][0] * M[2][1] - M[1][1] * M[2][0]) * s;
+    out[2][1] = (M[0][1] * M[2][0] - M[0][0] * M[2][1]) * s;
+    out[2][2] = (M[0][0] * M[1][1] - M[0][1] * M[1][0]) * s;
+}
+
+}  // namespace sph

@@ -1,0 +1,80 @@
+// sph_kernels.h -- host-side view of the kernels in sph_kernels.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "sph_internal.cuh"
+
+namespace sph {
+
+// The float64 master state's arrays, in one buffer set's order.
+struct MasterView {
+    double *x[3], *v[3], *rho, *m, *h;
+    uint8_t *fluid;
+    int *orig;
+};
+
+// The boundary the device steps enforce (kind 0 none, 1 container, 2 bed, 3 height field).
+struct Enforcement {
+    int kind;
+    double lower[3], upper[3];
+    int openTop;
+    const double *bedX, *bedZ;
+    int bedCount;
+    double clearance;
+    int sideWalls;
+    double width;
+    int offshoreWall;
+    double wallX, pistonSpeed, endLimit;
+    const double *table;
+    int tableNx, tableNy;
+    double originX, originY, stepX, stepY, lowY, highY, lowX, highX;
+};
+
+enum class Stage { ShepardSum, ShepardApply, Wall, Gradients, Momentum, Kick, Continuity, Xsph };
+
+struct LaunchArgs {
+    Params P;
+    Frame F;
+    cudaStream_t stream;
+    Control *ctl;
+    double *blockMaxima;
+    Enforcement E;
+    int flag;               // Wall: write the density too; Continuity / Xsph: the epilogue's mode
+    int wantG, wantL, wantRho;
+    float floorDet;
+    const float *densities; // Xsph: the densities it divides by; null for the frame's
+};
+
+void launchStage(const LaunchArgs &A, Stage stage);
+void launchCellKeys(const Params &P, int n, const MasterView &M, int origBits, unsigned long long *keys, int *vals,
+                    const Control *ctl, cudaStream_t st);
+int radixBlocks(int n);
+void launchRadixSort(int n, int bits, unsigned long long *keys, int *vals, unsigned long long *keysAlt, int *valsAlt,
+                     unsigned *counts, const Control *ctl, cudaStream_t st, unsigned long long **keysOut,
+                     int **valsOut);
+void launchCellStart(const unsigned long long *sortedKeys, int n, int origBits, int numCells, int *cellStart,
+                     const Control *ctl, cudaStream_t st);
+void launchGather(const Params &P, int n, const int *perm, const unsigned long long *sortedKeys, int origBits,
+                  const MasterView &from, const MasterView &to, const Frame &F, const Control *ctl, cudaStream_t st);
+void launchLoadFields(const Params &P, int n, const int *orig, const double *v, const double *rho, const double *p,
+                      double deviationReference, const Frame &F, cudaStream_t st);
+void launchLoadMaster(int n, int dim, const double *x, const double *v, const double *rho, const double *m,
+                      const uint8_t *fluid, const double *h, double hDefault, const MasterView &M, cudaStream_t st);
+void launchStepEnd(Control *ctl, cudaStream_t st);
+void launchEnforce(int n, int dim, const MasterView &M, const Enforcement &E, cudaStream_t st);
+void launchRefreshDensity(int n, const double *rho, float *out, cudaStream_t st);
+void launchScatterDouble(int n, int dim, const int *orig, const double *const *columns, double *out, cudaStream_t st);
+void launchScatterFloat4(int n, int dim, const int *orig, const float4 *values, double *out, cudaStream_t st);
+void launchScatterFloat(int n, const int *orig, const float *values, double *out, cudaStream_t st);
+void launchScatterMatrix(int n, int dim, const int *orig, const Frame &F, int which, double *out, cudaStream_t st);
+void launchScatterPressure(int n, int dim, const int *orig, const Frame &F, double *out, cudaStream_t st);
+void launchNeighbourRows(const Params &P, const Frame &F, const int64_t *offsets, int *rows, long long *counts,
+                         double radius2, cudaStream_t st);
+void launchCellOrderKey(int n, int dim, const double *positions, double width, const long long shape[3],
+                        long long *keys, cudaStream_t st);
+void launchSplit(int n, int dim, const MasterView &M, const uint8_t *chosen, const int *rank, double rho0,
+                 double lengthRatio, int total, cudaStream_t st);
+
+}  // namespace sph

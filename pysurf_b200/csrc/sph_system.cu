@@ -1,0 +1,1403 @@
+// sph_system.cu -- the particle-system handle behind the C-ABI (include/pysurf_b200.h).
+//
+// One handle holds one particle system on one device: the float64 master state (double
+// buffered), the float32 sweep frame, the cell list and the sort scratch, all sized to a
+// capacity that grows by a quarter at a time as the reference's device arrays do
+// (src/pysurf/sphGpu.py:1572-1594).  Host arrays move through pinned staging, or straight from
+// the caller's memory when it is pinned already.
+//
+// A device-resident step is captured once into a CUDA graph, twice over: a step moves the master
+// to the other buffer, so one graph starts from each.  Runs of steps replay them alternately;
+// each step's time step is taken on the device from its own maxima, and the host reads the clock
+// back only when it must decide whether to launch more.  Events between the stages of each graph
+// time every stage of the last step (sph_stage_times).
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "../../include/pysurf_b200.h"
+#include "sph_kernels.h"
+
+using namespace sph;
+
+namespace {
+
+constexpr int kStageCount = 7;      // cells, filter, wall, gradients, momentum, kick, continuity
+
+thread_local std::string lastError;
+
+int fail(int code, const std::string &message)
+{
+    lastError = message;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                                   \
+    do {                                                                                                 \
+        cudaError_t err_ = (expr);                                                                       \
+        if (err_ != cudaSuccess)                                                                         \
+            return fail(err_ == cudaErrorMemoryAllocation ? SPH_ERR_NOMEM : SPH_ERR_CUDA,               \
+                        std::string(#expr) + ": " + cudaGetErrorString(err_));                           \
+    } while (0)
+
+#define TRY(expr)                                                                                        \
+    do {                                                                                                 \
+        int status_ = (expr);                                                                            \
+        if (status_ != SPH_OK) return status_;                                                           \
+    } while (0)
+
+double sigmaUnit(int kind, int dim)
+{
+    const double pi = 3.14159265358979323846;
+    if (kind == 1) return dim == 2 ? 7.0 / (4.0 * pi) : 21.0 / (16.0 * pi);
+    return dim == 2 ? 10.0 / (7.0 * pi) : 1.0 / pi;
+}
+
+int bitsFor(long long value)
+{
+    int bits = 1;
+    while ((1ll << bits) <= value) ++bits;
+    return bits;
+}
+
+template <class T>
+int deviceAlloc(T **ptr, size_t count)
+{
+    *ptr = nullptr;
+    if (count == 0) count = 1;
+    cudaError_t err = cudaMalloc((void **)ptr, count * sizeof(T));
+    if (err != cudaSuccess) return fail(SPH_ERR_NOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(err));
+    return SPH_OK;
+}
+
+}  // namespace
+
+struct SphSystem {
+    // configuration
+    int device = 0;
+    int dim = 2, kind = 0;
+    double h = 0.0;
+    double domainMin[3] = {0, 0, 0}, domainMax[3] = {0, 0, 0};
+    double period = 0.0;
+    int precise = 1;
+    int ncs = 1;
+    int64_t gridShape[3] = {1, 1, 1};
+    // physics (setPhysics) and the sums' switches
+    double rho0 = 1000.0, c0 = 1.0, alpha = 0.0, boundaryFactor = 0.0, gravity[3] = {0, 0, 0};
+    double xsphEpsilon = 0.0, densityFloor = 0.0;
+    int diffusionMode = 0;
+    double diffusionDelta = 0.1, diffusionC0 = 1.0, diffusionRho0 = 1000.0, diffusionG = 0.0;
+    int wallExtrapolated = 0, tension = 0, corrected = 0, limited = 0;
+    bool physicsSet = false;
+    Enforcement enforcement{};
+    double *bedX = nullptr, *bedZ = nullptr, *table = nullptr;
+    // state
+    int n = 0, capacity = 0;
+    bool mixedH = false;
+    double hMin = 0.0;
+    int cur = 0;
+    bool resident = false;      // master holds velocities and densities (push)
+    bool framed = false;        // the frame is in the master's order (its pressures are current)
+    bool cellsFresh = false;    // the cell list matches the master's positions
+    // grid
+    double origin[3] = {0, 0, 0}, cellWidth = 0.0;
+    int nc[3] = {1, 1, 1};
+    int numCells = 1;
+    // device memory
+    MasterView master[2]{};
+    float4 *pa = nullptr, *pb = nullptr, *kin = nullptr, *G[3] = {}, *L[3] = {}, *gradRho = nullptr, *acc = nullptr,
+           *vec = nullptr;
+    float2 *aux = nullptr;
+    float *rate = nullptr, *scalar = nullptr;
+    int *cell = nullptr, *cellStart = nullptr;
+    unsigned long long *keys[2] = {nullptr, nullptr};
+    int *vals[2] = {nullptr, nullptr};
+    unsigned *counts = nullptr;
+    double *blockMaxima = nullptr;
+    Control *ctl = nullptr;
+    // Caller-order float64 staging on the device, kStageSlots rows of capacity doubles:
+    //   inputs   0-2 vectors, 3 densities, 4 pressures (loadState: 0-2 x, 3-5 v, 6 rho, 7 m, 8 h)
+    //   outputs  5-13 (up to dim x dim per particle)
+    //   15       a small table of device pointers
+    static constexpr int kStageSlots = 16;
+    static constexpr int kOutSlot = 5;
+    double *dStage = nullptr;
+    uint8_t *dStageU8 = nullptr;
+    int *dRank = nullptr;
+    Control *hCtl = nullptr;    // pinned
+    int cellStartCapacity = 0;
+    // execution
+    cudaStream_t stream = nullptr;
+    bool ownStream = false;
+    cudaGraphExec_t graphs[2] = {nullptr, nullptr};  // one step from master buffer 0, one from buffer 1
+    cudaEvent_t stageEvents[2][kStageCount + 1] = {};
+    bool graphDirty = true;
+    bool graphFilter = false;
+    int graphNodes = 0;
+    int lastGraph = 0;
+    int beginCur = 0;
+    long long beginStep = 0;
+    long long enqueued = 0;
+    cudaEvent_t evStart = nullptr, evStop = nullptr;
+    double lastAdvanceMs = 0.0;
+
+    // ---- memory ------------------------------------------------------------------------------
+
+    int freeArrays()
+    {
+        for (int b = 0; b < 2; ++b) {
+            MasterView &M = master[b];
+            for (int a = 0; a < 3; ++a) { cudaFree(M.x[a]); cudaFree(M.v[a]); }
+            cudaFree(M.rho); cudaFree(M.m); cudaFree(M.h); cudaFree(M.fluid); cudaFree(M.orig);
+            M = MasterView{};
+            cudaFree(keys[b]); cudaFree(vals[b]);
+            keys[b] = nullptr; vals[b] = nullptr;
+        }
+        void *ptrs[] = {pa, pb, kin, G[0], G[1], G[2], L[0], L[1], L[2], gradRho, acc, vec, aux, rate, scalar, cell,
+                        counts, blockMaxima, dStage, dStageU8, dRank};
+        for (void *p : ptrs) cudaFree(p);
+        pa = pb = kin = gradRho = acc = vec = nullptr;
+        for (int a = 0; a < 3; ++a) G[a] = L[a] = nullptr;
+        aux = nullptr; rate = scalar = nullptr; cell = nullptr; counts = nullptr; blockMaxima = nullptr;
+        dStage = nullptr; dStageU8 = nullptr; dRank = nullptr;
+        capacity = 0;
+        return SPH_OK;
+    }
+
+    // Arrays for at least `count` particles; with `preserve`, the current master survives.
+    int reserve(int count, bool preserve)
+    {
+        if (count <= capacity) return SPH_OK;
+        int cap = std::max(count, (int)(1.25 * capacity));
+        MasterView old = master[cur];
+        // keep the current master by moving it into freshly allocated arrays
+        MasterView fresh{};
+        for (int a = 0; a < 3; ++a) {
+            TRY(deviceAlloc(&fresh.x[a], cap));
+            TRY(deviceAlloc(&fresh.v[a], cap));
+        }
+        TRY(deviceAlloc(&fresh.rho, cap));
+        TRY(deviceAlloc(&fresh.m, cap));
+        TRY(deviceAlloc(&fresh.h, cap));
+        TRY(deviceAlloc(&fresh.fluid, cap));
+        TRY(deviceAlloc(&fresh.orig, cap));
+        if (preserve && n > 0) {
+            for (int a = 0; a < dim; ++a) {
+                CUDA_TRY(cudaMemcpyAsync(fresh.x[a], old.x[a], n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+                CUDA_TRY(cudaMemcpyAsync(fresh.v[a], old.v[a], n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+            }
+            CUDA_TRY(cudaMemcpyAsync(fresh.rho, old.rho, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+            CUDA_TRY(cudaMemcpyAsync(fresh.m, old.m, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+            CUDA_TRY(cudaMemcpyAsync(fresh.h, old.h, n * sizeof(double), cudaMemcpyDeviceToDevice, stream));
+            CUDA_TRY(cudaMemcpyAsync(fresh.fluid, old.fluid, n, cudaMemcpyDeviceToDevice, stream));
+            CUDA_TRY(cudaMemcpyAsync(fresh.orig, old.orig, n * sizeof(int), cudaMemcpyDeviceToDevice, stream));
+            CUDA_TRY(cudaStreamSynchronize(stream));
+        }
+        // the old master goes with the rest; the fresh one becomes buffer 0
+        if (old.x[0] == master[0].x[0]) master[0] = MasterView{};
+        else master[1] = MasterView{};
+        for (int a = 0; a < 3; ++a) { cudaFree(old.x[a]); cudaFree(old.v[a]); }
+        cudaFree(old.rho); cudaFree(old.m); cudaFree(old.h); cudaFree(old.fluid); cudaFree(old.orig);
+        freeArrays();
+        capacity = cap;
+        master[0] = fresh;
+        cur = 0;
+        MasterView &M = master[1];
+        for (int a = 0; a < 3; ++a) {
+            TRY(deviceAlloc(&M.x[a], cap));
+            TRY(deviceAlloc(&M.v[a], cap));
+        }
+        TRY(deviceAlloc(&M.rho, cap));
+        TRY(deviceAlloc(&M.m, cap));
+        TRY(deviceAlloc(&M.h, cap));
+        TRY(deviceAlloc(&M.fluid, cap));
+        TRY(deviceAlloc(&M.orig, cap));
+        TRY(deviceAlloc(&pa, cap));
+        TRY(deviceAlloc(&pb, cap));
+        TRY(deviceAlloc(&kin, cap));
+        TRY(deviceAlloc(&aux, cap));
+        for (int a = 0; a < 3; ++a) { TRY(deviceAlloc(&G[a], cap)); TRY(deviceAlloc(&L[a], cap)); }
+        TRY(deviceAlloc(&gradRho, cap));
+        TRY(deviceAlloc(&acc, cap));
+        TRY(deviceAlloc(&vec, cap));
+        TRY(deviceAlloc(&rate, cap));
+        TRY(deviceAlloc(&scalar, cap));
+        TRY(deviceAlloc(&cell, cap));
+        for (int b = 0; b < 2; ++b) { TRY(deviceAlloc(&keys[b], cap)); TRY(deviceAlloc(&vals[b], cap)); }
+        TRY(deviceAlloc(&counts, (size_t)256 * radixBlocks(cap)));
+        TRY(deviceAlloc(&blockMaxima, (size_t)2 * ((cap + kBlock - 1) / kBlock)));
+        TRY(deviceAlloc(&dStage, (size_t)kStageSlots * cap));
+        TRY(deviceAlloc(&dStageU8, cap));
+        TRY(deviceAlloc(&dRank, cap));
+        CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(float4) * cap, stream));
+        CUDA_TRY(cudaMemsetAsync(kin, 0, sizeof(float4) * cap, stream));
+        CUDA_TRY(cudaMemsetAsync(aux, 0, sizeof(float2) * cap, stream));
+        graphDirty = true;
+        framed = false;
+        return SPH_OK;
+    }
+
+    // ---- grid ----------------------------------------------------------------------------------
+
+    int setupGrid()
+    {
+        cellWidth = 2.0 * h / ncs;
+        long long total = 1;
+        for (int a = 0; a < 3; ++a) {
+            if (a < dim) {
+                origin[a] = domainMin[a] - cellWidth;
+                nc[a] = (int)ceil((domainMax[a] - domainMin[a]) / cellWidth) + 3;
+            } else {
+                origin[a] = 0.0;
+                nc[a] = 1;
+            }
+            total *= nc[a];
+        }
+        // cap the cells as the reference caps its grid; wider cells keep the stencil valid
+        while (total > (1ll << 25)) {
+            cellWidth *= 1.25;
+            total = 1;
+            for (int a = 0; a < dim; ++a) {
+                nc[a] = (int)ceil((domainMax[a] - domainMin[a]) / cellWidth) + 3;
+                total *= nc[a];
+            }
+        }
+        numCells = (int)total;
+        if (numCells + 1 > cellStartCapacity) {
+            cudaFree(cellStart);
+            TRY(deviceAlloc(&cellStart, numCells + 1));
+            cellStartCapacity = numCells + 1;
+        }
+        // the reference's hash grid shape (src/pysurf/sphGpu.py:1466-1478)
+        double extent[3] = {0, 0, 0};
+        for (int a = 0; a < dim; ++a) extent[a] = domainMax[a] - domainMin[a];
+        long long cells[3];
+        for (int a = 0; a < 3; ++a) {
+            long long c = (long long)ceil(extent[a] / (2.0 * h)) + 3;
+            cells[a] = c > 1 ? c : 1;
+        }
+        if (dim == 2) cells[2] = 1;
+        while (cells[0] * cells[1] * cells[2] > (1ll << 25))
+            for (int a = 0; a < 3; ++a) cells[a] = std::max((long long)(cells[a] * 0.8), 1ll);
+        for (int a = 0; a < 3; ++a) gridShape[a] = cells[a];
+        graphDirty = true;
+        framed = false;
+        return SPH_OK;
+    }
+
+    // ---- parameters ----------------------------------------------------------------------------
+
+    Params params() const
+    {
+        Params P{};
+        P.n = n;
+        P.dim = dim;
+        P.kind = kind;
+        P.mixedH = mixedH ? 1 : 0;
+        P.hMax = (float)h;
+        P.sigmaUnit = (float)sigmaUnit(kind, dim);
+        for (int a = 0; a < 3; ++a) { P.origin[a] = origin[a]; P.nc[a] = nc[a]; }
+        P.cellWidth = cellWidth;
+        P.ncs = ncs;
+        P.precise = precise;
+        P.period = period;
+        P.periodF = (float)period;
+        P.c0 = (float)c0;
+        P.alpha = (float)alpha;
+        P.boundaryFactor = (float)boundaryFactor;
+        for (int a = 0; a < 3; ++a) { P.g[a] = (float)gravity[a]; P.gravity64[a] = gravity[a]; }
+        P.rho0 = rho0;
+        P.stiffness = rho0 * c0 * c0 / 7.0;
+        P.densityFloor = densityFloor;
+        P.devReference = diffusionRho0;
+        P.rho0F = (float)diffusionRho0;
+        P.tension = tension;
+        P.diffusion = diffusionMode;
+        P.diffusionFactor = (float)(2.0 * diffusionDelta * diffusionC0);
+        P.gravityOverSound = (float)(diffusionG / (diffusionC0 * diffusionC0));
+        P.corrected = corrected;
+        P.limited = limited;
+        P.wallExtrapolated = wallExtrapolated;
+        P.xsphEpsilon = (float)xsphEpsilon;
+        return P;
+    }
+
+    Frame frame() const
+    {
+        Frame F{};
+        F.pa = pa; F.pb = pb; F.kin = kin; F.aux = aux;
+        F.cell = cell; F.cellStart = cellStart;
+        F.G0 = G[0]; F.G1 = G[1]; F.G2 = G[2];
+        F.L0 = L[0]; F.L1 = L[1]; F.L2 = L[2];
+        F.gradRho = gradRho; F.acc = acc; F.rate = rate; F.scalar = scalar; F.vec = vec;
+        const MasterView &M = master[cur];
+        for (int a = 0; a < 3; ++a) { F.x[a] = M.x[a]; F.v[a] = M.v[a]; }
+        F.rho = M.rho; F.m = M.m; F.h = M.h; F.fluid = M.fluid; F.orig = M.orig;
+        return F;
+    }
+
+    LaunchArgs args(Control *control) const
+    {
+        LaunchArgs A{};
+        A.P = params();
+        A.F = frame();
+        A.stream = stream;
+        A.ctl = control;
+        A.blockMaxima = control ? blockMaxima : nullptr;
+        A.E = enforcement;
+        A.floorDet = (float)pow(0.25, dim);
+        return A;
+    }
+
+    // ---- cell list -----------------------------------------------------------------------------
+
+    // Sort the master by (cell, caller index), permute it into the other buffer, and build the
+    // frame and the cell list.
+    // control: the device clock that gates the step (null: always runs).
+    void rebuild(const Control *control = nullptr)
+    {
+        if (n == 0) return;
+        Params P = params();
+        int origBits = bitsFor(std::max(n - 1, 1));
+        int cellBits = bitsFor(std::max(numCells - 1, 1));
+        int bits = origBits + cellBits;
+        launchCellKeys(P, n, master[cur], origBits, keys[0], vals[0], control, stream);
+        unsigned long long *sortedKeys;
+        int *perm;
+        launchRadixSort(n, bits, keys[0], vals[0], keys[1], vals[1], counts, control, stream, &sortedKeys, &perm);
+        launchCellStart(sortedKeys, n, origBits, numCells, cellStart, control, stream);
+        int next = 1 - cur;
+        Frame F = frame();
+        const MasterView &to = master[next];
+        for (int a = 0; a < 3; ++a) { F.x[a] = to.x[a]; F.v[a] = to.v[a]; }
+        F.rho = to.rho; F.m = to.m; F.h = to.h; F.fluid = to.fluid; F.orig = to.orig;
+        launchGather(P, n, perm, sortedKeys, origBits, master[cur], to, F, control, stream);
+        cur = next;
+        framed = true;
+        cellsFresh = true;
+    }
+
+    // ---- staging -------------------------------------------------------------------------------
+
+    // Copy a caller array of `count` elements of `size` bytes to device memory at `dst`.
+    int upload(void *dst, const void *src, size_t bytes)
+    {
+        if (bytes == 0) return SPH_OK;
+        cudaPointerAttributes attr;
+        bool pinned = cudaPointerGetAttributes(&attr, src) == cudaSuccess && attr.type == cudaMemoryTypeHost;
+        cudaGetLastError();
+        if (pinned) {
+            CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
+        } else {
+            CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
+        }
+        return SPH_OK;
+    }
+
+    int download(void *dst, const void *src, size_t bytes)
+    {
+        if (bytes == 0) return SPH_OK;
+        CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream));
+        return SPH_OK;
+    }
+
+    double *stage(int slot) const { return dStage + (size_t)slot * capacity; }
+
+    int readError()
+    {
+        CUDA_TRY(cudaMemcpyAsync(hCtl, ctl, sizeof(Control), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        if (hCtl->error & kErrNonFinite) return fail(SPH_ERR_NONFINITE, "the state stopped being finite");
+        if (hCtl->error & kErrTimeStep) return fail(SPH_ERR_TIMESTEP, "the time step collapsed");
+        return SPH_OK;
+    }
+
+    int writeControl()
+    {
+        CUDA_TRY(cudaMemcpyAsync(ctl, hCtl, sizeof(Control), cudaMemcpyHostToDevice, stream));
+        return SPH_OK;
+    }
+};
+
+// ================================================================================================
+// C-ABI
+// ================================================================================================
+
+#define CHECK_SYS(sys)                                                                                   \
+    do {                                                                                                 \
+        if (!(sys)) return fail(SPH_ERR_INVALID, "null handle");                                        \
+        cudaSetDevice((sys)->device);                                                                    \
+    } while (0)
+
+extern "C" {
+
+const char *sph_last_error(void) { return lastError.c_str(); }
+
+int sph_version(void) { return 1; }
+
+int sph_create(int dimensions, double smoothing_length, const double *domain_min, const double *domain_max,
+               double period, int precise, int kernel_type, int device, SphSystem **out)
+{
+    if (!out) return fail(SPH_ERR_INVALID, "null output handle");
+    *out = nullptr;
+    if (dimensions != 2 && dimensions != 3) return fail(SPH_ERR_INVALID, "dimensions must be 2 or 3");
+    if (!(smoothing_length > 0.0)) return fail(SPH_ERR_INVALID, "the smoothing length must be positive");
+    if (kernel_type != 0 && kernel_type != 1) return fail(SPH_ERR_INVALID, "kernel type must be 0 or 1");
+    if (period > 0.0 && dimensions != 3) return fail(SPH_ERR_INVALID, "a periodic axis needs three dimensions");
+    if (!domain_min || !domain_max) return fail(SPH_ERR_INVALID, "null domain");
+    CUDA_TRY(cudaSetDevice(device));
+    SphSystem *s = new SphSystem();
+    s->device = device;
+    s->dim = dimensions;
+    s->kind = kernel_type;
+    s->h = smoothing_length;
+    s->period = period > 0.0 ? period : 0.0;
+    s->precise = precise ? 1 : 0;
+    for (int a = 0; a < dimensions; ++a) {
+        s->domainMin[a] = domain_min[a];
+        s->domainMax[a] = std::max(domain_max[a], domain_min[a]);
+    }
+    s->hMin = smoothing_length;
+    int status = SPH_OK;
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) status = SPH_ERR_CUDA;
+    s->ownStream = true;
+    if (status == SPH_OK && cudaMalloc((void **)&s->ctl, sizeof(Control)) != cudaSuccess) status = SPH_ERR_NOMEM;
+    if (status == SPH_OK && cudaMallocHost((void **)&s->hCtl, sizeof(Control)) != cudaSuccess) status = SPH_ERR_NOMEM;
+    if (status == SPH_OK && (cudaEventCreate(&s->evStart) != cudaSuccess || cudaEventCreate(&s->evStop) != cudaSuccess))
+        status = SPH_ERR_CUDA;
+    for (int b = 0; b < 2 && status == SPH_OK; ++b)
+        for (int k = 0; k <= kStageCount && status == SPH_OK; ++k)
+            if (cudaEventCreate(&s->stageEvents[b][k]) != cudaSuccess) status = SPH_ERR_CUDA;
+    if (status == SPH_OK) status = s->setupGrid();
+    if (status != SPH_OK) {
+        sph_destroy(s);
+        return fail(status, "sph_create: " + lastError);
+    }
+    memset(s->hCtl, 0, sizeof(Control));
+    s->hCtl->active = 1;
+    cudaMemcpy(s->ctl, s->hCtl, sizeof(Control), cudaMemcpyHostToDevice);
+    *out = s;
+    return SPH_OK;
+}
+
+int sph_destroy(SphSystem *sys)
+{
+    if (!sys) return SPH_OK;
+    cudaSetDevice(sys->device);
+    if (sys->stream) cudaStreamSynchronize(sys->stream);
+    for (int b = 0; b < 2; ++b) {
+        if (sys->graphs[b]) cudaGraphExecDestroy(sys->graphs[b]);
+        for (int k = 0; k <= kStageCount; ++k)
+            if (sys->stageEvents[b][k]) cudaEventDestroy(sys->stageEvents[b][k]);
+    }
+    sys->freeArrays();
+    cudaFree(sys->cellStart);
+    cudaFree(sys->ctl);
+    cudaFree(sys->bedX);
+    cudaFree(sys->bedZ);
+    cudaFree(sys->table);
+    if (sys->hCtl) cudaFreeHost(sys->hCtl);
+    if (sys->evStart) cudaEventDestroy(sys->evStart);
+    if (sys->evStop) cudaEventDestroy(sys->evStop);
+    if (sys->ownStream && sys->stream) cudaStreamDestroy(sys->stream);
+    delete sys;
+    return SPH_OK;
+}
+
+int sph_grid_shape(const SphSystem *sys, int64_t shape[3])
+{
+    if (!sys || !shape) return fail(SPH_ERR_INVALID, "null argument");
+    for (int a = 0; a < 3; ++a) shape[a] = sys->gridShape[a];
+    return SPH_OK;
+}
+
+int sph_set_cells_per_support(SphSystem *sys, int cells)
+{
+    CHECK_SYS(sys);
+    if (cells < 1 || cells > 4) return fail(SPH_ERR_INVALID, "cells per support must be 1 to 4");
+    sys->ncs = cells;
+    return sys->setupGrid();
+}
+
+int sph_set_stream(SphSystem *sys, void *stream)
+{
+    CHECK_SYS(sys);
+    cudaStreamSynchronize(sys->stream);
+    if (sys->ownStream && sys->stream) cudaStreamDestroy(sys->stream);
+    if (stream) {
+        sys->stream = (cudaStream_t)stream;
+        sys->ownStream = false;
+    } else {
+        CUDA_TRY(cudaStreamCreateWithFlags(&sys->stream, cudaStreamNonBlocking));
+        sys->ownStream = true;
+    }
+    sys->graphDirty = true;
+    return SPH_OK;
+}
+
+int sph_set_diffusion(SphSystem *sys, int mode, double delta, double sound_speed, double reference_density,
+                      double gravity)
+{
+    CHECK_SYS(sys);
+    if (mode < 0 || mode > 3) return fail(SPH_ERR_INVALID, "diffusion mode must be 0 to 3");
+    if (!(sound_speed > 0.0)) return fail(SPH_ERR_INVALID, "the sound speed must be positive");
+    sys->diffusionMode = mode;
+    sys->diffusionDelta = delta;
+    sys->diffusionC0 = sound_speed;
+    sys->diffusionRho0 = reference_density;
+    sys->diffusionG = gravity;
+    sys->graphDirty = true;
+    return SPH_OK;
+}
+
+int sph_set_wall_pressure(SphSystem *sys, int extrapolated)
+{
+    CHECK_SYS(sys);
+    sys->wallExtrapolated = extrapolated ? 1 : 0;
+    sys->graphDirty = true;
+    return SPH_OK;
+}
+
+int sph_set_negative_pressure(SphSystem *sys, int enabled)
+{
+    CHECK_SYS(sys);
+    sys->tension = enabled ? 1 : 0;
+    sys->graphDirty = true;
+    return SPH_OK;
+}
+
+int sph_set_continuity_correction(SphSystem *sys, int enabled)
+{
+    CHECK_SYS(sys);
+    sys->corrected = enabled ? 1 : 0;
+    sys->graphDirty = true;
+    return SPH_OK;
+}
+
+int sph_set_viscosity_limiter(SphSystem *sys, int enabled)
+{
+    CHECK_SYS(sys);
+    sys->limited = enabled ? 1 : 0;
+    sys->graphDirty = true;
+    return SPH_OK;
+}
+
+int sph_set_physics(SphSystem *sys, double reference_density, double sound_speed, double alpha,
+                    double boundary_viscosity_factor, const double *gravity, double xsph_epsilon, double density_floor)
+{
+    CHECK_SYS(sys);
+    if (!gravity) return fail(SPH_ERR_INVALID, "null gravity");
+    if (!(reference_density > 0.0) || !(sound_speed > 0.0))
+        return fail(SPH_ERR_INVALID, "the reference density and sound speed must be positive");
+    sys->rho0 = reference_density;
+    sys->c0 = sound_speed;
+    sys->alpha = alpha;
+    sys->boundaryFactor = boundary_viscosity_factor;
+    for (int a = 0; a < 3; ++a) sys->gravity[a] = a < sys->dim ? gravity[a] : 0.0;
+    sys->xsphEpsilon = xsph_epsilon;
+    sys->densityFloor = density_floor;
+    sys->physicsSet = true;
+    sys->graphDirty = true;
+    return SPH_OK;
+}
+
+// ---- host steps -------------------------------------------------------------------------------
+
+static int loadState(SphSystem *sys, int64_t count, const double *positions, const double *velocities,
+                     const double *densities, const double *masses, const uint8_t *is_fluid, const double *lengths)
+{
+    if (count < 0 || count > (int64_t)0x3FFFFFFF) return fail(SPH_ERR_INVALID, "particle count out of range");
+    if (count > 0 && (!positions || !masses || !is_fluid)) return fail(SPH_ERR_INVALID, "null state array");
+    int n = (int)count;
+    double hMax = 0.0, hMin = sys->h;
+    bool mixed = false;
+    if (lengths && n > 0) {
+        hMax = lengths[0];
+        hMin = lengths[0];
+        for (int i = 0; i < n; ++i) {
+            hMax = std::max(hMax, lengths[i]);
+            hMin = std::min(hMin, lengths[i]);
+            if (lengths[i] != sys->h) mixed = true;
+        }
+        if (hMax > sys->h * (1.0 + 1e-9))
+            return fail(SPH_ERR_INVALID, "a smoothing length of " + std::to_string(hMax) + " m exceeds the " +
+                                             std::to_string(sys->h) + " m the cell list is built for");
+        if (!(hMin > 0.0)) return fail(SPH_ERR_INVALID, "smoothing lengths must be positive");
+    }
+    TRY(sys->reserve(n, false));
+    if (sys->n != n) sys->graphDirty = true;
+    sys->n = n;
+    sys->mixedH = mixed;
+    sys->hMin = lengths && n > 0 ? hMin : sys->h;
+    if (n == 0) return SPH_OK;
+    int dim = sys->dim;
+    double *sx = sys->stage(0), *sv = sys->stage(3), *srho = sys->stage(6), *sm = sys->stage(7), *sh = sys->stage(8);
+    TRY(sys->upload(sx, positions, sizeof(double) * n * dim));
+    if (velocities) TRY(sys->upload(sv, velocities, sizeof(double) * n * dim));
+    if (densities) TRY(sys->upload(srho, densities, sizeof(double) * n));
+    TRY(sys->upload(sm, masses, sizeof(double) * n));
+    if (lengths) TRY(sys->upload(sh, lengths, sizeof(double) * n));
+    TRY(sys->upload(sys->dStageU8, is_fluid, n));
+    sys->cur = 0;
+    launchLoadMaster(n, dim, sx, velocities ? sv : nullptr, densities ? srho : nullptr, sm, sys->dStageU8,
+                     lengths ? sh : nullptr, sys->h, sys->master[0], sys->stream);
+    CUDA_TRY(cudaGetLastError());
+    sys->framed = false;
+    return SPH_OK;
+}
+
+int sph_update(SphSystem *sys, int64_t n, const double *positions, const double *masses, const uint8_t *is_fluid,
+               const double *lengths)
+{
+    CHECK_SYS(sys);
+    TRY(loadState(sys, n, positions, nullptr, nullptr, masses, is_fluid, lengths));
+    sys->resident = false;
+    sys->rebuild();
+    CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
+static int needFrame(SphSystem *sys)
+{
+    if (!sys->framed && sys->n > 0) return fail(SPH_ERR_STATE, "no particles: call sph_update or sph_push first");
+    if (!sys->cellsFresh && sys->n > 0) sys->rebuild();
+    return SPH_OK;
+}
+
+// Upload caller-order fields into the frame.
+static int loadFields(SphSystem *sys, const double *v, const double *rho, const double *p)
+{
+    int n = sys->n, dim = sys->dim;
+    if (n == 0) return SPH_OK;
+    double *sv = sys->stage(0), *srho = sys->stage(3), *sp = sys->stage(4);
+    if (v) TRY(sys->upload(sv, v, sizeof(double) * n * dim));
+    if (rho) TRY(sys->upload(srho, rho, sizeof(double) * n));
+    if (p) TRY(sys->upload(sp, p, sizeof(double) * n));
+    Params P = sys->params();
+    launchLoadFields(P, n, sys->master[sys->cur].orig, v ? sv : nullptr, rho ? srho : nullptr, p ? sp : nullptr,
+                     sys->diffusionRho0, sys->frame(), sys->stream);
+    CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
+static int finish(SphSystem *sys, double *out, size_t count)
+{
+    if (sys->n == 0) return SPH_OK;
+    double *dOut = sys->stage(SphSystem::kOutSlot);
+    TRY(sys->download(out, dOut, sizeof(double) * count));
+    CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
+int sph_pair_accelerations(SphSystem *sys, const double *velocities, const double *densities, const double *pressures,
+                           double sound_speed, double alpha, double boundary_factor, const double *gravity,
+                           double *out)
+{
+    CHECK_SYS(sys);
+    TRY(needFrame(sys));
+    if (sys->n > 0 && (!velocities || !densities || !pressures || !gravity || !out))
+        return fail(SPH_ERR_INVALID, "null argument");
+    if (sys->n == 0) return SPH_OK;
+    TRY(loadFields(sys, velocities, densities, pressures));
+    LaunchArgs A = sys->args(nullptr);
+    A.P.c0 = (float)sound_speed;
+    A.P.alpha = (float)alpha;
+    A.P.boundaryFactor = (float)boundary_factor;
+    for (int a = 0; a < 3; ++a) A.P.g[a] = a < sys->dim ? (float)gravity[a] : 0.0f;
+    if (sys->limited) {
+        A.wantG = 1;
+        launchStage(A, Stage::Gradients);
+    }
+    launchStage(A, Stage::Momentum);
+    launchScatterFloat4(sys->n, sys->dim, A.F.orig, sys->acc, sys->stage(SphSystem::kOutSlot), sys->stream);
+    return finish(sys, out, (size_t)sys->n * sys->dim);
+}
+
+int sph_continuity_rate(SphSystem *sys, const double *velocities, const double *densities, double *out)
+{
+    CHECK_SYS(sys);
+    TRY(needFrame(sys));
+    if (sys->n == 0) return SPH_OK;
+    if (!velocities || !out) return fail(SPH_ERR_INVALID, "null argument");
+    bool needsDensity = sys->diffusionMode != 0 || sys->corrected;
+    if (needsDensity && !densities)
+        return fail(SPH_ERR_INVALID, "the diffusive term and the correction need the densities");
+    TRY(loadFields(sys, velocities, needsDensity ? densities : nullptr, nullptr));
+    LaunchArgs A = sys->args(nullptr);
+    if (sys->corrected || sys->diffusionMode == 3) {
+        A.wantL = 1;
+        A.wantRho = sys->diffusionMode == 3;
+        launchStage(A, Stage::Gradients);
+        A.wantL = A.wantRho = 0;
+    }
+    A.flag = 0;
+    launchStage(A, Stage::Continuity);
+    launchScatterFloat(sys->n, A.F.orig, sys->rate, sys->stage(SphSystem::kOutSlot), sys->stream);
+    return finish(sys, out, sys->n);
+}
+
+int sph_xsph_velocity(SphSystem *sys, const double *velocities, const double *densities, double epsilon, double *out)
+{
+    CHECK_SYS(sys);
+    TRY(needFrame(sys));
+    if (sys->n == 0) return SPH_OK;
+    if (!velocities || !densities || !out) return fail(SPH_ERR_INVALID, "null argument");
+    TRY(loadFields(sys, velocities, densities, nullptr));
+    LaunchArgs A = sys->args(nullptr);
+    A.P.xsphEpsilon = (float)epsilon;
+    A.flag = 0;
+    A.densities = nullptr;
+    launchStage(A, Stage::Xsph);
+    launchScatterFloat4(sys->n, sys->dim, A.F.orig, sys->vec, sys->stage(SphSystem::kOutSlot), sys->stream);
+    return finish(sys, out, (size_t)sys->n * sys->dim);
+}
+
+int sph_wall_pressure(SphSystem *sys, const double *densities, const double *pressures, const double *gravity,
+                      double reference_density, double sound_speed, double *out)
+{
+    CHECK_SYS(sys);
+    TRY(needFrame(sys));
+    if (sys->n == 0) return SPH_OK;
+    if (!densities || !pressures || !gravity || !out) return fail(SPH_ERR_INVALID, "null argument");
+    TRY(loadFields(sys, nullptr, densities, pressures));
+    LaunchArgs A = sys->args(nullptr);
+    for (int a = 0; a < 3; ++a) A.P.g[a] = a < sys->dim ? (float)gravity[a] : 0.0f;
+    A.P.rho0 = reference_density;
+    A.P.stiffness = reference_density * sound_speed * sound_speed / 7.0;
+    A.flag = 0;
+    launchStage(A, Stage::Wall);
+    launchScatterPressure(sys->n, sys->dim, A.F.orig, A.F, sys->stage(SphSystem::kOutSlot), sys->stream);
+    return finish(sys, out, sys->n);
+}
+
+int sph_shepard_density(SphSystem *sys, const double *densities, double *out)
+{
+    CHECK_SYS(sys);
+    TRY(needFrame(sys));
+    if (sys->n == 0) return SPH_OK;
+    if (!densities || !out) return fail(SPH_ERR_INVALID, "null argument");
+    TRY(loadFields(sys, nullptr, densities, nullptr));
+    LaunchArgs A = sys->args(nullptr);
+    launchStage(A, Stage::ShepardSum);
+    launchScatterFloat(sys->n, A.F.orig, sys->scalar, sys->stage(SphSystem::kOutSlot), sys->stream);
+    return finish(sys, out, sys->n);
+}
+
+int sph_velocity_gradients(SphSystem *sys, const double *velocities, const double *densities, double *out)
+{
+    CHECK_SYS(sys);
+    TRY(needFrame(sys));
+    if (sys->n == 0) return SPH_OK;
+    if (!velocities || !densities || !out) return fail(SPH_ERR_INVALID, "null argument");
+    TRY(loadFields(sys, velocities, densities, nullptr));
+    LaunchArgs A = sys->args(nullptr);
+    A.wantG = 1;
+    launchStage(A, Stage::Gradients);
+    launchScatterMatrix(sys->n, sys->dim, A.F.orig, A.F, 0, sys->stage(SphSystem::kOutSlot), sys->stream);
+    return finish(sys, out, (size_t)sys->n * sys->dim * sys->dim);
+}
+
+int sph_correction_matrices(SphSystem *sys, const double *densities, double *out)
+{
+    CHECK_SYS(sys);
+    TRY(needFrame(sys));
+    if (sys->n == 0) return SPH_OK;
+    if (!densities || !out) return fail(SPH_ERR_INVALID, "null argument");
+    TRY(loadFields(sys, nullptr, densities, nullptr));
+    LaunchArgs A = sys->args(nullptr);
+    A.wantL = 1;
+    launchStage(A, Stage::Gradients);
+    launchScatterMatrix(sys->n, sys->dim, A.F.orig, A.F, 1, sys->stage(SphSystem::kOutSlot), sys->stream);
+    return finish(sys, out, (size_t)sys->n * sys->dim * sys->dim);
+}
+
+int sph_density_gradients(SphSystem *sys, const double *densities, double *out)
+{
+    CHECK_SYS(sys);
+    TRY(needFrame(sys));
+    if (sys->n == 0) return SPH_OK;
+    if (!densities || !out) return fail(SPH_ERR_INVALID, "null argument");
+    TRY(loadFields(sys, nullptr, densities, nullptr));
+    LaunchArgs A = sys->args(nullptr);
+    A.wantRho = 1;
+    launchStage(A, Stage::Gradients);
+    launchScatterFloat4(sys->n, sys->dim, A.F.orig, sys->gradRho, sys->stage(SphSystem::kOutSlot), sys->stream);
+    return finish(sys, out, (size_t)sys->n * sys->dim);
+}
+
+// ---- device-resident steps ------------------------------------------------------------------------
+
+int sph_push(SphSystem *sys, int64_t n, const double *positions, const double *velocities, const double *densities,
+             const double *masses, const uint8_t *is_fluid, const double *lengths)
+{
+    CHECK_SYS(sys);
+    if (n > 0 && (!velocities || !densities)) return fail(SPH_ERR_INVALID, "null state array");
+    TRY(loadState(sys, n, positions, velocities, densities, masses, is_fluid, lengths));
+    sys->resident = true;
+    // the frame follows at the first step; make the cell list now so host-step calls work too
+    sys->rebuild();
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    return SPH_OK;
+}
+
+int sph_count(const SphSystem *sys, int64_t *n)
+{
+    if (!sys || !n) return fail(SPH_ERR_INVALID, "null argument");
+    *n = sys->n;
+    return SPH_OK;
+}
+
+int sph_pull(SphSystem *sys, double *positions, double *velocities, double *densities, double *pressures,
+             double *accelerations, double *masses, double *lengths, uint8_t *is_fluid)
+{
+    CHECK_SYS(sys);
+    int n = sys->n, dim = sys->dim;
+    if (n == 0) return SPH_OK;
+    const MasterView &M = sys->master[sys->cur];
+    // device-side scatter of each field into caller order, then one copy out each
+    double *out = sys->stage(SphSystem::kOutSlot);
+    auto scatterColumns = [&](double *const *src, int width, double *host) -> int {
+        if (!host) return SPH_OK;
+        // the column pointers go to the device through the u8 staging's tail
+        const double *ptrs[3] = {src[0], src[1], src[2]};
+        double **dptrs = (double **)sys->stage(15);
+        CUDA_TRY(cudaMemcpyAsync(dptrs, ptrs, sizeof(ptrs), cudaMemcpyHostToDevice, sys->stream));
+        launchScatterDouble(n, width, M.orig, (const double *const *)dptrs, out, sys->stream);
+        TRY(sys->download(host, out, sizeof(double) * n * width));
+        CUDA_TRY(cudaStreamSynchronize(sys->stream));
+        return SPH_OK;
+    };
+    double *xcols[3] = {M.x[0], M.x[1], M.x[2]};
+    double *vcols[3] = {M.v[0], M.v[1], M.v[2]};
+    double *rcol[3] = {M.rho, nullptr, nullptr};
+    double *mcol[3] = {M.m, nullptr, nullptr};
+    double *hcol[3] = {M.h, nullptr, nullptr};
+    TRY(scatterColumns(xcols, dim, positions));
+    TRY(scatterColumns(vcols, dim, velocities));
+    TRY(scatterColumns(rcol, 1, densities));
+    TRY(scatterColumns(mcol, 1, masses));
+    TRY(scatterColumns(hcol, 1, lengths));
+    if (pressures && sys->framed) {
+        launchScatterPressure(n, dim, M.orig, sys->frame(), out, sys->stream);
+        TRY(sys->download(pressures, out, sizeof(double) * n));
+        CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    }
+    if (accelerations) {
+        launchScatterFloat4(n, dim, M.orig, sys->acc, out, sys->stream);
+        TRY(sys->download(accelerations, out, sizeof(double) * n * dim));
+        CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    }
+    if (is_fluid) {
+        // fluid flags: gather through a float scatter of 0/1
+        std::vector<uint8_t> flags(n);
+        std::vector<int> orig(n);
+        CUDA_TRY(cudaMemcpyAsync(flags.data(), M.fluid, n, cudaMemcpyDeviceToHost, sys->stream));
+        CUDA_TRY(cudaMemcpyAsync(orig.data(), M.orig, sizeof(int) * n, cudaMemcpyDeviceToHost, sys->stream));
+        CUDA_TRY(cudaStreamSynchronize(sys->stream));
+        for (int s = 0; s < n; ++s) is_fluid[orig[s]] = flags[s];
+    }
+    CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    CUDA_TRY(cudaGetLastError());
+    return SPH_OK;
+}
+
+int sph_clear_boundary(SphSystem *sys)
+{
+    CHECK_SYS(sys);
+    sys->enforcement = Enforcement{};
+    sys->graphDirty = true;
+    return SPH_OK;
+}
+
+int sph_set_boundary_container(SphSystem *sys, const double *lower, const double *upper, int open_top)
+{
+    CHECK_SYS(sys);
+    if (!lower || !upper) return fail(SPH_ERR_INVALID, "null bounds");
+    Enforcement E{};
+    E.kind = 1;
+    for (int a = 0; a < sys->dim; ++a) { E.lower[a] = lower[a]; E.upper[a] = upper[a]; }
+    E.openTop = open_top ? 1 : 0;
+    sys->enforcement = E;
+    sys->graphDirty = true;
+    return SPH_OK;
+}
+
+int sph_set_boundary_bed(SphSystem *sys, const double *bed_x, const double *bed_z, int64_t count, double clearance,
+                         int side_walls, double width, int offshore_wall, double wall_x, double piston_speed,
+                         double end_limit)
+{
+    CHECK_SYS(sys);
+    if (!bed_x || !bed_z || count < 2) return fail(SPH_ERR_INVALID, "a bed needs at least two vertices");
+    for (int64_t k = 1; k < count; ++k)
+        if (!(bed_x[k] > bed_x[k - 1])) return fail(SPH_ERR_INVALID, "bed x must increase strictly");
+    cudaFree(sys->bedX);
+    cudaFree(sys->bedZ);
+    TRY(deviceAlloc(&sys->bedX, count));
+    TRY(deviceAlloc(&sys->bedZ, count));
+    CUDA_TRY(cudaMemcpy(sys->bedX, bed_x, sizeof(double) * count, cudaMemcpyHostToDevice));
+    CUDA_TRY(cudaMemcpy(sys->bedZ, bed_z, sizeof(double) * count, cudaMemcpyHostToDevice));
+    Enforcement E{};
+    E.kind = 2;
+    E.bedX = sys->bedX;
+    E.bedZ = sys->bedZ;
+    E.bedCount = (int)count;
+    E.clearance = clearance;
+    E.sideWalls = side_walls ? 1 : 0;
+    E.width = width;
+    E.offshoreWall = offshore_wall ? 1 : 0;
+    E.wallX = wall_x;
+    E.pistonSpeed = piston_speed;
+    E.endLimit = end_limit;
+    sys->enforcement = E;
+    sys->graphDirty = true;
+    return SPH_OK;
+}
+
+int sph_set_boundary_height_field(SphSystem *sys, const double *table, int64_t nx, int64_t ny, double origin_x,
+                                  double origin_y, double step_x, double step_y, double clearance, double low_y,
+                                  double high_y, int offshore_wall, double low_x, double high_x)
+{
+    CHECK_SYS(sys);
+    if (sys->dim != 3) return fail(SPH_ERR_INVALID, "a height field needs three dimensions");
+    if (!table || nx < 1 || ny < 1) return fail(SPH_ERR_INVALID, "an empty height table");
+    cudaFree(sys->table);
+    TRY(deviceAlloc(&sys->table, (size_t)(nx * ny)));
+    CUDA_TRY(cudaMemcpy(sys->table, table, sizeof(double) * nx * ny, cudaMemcpyHostToDevice));
+    Enforcement E{};
+    E.kind = 3;
+    E.table = sys->table;
+    E.tableNx = (int)nx;
+    E.tableNy = (int)ny;
+    E.originX = origin_x;
+    E.originY = origin_y;
+    E.stepX = step_x;
+    E.stepY = step_y;
+    E.clearance = clearance;
+    E.lowY = low_y;
+    E.highY = high_y;
+    E.offshoreWall = offshore_wall ? 1 : 0;
+    E.lowX = low_x;
+    E.highX = high_x;
+    sys->enforcement = E;
+    sys->graphDirty = true;
+    return SPH_OK;
+}
+
+int sph_enforce_boundary(SphSystem *sys)
+{
+    CHECK_SYS(sys);
+    if (sys->n == 0) return SPH_OK;
+    launchEnforce(sys->n, sys->dim, sys->master[sys->cur], sys->enforcement, sys->stream);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    sys->cellsFresh = false;    // the positions moved; the next step re-sorts anyway
+    return SPH_OK;
+}
+
+// The stages a step's events bracket, in order (sph_stage_times reports them in this order).
+static const char *const kStageNames[kStageCount] = {"cells", "filter", "wall", "gradients", "momentum", "kick",
+                                                      "continuity"};
+
+// Records the event of stage k when a set of events is given (inside a captured step graph).
+static void mark(SphSystem *sys, cudaEvent_t *events, int k)
+{
+    if (events) cudaEventRecord(events[k], sys->stream);
+}
+
+// The first half of a step: cell list, optional filter, wall pressure, gradients, momentum.
+// filter: the Shepard stage is enqueued (the device decides each step whether it is due).
+static void enqueueRates(SphSystem *sys, bool filter, cudaEvent_t *events = nullptr)
+{
+    mark(sys, events, 0);
+    sys->rebuild(sys->ctl);
+    mark(sys, events, 1);
+    LaunchArgs A = sys->args(sys->ctl);
+    if (filter) {
+        launchStage(A, Stage::ShepardSum);
+        launchStage(A, Stage::ShepardApply);
+    }
+    mark(sys, events, 2);
+    if (sys->wallExtrapolated) {
+        A.flag = 1;
+        launchStage(A, Stage::Wall);
+    }
+    mark(sys, events, 3);
+    bool wantL = sys->corrected || sys->diffusionMode == 3;
+    if (sys->limited || wantL) {
+        A.wantG = sys->limited;
+        A.wantL = wantL;
+        A.wantRho = sys->diffusionMode == 3;
+        launchStage(A, Stage::Gradients);
+        A.wantG = A.wantL = A.wantRho = 0;
+    }
+    mark(sys, events, 4);
+    launchStage(A, Stage::Momentum);
+    mark(sys, events, 5);
+}
+
+// The second half: kick, continuity with the density update, XSPH, drift and enforcement.
+static void enqueueIntegrate(SphSystem *sys, cudaEvent_t *events = nullptr)
+{
+    LaunchArgs A = sys->args(sys->ctl);
+    launchStage(A, Stage::Kick);
+    mark(sys, events, 6);
+    if (sys->xsphEpsilon > 0.0) {
+        A.flag = 1;
+        launchStage(A, Stage::Continuity);
+        launchRefreshDensity(sys->n, A.F.rho, sys->scalar, sys->stream);
+        A.flag = 2;
+        A.densities = sys->scalar;
+        launchStage(A, Stage::Xsph);
+    } else {
+        A.flag = 2;
+        launchStage(A, Stage::Continuity);
+    }
+    mark(sys, events, 7);
+}
+
+int sph_resident_rates(SphSystem *sys, int filter_density, double *max_speed, double *max_acceleration)
+{
+    CHECK_SYS(sys);
+    if (!sys->resident) return fail(SPH_ERR_STATE, "no device state: call sph_push first");
+    if (!sys->physicsSet) return fail(SPH_ERR_STATE, "call sph_set_physics first");
+    Control &c = *sys->hCtl;
+    c.active = 1;
+    c.hostDt = 1;
+    c.filterNow = filter_density ? 1 : 0;
+    c.filterInterval = 0;
+    c.ticket = 0;
+    c.error = 0;
+    c.vmax = c.amax = 0.0;
+    if (sys->n == 0) {
+        if (max_speed) *max_speed = 0.0;
+        if (max_acceleration) *max_acceleration = 0.0;
+        return SPH_OK;
+    }
+    TRY(sys->writeControl());
+    enqueueRates(sys, filter_density != 0);
+    CUDA_TRY(cudaGetLastError());
+    TRY(sys->readError());
+    if (max_speed) *max_speed = sys->hCtl->vmax;
+    if (max_acceleration) *max_acceleration = sys->hCtl->amax;
+    return SPH_OK;
+}
+
+int sph_resident_integrate(SphSystem *sys, double time_step)
+{
+    CHECK_SYS(sys);
+    if (!sys->resident) return fail(SPH_ERR_STATE, "no device state: call sph_push first");
+    if (!(time_step > 0.0) || !isfinite(time_step)) return fail(SPH_ERR_INVALID, "the time step must be positive");
+    if (sys->n == 0) return SPH_OK;
+    Control &c = *sys->hCtl;
+    c.active = 1;
+    c.hostDt = 1;
+    c.dt = time_step;
+    c.error = 0;
+    TRY(sys->writeControl());
+    enqueueIntegrate(sys);
+    CUDA_TRY(cudaGetLastError());
+    TRY(sys->readError());
+    sys->cellsFresh = false;
+    return SPH_OK;
+}
+
+// Two single-step graphs, one from each master buffer (a step moves the master to the other
+// buffer), each with events between its stages.
+static int captureSteps(SphSystem *sys, bool filter)
+{
+    for (int b = 0; b < 2; ++b) {
+        if (sys->graphs[b]) { cudaGraphExecDestroy(sys->graphs[b]); sys->graphs[b] = nullptr; }
+    }
+    const int keep = sys->cur;
+    for (int b = 0; b < 2; ++b) {
+        sys->cur = b;
+        cudaGraph_t g;
+        CUDA_TRY(cudaStreamBeginCapture(sys->stream, cudaStreamCaptureModeThreadLocal));
+        enqueueRates(sys, filter, sys->stageEvents[b]);
+        enqueueIntegrate(sys, sys->stageEvents[b]);
+        launchStepEnd(sys->ctl, sys->stream);
+        cudaError_t err = cudaStreamEndCapture(sys->stream, &g);
+        if (err != cudaSuccess) return fail(SPH_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(err));
+        err = cudaGraphInstantiate(&sys->graphs[b], g, 0);
+        if (err == cudaSuccess) {
+            size_t nodes = 0;
+            cudaGraphGetNodes(g, nullptr, &nodes);
+            sys->graphNodes = (int)nodes;
+        }
+        cudaGraphDestroy(g);
+        if (err != cudaSuccess) return fail(SPH_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(err));
+    }
+    sys->cur = keep;
+    sys->graphFilter = filter;
+    sys->graphDirty = false;
+    return SPH_OK;
+}
+
+int sph_begin_steps(SphSystem *sys, double time, int64_t step, double last_dt, double until_time, int64_t max_step,
+                    double shortest_length, double cfl, double max_time_step, int64_t filter_interval)
+{
+    CHECK_SYS(sys);
+    if (!sys->resident) return fail(SPH_ERR_STATE, "no device state: call sph_push first");
+    if (!sys->physicsSet) return fail(SPH_ERR_STATE, "call sph_set_physics first");
+    if (!(shortest_length > 0.0) || !(cfl > 0.0) || !(max_time_step > 0.0))
+        return fail(SPH_ERR_INVALID, "the shortest length, CFL number and largest step must be positive");
+    if (filter_interval < 0) return fail(SPH_ERR_INVALID, "the filter interval must not be negative");
+    Control &c = *sys->hCtl;
+    c.time = time;
+    c.untilTime = until_time;
+    c.step = step;
+    c.lastStep = max_step;
+    c.hMin = shortest_length;
+    c.cfl = cfl;
+    c.maxTimeStep = max_time_step;
+    c.filterInterval = filter_interval;
+    c.filterNow = 0;
+    c.hostDt = 0;
+    c.ticket = 0;
+    c.error = 0;
+    c.active = (time < until_time && step < max_step) ? 1 : 0;
+    c.dt = last_dt;
+    sys->beginStep = step;
+    sys->beginCur = sys->cur;
+    sys->enqueued = 0;
+    if (sys->n == 0) return SPH_OK;
+    TRY(sys->writeControl());
+    bool filter = filter_interval > 0;
+    if (sys->graphDirty || !sys->graphs[0] || filter != sys->graphFilter) TRY(captureSteps(sys, filter));
+    return SPH_OK;
+}
+
+int sph_enqueue_steps(SphSystem *sys, int64_t count)
+{
+    CHECK_SYS(sys);
+    if (count < 0) return fail(SPH_ERR_INVALID, "a negative step count");
+    if (sys->n == 0) return SPH_OK;
+    if (!sys->graphs[0]) return fail(SPH_ERR_STATE, "call sph_begin_steps first");
+    for (int64_t k = 0; k < count; ++k) {
+        CUDA_TRY(cudaGraphLaunch(sys->graphs[sys->cur], sys->stream));
+        sys->lastGraph = sys->cur;
+        sys->cur ^= 1;
+        ++sys->enqueued;
+    }
+    return SPH_OK;
+}
+
+int sph_finish_steps(SphSystem *sys, double *time, int64_t *step, double *last_dt)
+{
+    CHECK_SYS(sys);
+    if (sys->n > 0) {
+        CUDA_TRY(cudaMemcpyAsync(sys->hCtl, sys->ctl, sizeof(Control), cudaMemcpyDeviceToHost, sys->stream));
+        CUDA_TRY(cudaStreamSynchronize(sys->stream));
+        CUDA_TRY(cudaGetLastError());
+        // each step that ran moved the master to the other buffer; steps that did not, did nothing
+        const Control &c = *sys->hCtl;
+        sys->cur = sys->beginCur ^ (int)((c.step - sys->beginStep) & 1);
+        sys->cellsFresh = false;
+    }
+    const Control &c = *sys->hCtl;
+    if (time) *time = c.time;
+    if (step) *step = c.step;
+    if (last_dt) *last_dt = c.dt;
+    if (c.error & kErrNonFinite) return fail(SPH_ERR_NONFINITE, "the state stopped being finite");
+    if (c.error & kErrTimeStep) return fail(SPH_ERR_TIMESTEP, "the time step collapsed");
+    return SPH_OK;
+}
+
+int sph_advance(SphSystem *sys, double *time, int64_t *step, double *last_dt, double until_time, int64_t max_step,
+                double shortest_length, double cfl, double max_time_step, int64_t filter_interval)
+{
+    CHECK_SYS(sys);
+    if (!time || !step) return fail(SPH_ERR_INVALID, "null clock");
+    TRY(sph_begin_steps(sys, *time, *step, last_dt ? *last_dt : 0.0, until_time, max_step, shortest_length, cfl,
+                        max_time_step, filter_interval));
+    sys->lastAdvanceMs = 0.0;
+    if (sys->n == 0 || !sys->hCtl->active) return SPH_OK;
+    CUDA_TRY(cudaEventRecord(sys->evStart, sys->stream));
+    const long long maxLaunch = 1 << 20;
+    double t = *time, dt = last_dt ? *last_dt : 0.0;
+    // a first batch as long as the last step size suggests, within the step limit
+    double guess = dt > 0.0 ? (until_time - t) / dt + 1.0 : 2.0;
+    long long launches = (long long)std::max(1.0, std::min({guess, (double)(max_step - *step), (double)maxLaunch}));
+    int64_t s = *step;
+    int status = SPH_OK;
+    for (int round = 0; round < 1000000; ++round) {
+        TRY(sph_enqueue_steps(sys, launches));
+        CUDA_TRY(cudaEventRecord(sys->evStop, sys->stream));
+        status = sph_finish_steps(sys, &t, &s, &dt);
+        const Control &c = *sys->hCtl;
+        if (status != SPH_OK || !c.active) break;
+        // launch about as many steps as the clock still needs at the last step's size
+        double remaining = c.dt > 0.0 ? (c.untilTime - c.time) / c.dt : 1.0;
+        double left = (double)(c.lastStep - c.step);
+        launches = (long long)std::max(1.0, std::min({remaining + 1.0, left, (double)maxLaunch}));
+    }
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, sys->evStart, sys->evStop);
+    sys->lastAdvanceMs = ms;
+    *time = t;
+    *step = s;
+    if (last_dt) *last_dt = dt;
+    return status;
+}
+
+int sph_last_advance_ms(const SphSystem *sys, double *ms)
+{
+    if (!sys || !ms) return fail(SPH_ERR_INVALID, "null argument");
+    *ms = sys->lastAdvanceMs;
+    return SPH_OK;
+}
+
+int sph_stage_times(SphSystem *sys, double *ms, int64_t capacity, int64_t *count)
+{
+    CHECK_SYS(sys);
+    if (!count) return fail(SPH_ERR_INVALID, "null argument");
+    *count = kStageCount;
+    if (!ms || capacity < kStageCount) return ms ? fail(SPH_ERR_CAPACITY, "need one entry per stage") : SPH_OK;
+    if (!sys->graphs[0] || sys->enqueued == 0) return fail(SPH_ERR_STATE, "no step has run since sph_begin_steps");
+    CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    cudaEvent_t *events = sys->stageEvents[sys->lastGraph];
+    for (int k = 0; k < kStageCount; ++k) {
+        float t = 0.0f;
+        CUDA_TRY(cudaEventElapsedTime(&t, events[k], events[k + 1]));
+        ms[k] = t;
+    }
+    return SPH_OK;
+}
+
+const char *sph_stage_name(int64_t stage)
+{
+    return stage >= 0 && stage < kStageCount ? kStageNames[stage] : "";
+}
+
+int sph_step_launches(SphSystem *sys, int64_t *kernels)
+{
+    CHECK_SYS(sys);
+    if (!kernels) return fail(SPH_ERR_INVALID, "null argument");
+    *kernels = 0;
+    if (!sys->graphs[0]) return fail(SPH_ERR_STATE, "call sph_begin_steps first");
+    // the graph's nodes less its event records (kStageCount + 1 of them)
+    *kernels = sys->graphNodes - (kStageCount + 1);
+    return SPH_OK;
+}
+
+// ---- utilities ---------------------------------------------------------------------------------
+
+int sph_cell_order_key(const double *positions, int64_t n, int dimensions, double cell_width, const int64_t *shape,
+                       int64_t *keys, int device)
+{
+    if (n < 0 || (n > 0 && (!positions || !keys)) || !shape) return fail(SPH_ERR_INVALID, "null argument");
+    if (dimensions != 2 && dimensions != 3) return fail(SPH_ERR_INVALID, "dimensions must be 2 or 3");
+    if (!(cell_width > 0.0)) return fail(SPH_ERR_INVALID, "the cell width must be positive");
+    for (int a = 0; a < 3; ++a)
+        if (shape[a] < 1) return fail(SPH_ERR_INVALID, "grid shape entries must be positive");
+    if (n == 0) return SPH_OK;
+    CUDA_TRY(cudaSetDevice(device));
+    double *dx = nullptr;
+    long long *dk = nullptr;
+    CUDA_TRY(cudaMalloc((void **)&dx, sizeof(double) * n * dimensions));
+    cudaError_t err = cudaMalloc((void **)&dk, sizeof(long long) * n);
+    if (err != cudaSuccess) { cudaFree(dx); return fail(SPH_ERR_NOMEM, "cudaMalloc"); }
+    cudaMemcpy(dx, positions, sizeof(double) * n * dimensions, cudaMemcpyHostToDevice);
+    long long shp[3] = {shape[0], shape[1], shape[2]};
+    launchCellOrderKey((int)n, dimensions, dx, cell_width, shp, dk, 0);
+    err = cudaMemcpy(keys, dk, sizeof(long long) * n, cudaMemcpyDeviceToHost);
+    cudaFree(dx);
+    cudaFree(dk);
+    if (err != cudaSuccess) return fail(SPH_ERR_CUDA, cudaGetErrorString(err));
+    return SPH_OK;
+}
+
+int sph_neighbor_list(SphSystem *sys, double radius, int64_t *offsets, int32_t *neighbors, int64_t capacity,
+                      int64_t *total)
+{
+    CHECK_SYS(sys);
+    if (!offsets || !total) return fail(SPH_ERR_INVALID, "null argument");
+    if (!(radius > 0.0) || radius > 2.0 * sys->h * (1.0 + 1e-12))
+        return fail(SPH_ERR_INVALID, "the radius must be positive and within the cell list's support");
+    int n = sys->n;
+    offsets[0] = 0;
+    *total = 0;
+    if (n == 0) return SPH_OK;
+    if (!sys->cellsFresh) sys->rebuild();
+    Params P = sys->params();
+    Frame F = sys->frame();
+    long long *dCounts = (long long *)sys->stage(SphSystem::kOutSlot);
+    launchNeighbourRows(P, F, nullptr, nullptr, dCounts, radius * radius, sys->stream);
+    std::vector<long long> counts(n);
+    CUDA_TRY(cudaMemcpyAsync(counts.data(), dCounts, sizeof(long long) * n, cudaMemcpyDeviceToHost, sys->stream));
+    CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    for (int i = 0; i < n; ++i) offsets[i + 1] = offsets[i] + counts[i];
+    *total = offsets[n];
+    if (!neighbors || capacity < *total) return neighbors ? fail(SPH_ERR_CAPACITY, "neighbour array too small") : SPH_OK;
+    int64_t *dOffsets = nullptr;
+    int *dRows = nullptr;
+    CUDA_TRY(cudaMalloc((void **)&dOffsets, sizeof(int64_t) * (n + 1)));
+    cudaError_t err = cudaMalloc((void **)&dRows, sizeof(int) * std::max<int64_t>(*total, 1));
+    if (err != cudaSuccess) { cudaFree(dOffsets); return fail(SPH_ERR_NOMEM, "cudaMalloc"); }
+    cudaMemcpyAsync(dOffsets, offsets, sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice, sys->stream);
+    launchNeighbourRows(P, F, dOffsets, dRows, nullptr, radius * radius, sys->stream);
+    cudaMemcpyAsync(neighbors, dRows, sizeof(int) * *total, cudaMemcpyDeviceToHost, sys->stream);
+    err = cudaStreamSynchronize(sys->stream);
+    cudaFree(dOffsets);
+    cudaFree(dRows);
+    if (err != cudaSuccess) return fail(SPH_ERR_CUDA, cudaGetErrorString(err));
+    return SPH_OK;
+}
+
+int sph_split(SphSystem *sys, const uint8_t *mask, double reference_density, double length_ratio, int64_t *split)
+{
+    CHECK_SYS(sys);
+    if (!mask || !split) return fail(SPH_ERR_INVALID, "null argument");
+    if (!sys->resident) return fail(SPH_ERR_STATE, "no device state: call sph_push first");
+    if (!(length_ratio > 0.0) || length_ratio > 1.0) return fail(SPH_ERR_INVALID, "the length ratio must be in (0, 1]");
+    int n = sys->n, dim = sys->dim;
+    *split = 0;
+    if (n == 0) return SPH_OK;
+    // which mothers split, and their ranks in the caller's order, from the caller's mask and the
+    // device's fluid flags (read back in caller order)
+    std::vector<uint8_t> flags(n);
+    std::vector<int> orig(n);
+    const MasterView &M0 = sys->master[sys->cur];
+    CUDA_TRY(cudaMemcpyAsync(flags.data(), M0.fluid, n, cudaMemcpyDeviceToHost, sys->stream));
+    CUDA_TRY(cudaMemcpyAsync(orig.data(), M0.orig, sizeof(int) * n, cudaMemcpyDeviceToHost, sys->stream));
+    CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    std::vector<uint8_t> chosen(n, 0);
+    for (int s = 0; s < n; ++s) chosen[orig[s]] = mask[orig[s]] && flags[s] ? 1 : 0;
+    std::vector<int> rank(n);
+    int count = 0;
+    for (int o = 0; o < n; ++o) { rank[o] = count; count += chosen[o]; }
+    if (count == 0) return SPH_OK;
+    int perMother = (1 << dim) - 1;
+    long long grown = (long long)n + (long long)count * perMother;
+    if (grown > 0x3FFFFFFF) return fail(SPH_ERR_INVALID, "too many particles after the split");
+    TRY(sys->reserve((int)grown, true));
+    const MasterView &M = sys->master[sys->cur];
+    CUDA_TRY(cudaMemcpyAsync(sys->dStageU8, chosen.data(), n, cudaMemcpyHostToDevice, sys->stream));
+    CUDA_TRY(cudaMemcpyAsync(sys->dRank, rank.data(), sizeof(int) * n, cudaMemcpyHostToDevice, sys->stream));
+    launchSplit(n, dim, M, sys->dStageU8, sys->dRank, reference_density, length_ratio, n, sys->stream);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    sys->n = (int)grown;
+    sys->mixedH = true;
+    sys->hMin = std::min(sys->hMin, sys->h * length_ratio);
+    // hMin: the shortest length present, taken on the host from the master
+    std::vector<double> lengths(sys->n);
+    CUDA_TRY(cudaMemcpy(lengths.data(), M.h, sizeof(double) * sys->n, cudaMemcpyDeviceToHost));
+    double hMin = lengths[0];
+    bool mixed = false;
+    for (double v : lengths) { hMin = std::min(hMin, v); if (v != sys->h) mixed = true; }
+    sys->hMin = hMin;
+    sys->mixedH = mixed;
+    sys->framed = false;
+    sys->graphDirty = true;
+    *split = count;
+    return SPH_OK;
+}
+
+}  // extern "C"
