@@ -92,7 +92,7 @@ struct Control {
     double time, untilTime, dt;
     long long step, lastStep;
     double vmax, amax;          // this step's fluid maxima
-    double hMin, cfl, maxTimeStep;
+    double hMin, cfl, maxTimeStep, soundSpeed;   // the CFL step's inputs, float64 as the host takes them
     int active;                 // this step runs
     int hostDt;                 // dt comes from the host (residentIntegrate), not the maxima
     int filterNow;              // host-driven steps: this step filters the density (Shepard)

@@ -558,7 +558,7 @@ __global__ void __launch_bounds__(kBlock) momentumKernel(Params P, Frame F, Cont
         ctl->amax = amax;
         ctl->ticket = 0;
         if (!ctl->hostDt) {
-            double dt = cflTimeStep(ctl->hMin, (double)P.c0, vmax, amax, ctl->cfl, ctl->maxTimeStep);
+            double dt = cflTimeStep(ctl->hMin, ctl->soundSpeed, vmax, amax, ctl->cfl, ctl->maxTimeStep);
             if (!(dt > 0.0) || !isfinite(dt)) ctl->error |= kErrTimeStep;
             ctl->dt = dt;
         }

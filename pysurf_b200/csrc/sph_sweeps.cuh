@@ -11,10 +11,12 @@
 // (hi_i - hi_j) + (lo_i - lo_j).
 //
 // A periodic y axis (3D) is searched a second time from the particle's image across the seam
-// when it lies within its reach of the seam (src/pysurf/sphGpu.py:206-225); rows the first
-// search already walked are skipped, so no pair is counted twice whatever the grid's extent.
-// Pairs across the seam take their separation in float64: their points are a period apart and
-// their float32 difference would lose the digits the split keeps.
+// when it lies within its reach of the seam (src/pysurf/sphGpu.py:206-225).  Each walk tests its
+// candidates against its own origin (the particle, or its image), and a period longer than twice
+// the reach (the solver requires twice the support, src/pysurf/sphSolver.py:1465-1467) keeps any
+// neighbour from passing both tests.  Pairs across the seam take their separation in float64:
+// their points are a period apart and their float32 difference would lose the digits the split
+// keeps.
 #pragma once
 
 #include "sph_internal.cuh"
@@ -56,10 +58,10 @@ __device__ __forceinline__ void walkNeighbours(const Params &P, const Frame &F, 
 
     for (int image = 0; image < images; ++image) {
         const int yc = image == 0 ? cy : cyImage;
+        const float offset = image == 0 ? 0.0f : shift;     // the walk's origin: the particle, or its image
         const int y0 = max(yc - ncs, 0), y1 = min(yc + ncs, ny - 1);
         for (int zz = z0; zz <= z1; ++zz) {
             for (int yy = y0; yy <= y1; ++yy) {
-                if (image == 1 && yy >= cy - ncs && yy <= cy + ncs) continue;   // walked already
                 const int row = (zz * ny + yy) * nx;
                 const int begin = __ldg(&F.cellStart[row + x0]);
                 const int end = __ldg(&F.cellStart[row + x1 + 1]);
@@ -67,7 +69,7 @@ __device__ __forceinline__ void walkNeighbours(const Params &P, const Frame &F, 
                     float pj[3];
                     pointOf<D>(F, j, pj);
                     float cxv = pi[0] - pj[0];
-                    float cyv = (pi[1] + shift) - pj[1];
+                    float cyv = (pi[1] + offset) - pj[1];
                     float czv = D == 3 ? pi[2] - pj[2] : 0.0f;
                     float coarse = cxv * cxv + cyv * cyv + czv * czv;
                     if (coarse >= limit || j == i) continue;

@@ -1007,7 +1007,7 @@ static const char *const kStageNames[kStageCount] = {"cells", "filter", "wall", 
 // Records the event of stage k when a set of events is given (inside a captured step graph).
 static void mark(SphSystem *sys, cudaEvent_t *events, int k)
 {
-    if (events) cudaEventRecord(events[k], sys->stream);
+    if (events) cudaEventRecordWithFlags(events[k], sys->stream, cudaEventRecordExternal);
 }
 
 // The first half of a step: cell list, optional filter, wall pressure, gradients, momentum.
@@ -1156,6 +1156,7 @@ int sph_begin_steps(SphSystem *sys, double time, int64_t step, double last_dt, d
     c.hMin = shortest_length;
     c.cfl = cfl;
     c.maxTimeStep = max_time_step;
+    c.soundSpeed = sys->c0;
     c.filterInterval = filter_interval;
     c.filterNow = 0;
     c.hostDt = 0;

@@ -144,13 +144,15 @@ def test_a_resumed_run_follows_the_uninterrupted_one_bit_for_bit():
     assert np.array_equal(state.densities, whole.densities)
 
 
-def test_cell_size_changes_only_the_order_of_nothing():
-    # the cell list's resolution changes which cells are walked, not the pairs or their order of summation
+def test_cell_size_changes_only_the_order_of_sums():
+    # the cell list's resolution changes which cells are walked and the order neighbours are summed in
+    # (the sort is by cell, then index), not the pairs: the runs agree to float32 rounding of the sums
     case = caseFromRun(golden('runs.npz', 'deltaWendland'))
     a, ta, _ = deviceRun(case, 20, cellsPerSupport=1)
     b, tb, _ = deviceRun(case, 20, cellsPerSupport=2)
-    assert abs(ta - tb) <= 1e-12 * ta
+    assert abs(ta - tb) <= 1e-9 * ta
     assert np.abs(a.positions - b.positions).max() < 1e-9
+    assert np.abs(a.velocities - b.velocities).max() < 1e-5
 
 
 @pytest.mark.parametrize('mode', ['hydrostatic', 'antuono'])
