@@ -176,6 +176,24 @@ int sph_stage_times(SphSystem *sys, double *ms, int64_t capacity, int64_t *count
 const char *sph_stage_name(int64_t stage);
 int sph_step_launches(SphSystem *sys, int64_t *kernels);
 
+/* ---- For callers that cannot allocate device memory ----------------------------------------
+ *
+ * No counterpart in the reference.  Callers whose device memory is all owned by their own pool
+ * allocator, or whose loop must not enter the CUDA allocator while it runs, cannot let the library
+ * cudaMalloc.  This entry point allocates nothing: its inputs and output are the caller's device
+ * arrays, and its scratch is a fixed 64 KiB + 256 B file-scope device array that every GPU loading
+ * the library holds until exit.  It is the momentum sweep's closing reduction on its own: the
+ * largest fluid speed (float64) and acceleration (float32 length), and the time step from them
+ * (cflTimeStep, src/pysurf/sphSolver.py:1410-1424), written to out[0..2] on the device.
+ * velocities and accelerations are (n, dim) float64, is_fluid n bytes; stream a cudaStream_t or
+ * NULL.  It returns once the work is queued.  At most 16,777,216 particles: more is refused with
+ * SPH_ERR_INVALID before any launch.  The first call on a device looks the scratch's address up
+ * with that device current; make it before any stream capture begins.  Calls share the scratch:
+ * calls that overlap on the GPU race and must not be made. */
+int sph_fluid_maxima_noalloc(const double *velocities, const double *accelerations, const uint8_t *is_fluid,
+                             int64_t n, int dimensions, double smoothing_length, double sound_speed, double cfl,
+                             double max_time_step, double *out, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -76,6 +76,7 @@ SIGNATURES = {
     'sph_stage_times': [_h, _pd, _i64, _pi64],
     'sph_stage_name': [_i64],
     'sph_step_launches': [_h, _pi64],
+    'sph_fluid_maxima_noalloc': [_vp, _vp, _vp, _i64, _i, _d, _d, _d, _d, _vp, _vp],
 }
 
 

@@ -76,6 +76,11 @@ int deviceAlloc(T **ptr, size_t count)
 
 }  // namespace
 
+namespace sph {
+// Sets what sph_last_error() reports on this thread, for entry points defined in other files.
+void recordError(const std::string &message) { lastError = message; }
+}  // namespace sph
+
 struct SphSystem {
     // configuration
     int device = 0;
