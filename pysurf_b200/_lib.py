@@ -40,6 +40,8 @@ SIGNATURES = {
     'sph_grid_shape': [_h, _pi64],
     'sph_set_cells_per_support': [_h, _i],
     'sph_set_stream': [_h, _vp],
+    'sph_set_sweep_options': [_h, _i, _i],
+    'sph_neighbor_table': [_h, _pi64],
     'sph_set_diffusion': [_h, _i, _d, _d, _d, _d],
     'sph_set_wall_pressure': [_h, _i],
     'sph_set_negative_pressure': [_h, _i],

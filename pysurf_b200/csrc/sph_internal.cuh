@@ -65,6 +65,10 @@ struct Params {
     int wallExtrapolated;
     float xsphEpsilon;
     double gravity64[3];
+    // neighbour table: up to listCap entries a particle, entry k of slot i at k * listStride + i;
+    // listCap 0: no table, the sweeps walk the cells
+    int listCap;
+    int listStride;
 };
 
 // The float32 frame and the float64 master state, current buffers.
@@ -80,6 +84,8 @@ struct Frame {
     float *rate;            // d rho / dt
     float *scalar;          // scratch per particle (Shepard, wall pressure outputs)
     float4 *vec;            // scratch per particle (XSPH transport velocity)
+    int *nbr;               // neighbour table (column-major), top bit: a pair across the periodic seam
+    int *ncount;            // each slot's neighbour count (may exceed the table's capacity)
     // master (current buffers)
     double *x[3], *v[3], *rho, *m, *h;
     uint8_t *fluid;
@@ -137,6 +143,16 @@ __device__ __forceinline__ float kernelSlope(float q, float h, float sigma)
 }
 
 __device__ __forceinline__ int clampi(int a, int lo, int hi) { return a < lo ? lo : (a > hi ? hi : a); }
+
+// Tait pressure B ((rho / rho0)^7 - 1), the power as three multiplies, clamped at zero unless the
+// fluid may carry tension (src/pysurf/sphGpu.py:1058-1070).
+__device__ __forceinline__ double taitPressure(const Params &P, double rho, bool fluid)
+{
+    double ratio = rho / P.rho0, sq = ratio * ratio;
+    double p = P.stiffness * (sq * sq * sq * ratio - 1.0);
+    if (!P.tension || !fluid) p = p > 0.0 ? p : 0.0;
+    return p;
+}
 
 // Cell coordinate of a float64 coordinate along an axis, clamped onto the grid.  Clamping is
 // monotone and never parts two cells further than they were, so the +-ncs stencil still finds

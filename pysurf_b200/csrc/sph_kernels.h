@@ -32,7 +32,7 @@ struct Enforcement {
     double originX, originY, stepX, stepY, lowY, highY, lowX, highX;
 };
 
-enum class Stage { ShepardSum, ShepardApply, Wall, Gradients, Momentum, Kick, Continuity, Xsph };
+enum class Stage { ShepardSum, ShepardApply, Wall, Gradients, Momentum, Kick, Continuity, Xsph, List };
 
 struct LaunchArgs {
     Params P;
@@ -45,6 +45,8 @@ struct LaunchArgs {
     int wantG, wantL, wantRho;
     float floorDet;
     const float *densities; // Xsph: the densities it divides by; null for the frame's
+    int threads;            // threads per particle in the sweeps: 1, 2 or 4
+    int *maxCount;          // List: the largest neighbour count goes here (atomic max), when given
 };
 
 void launchStage(const LaunchArgs &A, Stage stage);

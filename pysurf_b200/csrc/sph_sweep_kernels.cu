@@ -1,0 +1,642 @@
+// sph_sweep_kernels.cu -- the neighbour sweeps of the delta-SPH step.
+//
+//   list  the step's neighbour table, from one walk over the cells
+//   S     Shepard filter (src/pysurf/sphGpu.py:768-802, 1040-1056)
+//   A     wall pressure: boundary rows over fluid neighbours (src/pysurf/sphSolver.py:1045-1106;
+//         src/pysurf/sphGpu.py:804-854)
+//   B     gradients: fluid rows, velocity gradient G (src/pysurf/sphSolver.py:1151-1190), correction L
+//         (656-689) and renormalized density gradient (691-716), from one pass over the neighbours
+//   C     momentum: fluid rows (src/pysurf/sphSolver.py:1122-1149, 1192-1230, 1328-1356;
+//         src/pysurf/sphGpu.py:303-414), with the fluid maxima (1072-1082) and the time step
+//         (src/pysurf/sphSolver.py:1410-1424) in the epilogue
+//   D     continuity (src/pysurf/sphSolver.py:623-654, 718-822; src/pysurf/sphGpu.py:430-545), with
+//         the density update (1111-1140), and, when XSPH is off, the drift and the enforcement
+//   X     XSPH (src/pysurf/sphSolver.py:1358-1377; src/pysurf/sphGpu.py:725-766), then drift and
+//         enforcement
+//
+// Each sweep is templated on the dimension D, the kernel K (0 cubic spline, 1 Wendland C2) and
+// the threads per particle T.  Sums are float32 in a fixed order, no atomics on them.
+#include <math.h>
+
+#include "sph_enforce.cuh"
+#include "sph_kernels.h"
+#include "sph_sweeps.cuh"
+
+namespace sph {
+
+// ------------------------------------------------------------------------------------------
+// The neighbour table
+// ------------------------------------------------------------------------------------------
+
+struct RecordVisit {
+    static constexpr bool kSkipCoincident = false;
+    int *column;
+    int stride, cap, count;
+    __device__ bool accept(bool) const { return true; }
+    __device__ void operator()(int j, const float *, float, float, bool, int image)
+    {
+        if (count < cap) column[(size_t)count * stride] = image ? (j | (int)0x80000000) : j;
+        ++count;
+    }
+};
+
+// Each slot's neighbours in the walk's order; the count is the whole count even when the row is
+// full (the sweeps then walk the cells for that slot).  maxCount: the largest count, when given.
+template <int D>
+__global__ void __launch_bounds__(kBlock) listKernel(Params P, Frame F, const Control *ctl, int *maxCount)
+{
+    if (ctl && !ctl->active) return;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    RecordVisit visit{F.nbr + i, P.listStride, P.listCap, 0};
+    forEachNeighbour<D, 1>(P, F, i, 0, fabsf(signedLength<D>(F, i)), visit, false);
+    F.ncount[i] = visit.count;
+    if (maxCount) atomicMax(maxCount, visit.count);
+}
+
+// ------------------------------------------------------------------------------------------
+// Sweep S: the Shepard filter
+// ------------------------------------------------------------------------------------------
+
+__device__ __forceinline__ bool filterDue(const Control *ctl)
+{
+    if (!ctl) return true;
+    if (!ctl->active) return false;
+    if (ctl->filterInterval > 0) return ctl->step > 0 && ctl->step % ctl->filterInterval == 0;
+    return ctl->filterNow != 0;
+}
+
+template <int D, int K>
+struct ShepardVisit {
+    static constexpr bool kSkipCoincident = false;
+    const Params &P; const Frame &F;
+    float num, den;
+    __device__ bool accept(bool) const { return true; }
+    __device__ void operator()(int j, const float *, float r, float h, bool, int)
+    {
+        float w = kernelValue<K>(r / h, sigmaAt(P.sigmaUnit, h, D));
+        float mj = massOf<D>(F, j);
+        num += mj * w;
+        den += mj / densityOf<D>(F, j) * w;
+    }
+};
+
+template <int D, int K, int T>
+__global__ void __launch_bounds__(kBlock) shepardKernel(Params P, Frame F, const Control *ctl)
+{
+    if (!filterDue(ctl)) return;
+    const Group<T> G = groupOf<T>();
+    const int i = G.i;
+    if (i >= P.n) return;
+    float hI = fabsf(signedLength<D>(F, i));
+    // the particle itself first, as the reference's sums start (src/pysurf/sphGpu.py:781-783)
+    float own = sigmaAt(P.sigmaUnit, hI, D);
+    float mi = massOf<D>(F, i);
+    ShepardVisit<D, K> visit{P, F, G.t == 0 ? mi * own : 0.0f, G.t == 0 ? mi / densityOf<D>(F, i) * own : 0.0f};
+    forEachNeighbour<D, T>(P, F, i, G.t, hI, visit);
+    float num = groupSum<T>(visit.num, G.mask), den = groupSum<T>(visit.den, G.mask);
+    if (G.t != 0) return;
+    F.scalar[i] = num / den;
+}
+
+// The fluid takes its filtered density (float64 from the float32 filter, as the reference
+// stores it), its deviation and its pressure; the boundary keeps its own.
+template <int D>
+__global__ void applyShepardKernel(Params P, Frame F, const Control *ctl)
+{
+    if (!filterDue(ctl)) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n || !F.fluid[i]) return;
+    float filtered = F.scalar[i];
+    double rho = (double)filtered;
+    F.rho[i] = rho;
+    float p = (float)taitPressure(P, rho, true);
+    float dev = (float)(rho - P.devReference);
+    if (D == 2) {
+        F.kin[i].z = filtered; F.kin[i].w = p; F.pb[i].z = dev;
+    } else {
+        F.kin[i].w = filtered; F.aux[i] = make_float2(p, dev);
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Sweep A: extrapolated wall pressure
+// ------------------------------------------------------------------------------------------
+
+template <int D, int K>
+struct WallVisit {
+    static constexpr bool kSkipCoincident = false;
+    const Params &P; const Frame &F;
+    float weight, total;
+    __device__ bool accept(bool fluidJ) const { return fluidJ; }
+    __device__ void operator()(int j, const float *d, float r, float h, bool, int)
+    {
+        float w = kernelValue<K>(r / h, sigmaAt(P.sigmaUnit, h, D));
+        float gd = P.g[0] * d[0] + P.g[1] * d[1] + (D == 3 ? P.g[2] * d[2] : 0.0f);
+        weight += w;
+        total += w * (pressureOf<D>(F, j) + densityOf<D>(F, j) * gd);
+    }
+};
+
+// Boundary rows only write their own entries and only fluid entries are read, so the frame is
+// updated in place.  writeDensity: the master float64 density takes Tait^-1(p_w) too.
+template <int D, int K, int T>
+__global__ void __launch_bounds__(kBlock) wallPressureKernel(Params P, Frame F, const Control *ctl, int writeDensity)
+{
+    if (ctl && !ctl->active) return;
+    const Group<T> G = groupOf<T>();
+    const int i = G.i;
+    if (i >= P.n) return;
+    float hs = signedLength<D>(F, i);
+    if (hs > 0.0f) return;
+    WallVisit<D, K> visit{P, F, 0.0f, 0.0f};
+    forEachNeighbour<D, T>(P, F, i, G.t, -hs, visit);
+    float weight = groupSum<T>(visit.weight, G.mask), total = groupSum<T>(visit.total, G.mask);
+    if (G.t != 0) return;
+    float p = 0.0f;
+    if (weight > 0.0f) p = fmaxf(total / weight, 0.0f);
+    double rho = P.rho0 * pow(1.0 + (double)p / P.stiffness, 1.0 / 7.0);
+    float dev = (float)(rho - P.devReference);
+    F.scalar[i] = p;
+    if (D == 2) {
+        F.kin[i].w = p;
+        if (writeDensity) { F.kin[i].z = (float)rho; F.pb[i].z = dev; }
+    } else {
+        F.aux[i].x = p;
+        if (writeDensity) { F.kin[i].w = (float)rho; F.aux[i].y = dev; }
+    }
+    if (writeDensity) F.rho[i] = rho;
+}
+
+// ------------------------------------------------------------------------------------------
+// Sweep B: G, L and grad rho from one pass
+// ------------------------------------------------------------------------------------------
+
+template <int D, int K>
+struct GradientVisit {
+    static constexpr bool kSkipCoincident = true;
+    const Params &P; const Frame &F;
+    bool wantG, wantL, wantRho;
+    float vi[3], devI;
+    float S[3][3], Mf[3][3], M[3][3], gsum[3];
+    __device__ bool accept(bool) const { return true; }
+    __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int)
+    {
+        float slope = kernelSlope<K>(r / h, h, sigmaAt(P.sigmaUnit, h, D));
+        float w = massOf<D>(F, j) / densityOf<D>(F, j) * slope / r;
+        if (wantG && fluidJ) {
+            float vj[3];
+            velocityOf<D>(F, j, vj);
+            for (int a = 0; a < D; ++a)
+                for (int b = 0; b < D; ++b) {
+                    S[a][b] += w * (vj[a] - vi[a]) * d[b];
+                    Mf[a][b] += -w * d[a] * d[b];
+                }
+        }
+        if (wantL)
+            for (int a = 0; a < D; ++a)
+                for (int b = 0; b < D; ++b) M[a][b] += -w * d[a] * d[b];
+        if (wantRho) {
+            float t = w * (deviationOf<D>(F, j) - devI);
+            for (int a = 0; a < D; ++a) gsum[a] += t * d[a];
+        }
+    }
+};
+
+template <int D, int T>
+__device__ __forceinline__ void groupSumMatrix(float M[3][3], unsigned mask)
+{
+    for (int a = 0; a < D; ++a)
+        for (int b = 0; b < D; ++b) M[a][b] = groupSum<T>(M[a][b], mask);
+}
+
+template <int D, int K, int T>
+__global__ void __launch_bounds__(kBlock)
+gradientKernel(Params P, Frame F, const Control *ctl, int wantG, int wantL, int wantRho, float floorDet)
+{
+    if (ctl && !ctl->active) return;
+    const Group<T> G = groupOf<T>();
+    const int i = G.i;
+    if (i >= P.n) return;
+    float hs = signedLength<D>(F, i);
+    if (hs <= 0.0f) {
+        if (G.t != 0) return;
+        float zero[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        float ident[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+        if (wantG) storeMatrix<D>(F.G0, F.G1, F.G2, i, zero);
+        if (wantL) storeMatrix<D>(F.L0, F.L1, F.L2, i, ident);
+        if (wantRho) F.gradRho[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        return;
+    }
+    GradientVisit<D, K> visit{P, F, wantG != 0, wantL != 0 || wantRho != 0, wantRho != 0};
+    velocityOf<D>(F, i, visit.vi);
+    visit.devI = deviationOf<D>(F, i);
+    for (int a = 0; a < 3; ++a) {
+        visit.gsum[a] = 0.0f;
+        for (int b = 0; b < 3; ++b) { visit.S[a][b] = 0.0f; visit.Mf[a][b] = 0.0f; visit.M[a][b] = 0.0f; }
+    }
+    forEachNeighbour<D, T>(P, F, i, G.t, hs, visit);
+    if (wantG) { groupSumMatrix<D, T>(visit.S, G.mask); groupSumMatrix<D, T>(visit.Mf, G.mask); }
+    if (wantL || wantRho) groupSumMatrix<D, T>(visit.M, G.mask);
+    if (wantRho)
+        for (int a = 0; a < D; ++a) visit.gsum[a] = groupSum<T>(visit.gsum[a], G.mask);
+    if (G.t != 0) return;
+    if (wantG) {
+        float Gm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+        if (determinant<D>(visit.Mf) >= floorDet) {
+            float inv[3][3];
+            inverse<D>(visit.Mf, inv);
+            for (int a = 0; a < D; ++a)
+                for (int b = 0; b < D; ++b) {
+                    float t = 0.0f;
+                    for (int c = 0; c < D; ++c) t += visit.S[a][c] * inv[c][b];
+                    Gm[a][b] = t;
+                }
+        }
+        storeMatrix<D>(F.G0, F.G1, F.G2, i, Gm);
+    }
+    if (wantL || wantRho) {
+        float L[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+        if (determinant<D>(visit.M) >= floorDet) inverse<D>(visit.M, L);
+        if (wantL) storeMatrix<D>(F.L0, F.L1, F.L2, i, L);
+        if (wantRho) {
+            float g[3] = {0.0f, 0.0f, 0.0f};
+            for (int a = 0; a < D; ++a)
+                for (int b = 0; b < D; ++b) g[a] += L[a][b] * visit.gsum[b];
+            F.gradRho[i] = make_float4(g[0], g[1], g[2], 0.0f);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------------
+// Sweep C: accelerations, fluid maxima, time step
+// ------------------------------------------------------------------------------------------
+
+template <int D, int K>
+struct MomentumVisit {
+    static constexpr bool kSkipCoincident = true;
+    const Params &P; const Frame &F;
+    float vi[3], rhoI, own;
+    float Gi[3][3];
+    float total[3];
+    __device__ bool accept(bool) const { return true; }
+    __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int)
+    {
+        float vj[3];
+        velocityOf<D>(F, j, vj);
+        float rel[3] = {vi[0] - vj[0], vi[1] - vj[1], vi[2] - vj[2]};
+        float approach = rel[0] * d[0] + rel[1] * d[1] + (D == 3 ? rel[2] * d[2] : 0.0f);
+        float rhoJ = densityOf<D>(F, j);
+        float viscosity = 0.0f;
+        if (approach < 0.0f && P.limited && fluidJ) {
+            float Gj[3][3];
+            loadMatrix<D>(F.G0, F.G1, F.G2, j, Gj);
+            float rampI[3] = {0, 0, 0}, rampJ[3] = {0, 0, 0};
+            float slopeI = 0.0f, slopeJ = 0.0f;
+            for (int a = 0; a < D; ++a) {
+                for (int b = 0; b < D; ++b) { rampI[a] += Gi[a][b] * d[b]; rampJ[a] += Gj[a][b] * d[b]; }
+                slopeI += d[a] * rampI[a];
+                slopeJ += d[a] * rampJ[a];
+            }
+            float limiter = 0.0f;
+            if (slopeI * slopeJ > 0.0f) {
+                float ratio = slopeI / slopeJ;
+                limiter = fminf(1.0f, 4.0f * ratio / ((1.0f + ratio) * (1.0f + ratio)));
+                float eta = r / h;
+                if (eta < kCloseDistance) {
+                    float fade = (eta - kCloseDistance) / kFoldWidth;
+                    limiter *= expf(-fade * fade);
+                }
+            }
+            approach = 0.0f;
+            for (int a = 0; a < D; ++a) approach += (rel[a] - 0.5f * limiter * (rampI[a] + rampJ[a])) * d[a];
+        }
+        if (approach < 0.0f) {
+            float mu = h * approach / (r * r + kViscositySoftening * h * h);
+            viscosity = -P.alpha * P.c0 * mu / (0.5f * (rhoI + rhoJ));
+            if (!fluidJ) viscosity *= P.boundaryFactor;
+        }
+        float coefficient = -(own + pressureOf<D>(F, j) / (rhoJ * rhoJ) + viscosity) * massOf<D>(F, j);
+        float slope = kernelSlope<K>(r / h, h, sigmaAt(P.sigmaUnit, h, D));
+        float f = coefficient * slope / r;
+        for (int a = 0; a < D; ++a) total[a] += f * d[a];
+    }
+};
+
+__device__ __forceinline__ double blockMax(double value, double *shared)
+{
+    for (int offset = 16; offset > 0; offset >>= 1) value = fmax(value, __shfl_down_sync(0xFFFFFFFFu, value, offset));
+    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __syncthreads();
+    if (lane == 0) shared[warp] = value;
+    __syncthreads();
+    if (warp == 0) {
+        value = lane < (int)(blockDim.x >> 5) ? shared[lane] : 0.0;
+        for (int offset = 16; offset > 0; offset >>= 1) value = fmax(value, __shfl_down_sync(0xFFFFFFFFu, value, offset));
+    }
+    return value;
+}
+
+__device__ __forceinline__ double cflTimeStep(double h, double c0, double vmax, double amax, double cfl, double maxdt)
+{
+    double dt = cfl * h / (c0 + vmax);
+    if (amax > 1e-12) dt = fmin(dt, cfl * sqrt(h / amax));
+    return fmin(dt, maxdt);
+}
+
+template <int D, int K, int T>
+__global__ void __launch_bounds__(kBlock) momentumKernel(Params P, Frame F, Control *ctl, double *blockMaxima)
+{
+    __shared__ double shared[kBlock / 32];
+    __shared__ bool last;
+    if (ctl && !ctl->active) return;
+    const Group<T> G = groupOf<T>();
+    const int i = G.i;
+    double speed = 0.0, accel = 0.0;
+    if (i < P.n) {
+        float hs = signedLength<D>(F, i);
+        if (hs <= 0.0f) {
+            if (G.t == 0) F.acc[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        } else {
+            MomentumVisit<D, K> visit{P, F};
+            velocityOf<D>(F, i, visit.vi);
+            visit.rhoI = densityOf<D>(F, i);
+            visit.own = pressureOf<D>(F, i) / (visit.rhoI * visit.rhoI);
+            if (P.limited) loadMatrix<D>(F.G0, F.G1, F.G2, i, visit.Gi);
+            visit.total[0] = visit.total[1] = visit.total[2] = 0.0f;
+            forEachNeighbour<D, T>(P, F, i, G.t, hs, visit);
+            for (int a = 0; a < D; ++a) visit.total[a] = groupSum<T>(visit.total[a], G.mask);
+            if (G.t == 0) {
+                float a[3] = {visit.total[0] + P.g[0], visit.total[1] + P.g[1],
+                              D == 3 ? visit.total[2] + P.g[2] : 0.0f};
+                F.acc[i] = make_float4(a[0], a[1], a[2], 0.0f);
+                double v2 = 0.0;
+                for (int c = 0; c < D; ++c) v2 += F.v[c][i] * F.v[c][i];
+                speed = sqrt(v2);
+                accel = (double)sqrtf(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+            }
+        }
+    }
+    if (!blockMaxima) return;
+    double bs = blockMax(speed, shared);
+    double ba = blockMax(accel, shared);
+    if (threadIdx.x == 0) {
+        blockMaxima[2 * blockIdx.x] = bs;
+        blockMaxima[2 * blockIdx.x + 1] = ba;
+        __threadfence();
+        unsigned ticket = atomicAdd(&ctl->ticket, 1u);
+        last = ticket == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    // The last block reduces every block's maxima (max is order-free, so this is deterministic)
+    __threadfence();
+    double vmax = 0.0, amax = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+        vmax = fmax(vmax, ((volatile double *)blockMaxima)[2 * b]);
+        amax = fmax(amax, ((volatile double *)blockMaxima)[2 * b + 1]);
+    }
+    vmax = blockMax(vmax, shared);
+    amax = blockMax(amax, shared);
+    if (threadIdx.x == 0) {
+        ctl->vmax = vmax;
+        ctl->amax = amax;
+        ctl->ticket = 0;
+        if (!ctl->hostDt) {
+            double dt = cflTimeStep(ctl->hMin, ctl->soundSpeed, vmax, amax, ctl->cfl, ctl->maxTimeStep);
+            if (!(dt > 0.0) || !isfinite(dt)) ctl->error |= kErrTimeStep;
+            ctl->dt = dt;
+        }
+    }
+}
+
+// v += a dt on the fluid (src/pysurf/sphGpu.py:1084-1109); the frame takes the kicked velocity.
+template <int D>
+__global__ void kickKernel(Params P, Frame F, Control *ctl)
+{
+    if (!ctl->active) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n || !F.fluid[i]) return;
+    double dt = ctl->dt;
+    float4 a = F.acc[i];
+    double v[3] = {0.0, 0.0, 0.0};
+    float av[3] = {a.x, a.y, a.z};
+    for (int c = 0; c < D; ++c) {
+        v[c] = F.v[c][i] + (double)av[c] * dt;
+        F.v[c][i] = v[c];
+    }
+    float4 k = F.kin[i];
+    k.x = (float)v[0]; k.y = (float)v[1];
+    if (D == 3) k.z = (float)v[2];
+    F.kin[i] = k;
+}
+
+// Drift (src/pysurf/sphGpu.py:1142-1186), the periodic wrap and the enforcement of one fluid slot.
+template <int D>
+__device__ __forceinline__ void driftAndEnforce(const Params &P, const Frame &F, const Enforcement &E, int i, double dt,
+                                                const double *transport, Control *ctl)
+{
+    double x[3] = {0.0, 0.0, 0.0}, v[3] = {0.0, 0.0, 0.0};
+    for (int a = 0; a < D; ++a) {
+        v[a] = F.v[a][i];
+        x[a] = F.x[a][i] + (transport ? transport[a] : v[a]) * dt;
+    }
+    if (P.period > 0.0) x[1] = x[1] - P.period * floor(x[1] / P.period);
+    enforceOne(E, D, x, v);
+    bool finite = true;
+    for (int a = 0; a < D; ++a) {
+        F.x[a][i] = x[a];
+        F.v[a][i] = v[a];
+        finite = finite && isfinite(x[a]) && isfinite(v[a]);
+    }
+    if (!finite) atomicOr(&ctl->error, kErrNonFinite);
+}
+
+// ------------------------------------------------------------------------------------------
+// Sweep D: continuity with the density update, drift and enforcement
+// ------------------------------------------------------------------------------------------
+
+template <int D, int K>
+struct ContinuityVisit {
+    static constexpr bool kSkipCoincident = true;
+    const Params &P; const Frame &F;
+    bool boundaryI, diffuses, corrected;
+    float vi[3], devI, Li[3][3], gi[3];
+    float total;
+    __device__ bool accept(bool fluidJ) const { return !(boundaryI && !fluidJ); }
+    __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int)
+    {
+        float slope = kernelSlope<K>(r / h, h, sigmaAt(P.sigmaUnit, h, D));
+        float vj[3];
+        velocityOf<D>(F, j, vj);
+        float mj = massOf<D>(F, j);
+        float dot = 0.0f;
+        if (corrected) {
+            for (int a = 0; a < D; ++a) {
+                float ld = 0.0f;
+                for (int b = 0; b < D; ++b) ld += Li[a][b] * d[b];
+                dot += (vi[a] - vj[a]) * ld;
+            }
+        } else {
+            for (int a = 0; a < D; ++a) dot += (vi[a] - vj[a]) * d[a];
+        }
+        total += mj * dot * slope / r;
+        if (diffuses && fluidJ) {
+            float devJ = deviationOf<D>(F, j);
+            float difference = devJ - devI;
+            if (P.diffusion == 2) {
+                float ratio = 1.0f + 0.5f * (devI + devJ) / P.rho0F;
+                float sq = ratio * ratio;
+                difference -= P.rho0F * P.gravityOverSound * d[D - 1] / (sq * sq * ratio);
+            } else if (P.diffusion == 3) {
+                float4 gj = __ldg(&F.gradRho[j]);
+                float gjv[3] = {gj.x, gj.y, gj.z};
+                float t = 0.0f;
+                for (int a = 0; a < D; ++a) t += (gi[a] + gjv[a]) * d[a];
+                difference += 0.5f * t;
+            }
+            total += P.diffusionFactor * h * mj / densityOf<D>(F, j) * difference * (-slope * r)
+                   / (r * r + kViscositySoftening * h * h);
+        }
+    }
+};
+
+// mode 0: the rate only; 1: advance the density; 2: advance, drift and enforce.
+template <int D, int K, int T>
+__global__ void __launch_bounds__(kBlock) continuityKernel(Params P, Frame F, Control *ctl, Enforcement E, int mode)
+{
+    if (ctl && !ctl->active) return;
+    const Group<T> G = groupOf<T>();
+    const int i = G.i;
+    if (i >= P.n) return;
+    float hs = signedLength<D>(F, i);
+    ContinuityVisit<D, K> visit{P, F};
+    visit.boundaryI = hs <= 0.0f;
+    visit.diffuses = P.diffusion != 0 && !visit.boundaryI;
+    visit.corrected = P.corrected && !visit.boundaryI;
+    velocityOf<D>(F, i, visit.vi);
+    visit.devI = deviationOf<D>(F, i);
+    if (visit.corrected) loadMatrix<D>(F.L0, F.L1, F.L2, i, visit.Li);
+    visit.gi[0] = visit.gi[1] = visit.gi[2] = 0.0f;
+    if (visit.diffuses && P.diffusion == 3) {
+        float4 g = F.gradRho[i];
+        visit.gi[0] = g.x; visit.gi[1] = g.y; visit.gi[2] = g.z;
+    }
+    visit.total = 0.0f;
+    forEachNeighbour<D, T>(P, F, i, G.t, fabsf(hs), visit);
+    const float rate = groupSum<T>(visit.total, G.mask);
+    if (G.t != 0) return;
+    F.rate[i] = rate;
+    if (mode == 0) return;
+    double dt = ctl->dt;
+    double rho = F.rho[i] + (double)rate * dt;
+    bool fluid = hs > 0.0f;
+    if (P.densityFloor > 0.0 && fluid) rho = fmax(rho, P.densityFloor);
+    F.rho[i] = rho;
+    if (!isfinite(rho)) atomicOr(&ctl->error, kErrNonFinite);
+    if (mode == 2 && fluid) driftAndEnforce<D>(P, F, E, i, dt, nullptr, ctl);
+}
+
+// ------------------------------------------------------------------------------------------
+// Sweep X: XSPH over fluid pairs, with the densities the step has just advanced
+// ------------------------------------------------------------------------------------------
+
+template <int D, int K>
+struct XsphVisit {
+    static constexpr bool kSkipCoincident = false;
+    const Params &P; const Frame &F; const float *densities;
+    float vi[3], rhoI, corr[3];
+    __device__ bool accept(bool fluidJ) const { return fluidJ; }
+    __device__ void operator()(int j, const float *, float r, float h, bool, int)
+    {
+        float w = kernelValue<K>(r / h, sigmaAt(P.sigmaUnit, h, D));
+        float rhoJ = densities ? densities[j] : densityOf<D>(F, j);
+        float weight = massOf<D>(F, j) * w / (0.5f * (rhoI + rhoJ));
+        float vj[3];
+        velocityOf<D>(F, j, vj);
+        for (int a = 0; a < D; ++a) corr[a] += weight * (vj[a] - vi[a]);
+    }
+};
+
+// densities: the float32 densities the sum divides by (null: the frame's).  mode 0: the transport
+// velocity into F.vec only; 2: drift with it and enforce.
+template <int D, int K, int T>
+__global__ void __launch_bounds__(kBlock)
+xsphKernel(Params P, Frame F, Control *ctl, Enforcement E, const float *densities, int mode)
+{
+    if (ctl && !ctl->active) return;
+    const Group<T> G = groupOf<T>();
+    const int i = G.i;
+    if (i >= P.n) return;
+    float hs = signedLength<D>(F, i);
+    float v[3];
+    velocityOf<D>(F, i, v);
+    if (hs <= 0.0f) {
+        if (G.t == 0) F.vec[i] = make_float4(v[0], v[1], v[2], 0.0f);
+        return;
+    }
+    XsphVisit<D, K> visit{P, F, densities};
+    visit.vi[0] = v[0]; visit.vi[1] = v[1]; visit.vi[2] = v[2];
+    visit.rhoI = densities ? densities[i] : densityOf<D>(F, i);
+    visit.corr[0] = visit.corr[1] = visit.corr[2] = 0.0f;
+    forEachNeighbour<D, T>(P, F, i, G.t, hs, visit);
+    for (int a = 0; a < D; ++a) visit.corr[a] = groupSum<T>(visit.corr[a], G.mask);
+    if (G.t != 0) return;
+    float t[3];
+    for (int a = 0; a < 3; ++a) t[a] = v[a] + P.xsphEpsilon * visit.corr[a];
+    F.vec[i] = make_float4(t[0], t[1], t[2], 0.0f);
+    if (mode != 2) return;
+    double transport[3] = {(double)t[0], (double)t[1], (double)t[2]};
+    driftAndEnforce<D>(P, F, E, i, ctl->dt, transport, ctl);
+}
+
+// ------------------------------------------------------------------------------------------
+// Launchers
+// ------------------------------------------------------------------------------------------
+
+static inline int blocksFor(long long n, int block) { return (int)((n + block - 1) / block); }
+
+template <int D, int K, int T>
+static void launchT(const LaunchArgs &A, Stage stage)
+{
+    const Params &P = A.P;
+    const Frame &F = A.F;
+    const int grid = blocksFor((long long)P.n * T, kBlock), pointwise = blocksFor(P.n, kBlock);
+    if (P.n == 0) return;
+    cudaStream_t st = A.stream;
+    switch (stage) {
+    case Stage::ShepardSum: shepardKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl); break;
+    case Stage::ShepardApply: applyShepardKernel<D><<<pointwise, kBlock, 0, st>>>(P, F, A.ctl); break;
+    case Stage::Wall: wallPressureKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.flag); break;
+    case Stage::Gradients:
+        gradientKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.wantG, A.wantL, A.wantRho, A.floorDet);
+        break;
+    case Stage::Momentum: momentumKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.blockMaxima); break;
+    case Stage::Kick: kickKernel<D><<<pointwise, kBlock, 0, st>>>(P, F, A.ctl); break;
+    case Stage::Continuity: continuityKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.flag); break;
+    case Stage::Xsph: xsphKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.densities, A.flag); break;
+    case Stage::List:
+        if (D == 2) listKernel<2><<<pointwise, kBlock, 0, st>>>(P, F, A.ctl, A.maxCount);
+        else listKernel<3><<<pointwise, kBlock, 0, st>>>(P, F, A.ctl, A.maxCount);
+        break;
+    }
+}
+
+template <int D, int K>
+static void launchDK(const LaunchArgs &A, Stage stage)
+{
+    if (A.threads >= 4) launchT<D, K, 4>(A, stage);
+    else if (A.threads == 2) launchT<D, K, 2>(A, stage);
+    else launchT<D, K, 1>(A, stage);
+}
+
+void launchStage(const LaunchArgs &A, Stage stage)
+{
+    const int D = A.P.dim, K = A.P.kind;
+    if (D == 2 && K == 0) launchDK<2, 0>(A, stage);
+    else if (D == 2 && K == 1) launchDK<2, 1>(A, stage);
+    else if (D == 3 && K == 0) launchDK<3, 0>(A, stage);
+    else launchDK<3, 1>(A, stage);
+}
+
+}  // namespace sph

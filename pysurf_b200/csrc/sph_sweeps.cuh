@@ -1,105 +1,218 @@
-// sph_sweeps.cuh -- the neighbour walk every sweep shares.
+// sph_sweeps.cuh -- the neighbour walk every sweep shares, and its neighbour table.
 //
-// One thread per sorted particle.  A particle's neighbours lie in the cells within +-ncs of its
-// own along each axis; cells are numbered x fastest, so each (y, z) row of the stencil is one
-// contiguous run of the sorted order, [cellStart[first], cellStart[last + 1]).  Threads of a
-// warp hold neighbouring particles of the same few cells, walk the same runs in step, and read
-// the same neighbour records, which the L1 cache serves to all of them at once.
+// A particle's neighbours lie in the cells within +-ncs of its own along each axis; cells are
+// numbered x fastest, so each (y, z) row of the stencil is one contiguous run of the sorted
+// order, [cellStart[first], cellStart[last + 1]).  Candidates are tested on their float32 points
+// first (the reference's coarse test, src/pysurf/sphGpu.py:330-336), and only survivors take the
+// precise separation (hi_i - hi_j) + (lo_i - lo_j).
 //
-// Candidates are tested on their float32 points first (the reference's coarse test,
-// src/pysurf/sphGpu.py:330-336), and only survivors take the precise separation
-// (hi_i - hi_j) + (lo_i - lo_j).
+// Each step the table kernel walks the cells once and records, per particle, the neighbours the
+// walk accepts, in the walk's order, in a column-major table (entry k of particle i at
+// k * stride + i, so a warp's reads of entry k are contiguous).  The sweeps then read the table
+// instead of walking the cells: no candidate that fails the distance test is visited again, so
+// a warp's lanes stay busy.  A particle with more neighbours than its row holds walks the cells
+// instead.  Table and walk feed one loop body, the visitor called from one place, so a sweep
+// gives the same bits either way.
+//
+// T threads serve one particle: lane t of the group takes the particle's neighbours t, t + T,
+// t + 2T, ... (counted in the walk's order), and the group sums its partial sums with a
+// butterfly of shuffles, which gives every lane the same bits (each level adds two values whose
+// order does not matter).  T = 1 is the plain one-thread-per-particle sweep.
 //
 // A periodic y axis (3D) is searched a second time from the particle's image across the seam
-// when it lies within its reach of the seam (src/pysurf/sphGpu.py:206-225).  Each walk tests its
-// candidates against its own origin (the particle, or its image), and a period longer than twice
+// when it lies within its reach of the seam (src/pysurf/sphGpu.py:206-225).  Each search tests
+// its candidates against its own origin (the particle, or its image); a period longer than twice
 // the reach (the solver requires twice the support, src/pysurf/sphSolver.py:1465-1467) keeps any
 // neighbour from passing both tests.  Pairs across the seam take their separation in float64:
 // their points are a period apart and their float32 difference would lose the digits the split
-// keeps.
+// keeps.  The table marks such pairs in the entry's top bit.
 #pragma once
 
 #include "sph_internal.cuh"
 
 namespace sph {
 
-// Walk the neighbours of slot i.  The visitor gets (j, d[3], r, h_ij, fluidJ) for every j != i
-// with r < 2 h_ij, and r >= 1e-12 when Visitor::kSkipCoincident.  Visitor::accept(fluidJ) is
-// asked first and may skip a neighbour before its separation is taken.
-template <int D, class Visitor>
-__device__ __forceinline__ void walkNeighbours(const Params &P, const Frame &F, int i, float hI, Visitor &visit)
+// The lanes of a group of T threads that serve one particle.
+template <int T>
+struct Group {
+    int i;              // the particle (sorted slot)
+    int t;              // this thread's lane in the group
+    unsigned mask;      // the group's lanes in the warp
+};
+
+template <int T>
+__device__ __forceinline__ Group<T> groupOf()
+{
+    const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    Group<T> G;
+    G.i = (int)(g / T);
+    G.t = (int)(g % T);
+    const int lane = threadIdx.x & 31;
+    G.mask = T >= 32 ? 0xFFFFFFFFu : (((1u << T) - 1u) << (lane & ~(T - 1)));
+    return G;
+}
+
+// The group's sum, the same bits on every lane.
+template <int T>
+__device__ __forceinline__ float groupSum(float value, unsigned mask)
+{
+    for (int offset = T / 2; offset > 0; offset >>= 1) value += __shfl_xor_sync(mask, value, offset, T);
+    return value;
+}
+
+// The candidates of slot i, one at a time: its table row when the row holds them all, else the
+// cells of its stencil (then twice for an image search across a periodic seam).
+template <int D>
+struct Candidates {
+    // table
+    const int *column;
+    int stride, count, k, step;
+    // walk
+    bool walking;
+    int images, image, cyImage, cy, ncs, nx, ny, x0, x1, z0, z1, zz, yy, j, end;
+    const int *cellStart;
+
+    __device__ __forceinline__ void startRow()
+    {
+        const int row = (zz * ny + yy) * nx;
+        j = __ldg(&cellStart[row + x0]) - 1;
+        end = __ldg(&cellStart[row + x1 + 1]);
+    }
+
+    __device__ __forceinline__ void startImage()
+    {
+        const int yc = image == 0 ? cy : cyImage;
+        yy = max(yc - ncs, 0);
+        zz = z0;
+        startRow();
+    }
+
+    // The next candidate into (jOut, imageOut); false when there are none left.
+    __device__ __forceinline__ bool next(int &jOut, int &imageOut)
+    {
+        if (!walking) {
+            if (k >= count) return false;
+            const int entry = __ldg(column + (size_t)k * stride);
+            k += step;
+            jOut = entry & 0x7FFFFFFF;
+            imageOut = entry < 0 ? 1 : 0;
+            return true;
+        }
+        while (true) {
+            if (++j < end) {
+                jOut = j;
+                imageOut = image;
+                return true;
+            }
+            const int yc = image == 0 ? cy : cyImage;
+            if (yy < min(yc + ncs, ny - 1)) {
+                ++yy;
+            } else if (zz < z1) {
+                ++zz;
+                yy = max(yc - ncs, 0);
+            } else if (++image < images) {
+                startImage();
+                continue;
+            } else {
+                return false;
+            }
+            startRow();
+        }
+    }
+};
+
+// Visit the neighbours of slot i.  Every neighbour j != i with r < 2 h_ij (the table's criterion)
+// is counted in the walk's order; lane t of T takes those whose count is t mod T (the table row
+// of a lane is read with step T from entry t).  Of those, the visitor gets (j, d, r, h_ij, fluidJ,
+// image) when Visitor::accept(fluidJ), and r >= 1e-12 where Visitor::kSkipCoincident.
+// useTable: false forces the walk (the table kernel itself).
+template <int D, int T, class Visitor>
+__device__ __forceinline__ void forEachNeighbour(const Params &P, const Frame &F, int i, int t, float hI,
+                                                 Visitor &visit, bool useTable = true)
 {
     float pi[3], li[3];
     pointOf<D>(F, i, pi);
     remainderOf<D>(F, i, li);
     const float reach = P.mixedH ? hI + P.hMax : 2.0f * P.hMax;
     const float limit = kCandidateMargin * reach * reach;
-    const int nx = P.nc[0], ny = P.nc[1], nz = P.nc[2];
-    const int c = F.cell[i];
-    const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
-    const int ncs = P.ncs;
-    const int x0 = max(cx - ncs, 0), x1 = min(cx + ncs, nx - 1);
-    const int z0 = D == 3 ? max(cz - ncs, 0) : 0, z1 = D == 3 ? min(cz + ncs, nz - 1) : 0;
-
-    // image search: the particle's image across the periodic seam, if within reach of it
-    int images = 1;
-    float shift = 0.0f;
     double shift64 = 0.0;
-    int cyImage = cy;
-    if (D == 3 && P.period > 0.0) {
-        if (pi[1] < reach || pi[1] > P.periodF - reach) {
-            images = 2;
-            shift64 = pi[1] < 0.5f * P.periodF ? P.period : -P.period;
-            shift = (float)shift64;
-            double y = (double)pi[1] + (double)li[1] + shift64;
-            cyImage = cellCoordinate(y, P.origin[1], P.cellWidth, ny);
-        }
+    bool seam = false;
+    if (D == 3 && P.period > 0.0 && (pi[1] < reach || pi[1] > P.periodF - reach)) {
+        seam = true;
+        shift64 = pi[1] < 0.5f * P.periodF ? P.period : -P.period;
     }
 
-    for (int image = 0; image < images; ++image) {
-        const int yc = image == 0 ? cy : cyImage;
-        const float offset = image == 0 ? 0.0f : shift;     // the walk's origin: the particle, or its image
-        const int y0 = max(yc - ncs, 0), y1 = min(yc + ncs, ny - 1);
-        for (int zz = z0; zz <= z1; ++zz) {
-            for (int yy = y0; yy <= y1; ++yy) {
-                const int row = (zz * ny + yy) * nx;
-                const int begin = __ldg(&F.cellStart[row + x0]);
-                const int end = __ldg(&F.cellStart[row + x1 + 1]);
-                for (int j = begin; j < end; ++j) {
-                    float pj[3];
-                    pointOf<D>(F, j, pj);
-                    float cxv = pi[0] - pj[0];
-                    float cyv = (pi[1] + offset) - pj[1];
-                    float czv = D == 3 ? pi[2] - pj[2] : 0.0f;
-                    float coarse = cxv * cxv + cyv * cyv + czv * czv;
-                    if (coarse >= limit || j == i) continue;
-                    const float hs = signedLength<D>(F, j);
-                    const bool fluidJ = hs > 0.0f;
-                    if (!visit.accept(fluidJ)) continue;
-                    float lj[3];
-                    remainderOf<D>(F, j, lj);
-                    float d[3];
-                    if (!P.precise) {
-                        // separationPrecision 'float32': the points alone (src/pysurf/sphGpu.py:227-242)
-                        d[0] = cxv; d[1] = cyv; d[2] = czv;
-                    } else if (image == 0) {
-                        d[0] = (pi[0] - pj[0]) + (li[0] - lj[0]);
-                        d[1] = (pi[1] - pj[1]) + (li[1] - lj[1]);
-                        d[2] = D == 3 ? (pi[2] - pj[2]) + (li[2] - lj[2]) : 0.0f;
-                    } else {
-                        for (int a = 0; a < D; ++a)
-                            d[a] = (float)(((double)pi[a] + (double)li[a]) - ((double)pj[a] + (double)lj[a]));
-                        d[1] = (float)((((double)pi[1] + (double)li[1]) + shift64) - ((double)pj[1] + (double)lj[1]));
-                    }
-                    const float r2 = d[0] * d[0] + d[1] * d[1] + (D == 3 ? d[2] * d[2] : 0.0f);
-                    const float r = sqrtf(r2);
-                    const float h = P.mixedH ? 0.5f * (hI + fabsf(hs)) : P.hMax;
-                    if (r >= 2.0f * h) continue;
-                    if (Visitor::kSkipCoincident && r < 1.0e-12f) continue;
-                    visit(j, d, r, h, fluidJ);
-                }
+    Candidates<D> C;
+    const int count = useTable && P.listCap > 0 ? __ldg(&F.ncount[i]) : 0;
+    C.walking = !(useTable && P.listCap > 0 && count <= P.listCap);
+    if (!C.walking) {
+        C.column = F.nbr + i;
+        C.stride = P.listStride;
+        C.count = count;
+        C.k = t;
+        C.step = T;
+    } else {
+        C.nx = P.nc[0];
+        C.ny = P.nc[1];
+        const int c = F.cell[i];
+        const int cx = c % C.nx, cz = c / (C.nx * C.ny);
+        C.cy = (c / C.nx) % C.ny;
+        C.ncs = P.ncs;
+        C.x0 = max(cx - C.ncs, 0);
+        C.x1 = min(cx + C.ncs, C.nx - 1);
+        C.z0 = D == 3 ? max(cz - C.ncs, 0) : 0;
+        C.z1 = D == 3 ? min(cz + C.ncs, P.nc[2] - 1) : 0;
+        C.cellStart = F.cellStart;
+        C.images = seam ? 2 : 1;
+        C.cyImage = seam ? cellCoordinate((double)pi[1] + (double)li[1] + shift64, P.origin[1], P.cellWidth, C.ny)
+                         : C.cy;
+        C.image = 0;
+        C.startImage();
+    }
+
+    int counted = 0, j = 0, image = 0;
+    while (C.next(j, image)) {
+        const float offset = image ? (float)shift64 : 0.0f;     // the search's origin: particle or image
+        float pj[3];
+        pointOf<D>(F, j, pj);
+        if (C.walking) {
+            const float cxv = pi[0] - pj[0];
+            const float cyv = (pi[1] + offset) - pj[1];
+            const float czv = D == 3 ? pi[2] - pj[2] : 0.0f;
+            if (cxv * cxv + cyv * cyv + czv * czv >= limit || j == i) continue;
+        }
+        const float hs = signedLength<D>(F, j);
+        const bool fluidJ = hs > 0.0f;
+        // a lone lane may skip a rejected neighbour before its separation; a group counts every one
+        if ((T == 1 || !C.walking) && !visit.accept(fluidJ)) continue;
+        float lj[3];
+        remainderOf<D>(F, j, lj);
+        float d[3];
+        if (!P.precise) {
+            // separationPrecision 'float32': the points alone (src/pysurf/sphGpu.py:227-242)
+            d[0] = pi[0] - pj[0];
+            d[1] = (pi[1] + offset) - pj[1];
+            d[2] = D == 3 ? pi[2] - pj[2] : 0.0f;
+        } else if (!image) {
+            d[0] = (pi[0] - pj[0]) + (li[0] - lj[0]);
+            d[1] = (pi[1] - pj[1]) + (li[1] - lj[1]);
+            d[2] = D == 3 ? (pi[2] - pj[2]) + (li[2] - lj[2]) : 0.0f;
+        } else {
+            for (int a = 0; a < D; ++a)
+                d[a] = (float)(((double)pi[a] + (double)li[a]) - ((double)pj[a] + (double)lj[a]));
+            d[1] = (float)((((double)pi[1] + (double)li[1]) + shift64) - ((double)pj[1] + (double)lj[1]));
+        }
+        const float r = sqrtf(d[0] * d[0] + d[1] * d[1] + (D == 3 ? d[2] * d[2] : 0.0f));
+        const float h = P.mixedH ? 0.5f * (hI + fabsf(hs)) : P.hMax;
+        if (C.walking) {
+            if (r >= 2.0f * h) continue;
+            if (T > 1) {
+                if (counted++ % T != t) continue;
+                if (!visit.accept(fluidJ)) continue;
             }
         }
+        if (Visitor::kSkipCoincident && r < 1.0e-12f) continue;
+        visit(j, d, r, h, fluidJ, image);
     }
 }
 

@@ -134,6 +134,13 @@ struct SphSystem {
     uint8_t *dStageU8 = nullptr;
     int *dRank = nullptr;
     Control *hCtl = nullptr;    // pinned
+    // the neighbour table: listCap entries a slot (0: the sweeps walk the cells), stride capacity
+    int *nbr = nullptr, *ncount = nullptr, *dMaxCount = nullptr;
+    size_t nbrEntries = 0;
+    int listCap = 0;
+    int tableMode = 1;          // 0 never build the table, 1 build it when it fits the budget
+    bool listDirty = true;      // the table's size must be taken again before the next step
+    int threads = 1;            // threads per particle in the sweeps
     int cellStartCapacity = 0;
     // execution
     cudaStream_t stream = nullptr;
@@ -163,8 +170,12 @@ struct SphSystem {
             keys[b] = nullptr; vals[b] = nullptr;
         }
         void *ptrs[] = {pa, pb, kin, G[0], G[1], G[2], L[0], L[1], L[2], gradRho, acc, vec, aux, rate, scalar, cell,
-                        counts, blockMaxima, dStage, dStageU8, dRank};
+                        counts, blockMaxima, dStage, dStageU8, dRank, nbr, ncount};
         for (void *p : ptrs) cudaFree(p);
+        nbr = ncount = nullptr;
+        nbrEntries = 0;
+        listCap = 0;
+        listDirty = true;
         pa = pb = kin = gradRho = acc = vec = nullptr;
         for (int a = 0; a < 3; ++a) G[a] = L[a] = nullptr;
         aux = nullptr; rate = scalar = nullptr; cell = nullptr; counts = nullptr; blockMaxima = nullptr;
@@ -234,10 +245,12 @@ struct SphSystem {
         TRY(deviceAlloc(&cell, cap));
         for (int b = 0; b < 2; ++b) { TRY(deviceAlloc(&keys[b], cap)); TRY(deviceAlloc(&vals[b], cap)); }
         TRY(deviceAlloc(&counts, (size_t)256 * radixBlocks(cap)));
-        TRY(deviceAlloc(&blockMaxima, (size_t)2 * ((cap + kBlock - 1) / kBlock)));
+        // one (speed, acceleration) pair per block of the momentum sweep, at up to 4 threads a particle
+        TRY(deviceAlloc(&blockMaxima, (size_t)2 * ((4ll * cap + kBlock - 1) / kBlock)));
         TRY(deviceAlloc(&dStage, (size_t)kStageSlots * cap));
         TRY(deviceAlloc(&dStageU8, cap));
         TRY(deviceAlloc(&dRank, cap));
+        TRY(deviceAlloc(&ncount, cap));
         CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(float4) * cap, stream));
         CUDA_TRY(cudaMemsetAsync(kin, 0, sizeof(float4) * cap, stream));
         CUDA_TRY(cudaMemsetAsync(aux, 0, sizeof(float2) * cap, stream));
@@ -290,7 +303,8 @@ struct SphSystem {
             for (int a = 0; a < 3; ++a) cells[a] = std::max((long long)(cells[a] * 0.8), 1ll);
         for (int a = 0; a < 3; ++a) gridShape[a] = cells[a];
         graphDirty = true;
-        framed = false;
+        cellsFresh = false;
+        listDirty = true;
         return SPH_OK;
     }
 
@@ -328,6 +342,8 @@ struct SphSystem {
         P.limited = limited;
         P.wallExtrapolated = wallExtrapolated;
         P.xsphEpsilon = (float)xsphEpsilon;
+        P.listCap = listCap;
+        P.listStride = capacity;
         return P;
     }
 
@@ -339,6 +355,7 @@ struct SphSystem {
         F.G0 = G[0]; F.G1 = G[1]; F.G2 = G[2];
         F.L0 = L[0]; F.L1 = L[1]; F.L2 = L[2];
         F.gradRho = gradRho; F.acc = acc; F.rate = rate; F.scalar = scalar; F.vec = vec;
+        F.nbr = nbr; F.ncount = ncount;
         const MasterView &M = master[cur];
         for (int a = 0; a < 3; ++a) { F.x[a] = M.x[a]; F.v[a] = M.v[a]; }
         F.rho = M.rho; F.m = M.m; F.h = M.h; F.fluid = M.fluid; F.orig = M.orig;
@@ -355,6 +372,7 @@ struct SphSystem {
         A.blockMaxima = control ? blockMaxima : nullptr;
         A.E = enforcement;
         A.floorDet = (float)pow(0.25, dim);
+        A.threads = threads;
         return A;
     }
 
@@ -384,6 +402,57 @@ struct SphSystem {
         cur = next;
         framed = true;
         cellsFresh = true;
+        if (listCap > 0) {
+            LaunchArgs A = args(const_cast<Control *>(control));
+            launchStage(A, Stage::List);
+        }
+    }
+
+    // Take the neighbour table's size from the current cell list: the largest count now, with room
+    // to grow by a quarter, if it fits in half the free device memory; otherwise no table.  Syncs.
+    int sizeList()
+    {
+        listDirty = false;
+        if (n == 0 || tableMode == 0) {
+            if (listCap) graphDirty = true;
+            listCap = 0;
+            return SPH_OK;
+        }
+        if (!cellsFresh) rebuild();
+        if (!dMaxCount) TRY(deviceAlloc(&dMaxCount, 1));
+        CUDA_TRY(cudaMemsetAsync(dMaxCount, 0, sizeof(int), stream));
+        const int keep = listCap;
+        listCap = 0;    // count only
+        LaunchArgs A = args(nullptr);
+        A.maxCount = dMaxCount;
+        launchStage(A, Stage::List);
+        int most = 0;
+        CUDA_TRY(cudaMemcpyAsync(&most, dMaxCount, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        int cap = ((most + most / 4 + 8) + 7) & ~7;
+        size_t entries = (size_t)cap * (size_t)capacity;
+        if (entries > nbrEntries) {
+            size_t freeBytes = 0, totalBytes = 0;
+            cudaMemGetInfo(&freeBytes, &totalBytes);
+            cudaFree(nbr);
+            nbr = nullptr;
+            nbrEntries = 0;
+            if (entries * sizeof(int) > freeBytes / 2 || deviceAlloc(&nbr, entries) != SPH_OK) {
+                nbr = nullptr;
+                cap = 0;
+                cudaGetLastError();
+            } else {
+                nbrEntries = entries;
+            }
+        }
+        listCap = cap;
+        if (listCap != keep) graphDirty = true;
+        if (listCap > 0) {
+            A = args(nullptr);
+            launchStage(A, Stage::List);
+        }
+        CUDA_TRY(cudaGetLastError());
+        return SPH_OK;
     }
 
     // ---- staging -------------------------------------------------------------------------------
@@ -501,6 +570,7 @@ int sph_destroy(SphSystem *sys)
     }
     sys->freeArrays();
     cudaFree(sys->cellStart);
+    cudaFree(sys->dMaxCount);
     cudaFree(sys->ctl);
     cudaFree(sys->bedX);
     cudaFree(sys->bedZ);
@@ -526,6 +596,27 @@ int sph_set_cells_per_support(SphSystem *sys, int cells)
     if (cells < 1 || cells > 4) return fail(SPH_ERR_INVALID, "cells per support must be 1 to 4");
     sys->ncs = cells;
     return sys->setupGrid();
+}
+
+int sph_set_sweep_options(SphSystem *sys, int neighbor_table, int threads_per_particle)
+{
+    CHECK_SYS(sys);
+    if (neighbor_table != 0 && neighbor_table != 1) return fail(SPH_ERR_INVALID, "neighbor_table must be 0 or 1");
+    if (threads_per_particle != 1 && threads_per_particle != 2 && threads_per_particle != 4)
+        return fail(SPH_ERR_INVALID, "threads per particle must be 1, 2 or 4");
+    sys->tableMode = neighbor_table;
+    sys->threads = threads_per_particle;
+    sys->listDirty = true;
+    sys->graphDirty = true;
+    if (neighbor_table == 0 && sys->listCap) sys->listCap = 0;
+    return SPH_OK;
+}
+
+int sph_neighbor_table(const SphSystem *sys, int64_t *row_capacity)
+{
+    if (!sys || !row_capacity) return fail(SPH_ERR_INVALID, "null argument");
+    *row_capacity = sys->listCap;
+    return SPH_OK;
 }
 
 int sph_set_stream(SphSystem *sys, void *stream)
@@ -662,6 +753,7 @@ int sph_update(SphSystem *sys, int64_t n, const double *positions, const double 
     TRY(loadState(sys, n, positions, nullptr, nullptr, masses, is_fluid, lengths));
     sys->resident = false;
     sys->rebuild();
+    if (sys->listDirty) TRY(sys->sizeList());
     CUDA_TRY(cudaGetLastError());
     return SPH_OK;
 }
@@ -846,6 +938,7 @@ int sph_push(SphSystem *sys, int64_t n, const double *positions, const double *v
     sys->resident = true;
     // the frame follows at the first step; make the cell list now so host-step calls work too
     sys->rebuild();
+    TRY(sys->sizeList());
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(sys->stream));
     return SPH_OK;
@@ -1084,6 +1177,7 @@ int sph_resident_rates(SphSystem *sys, int filter_density, double *max_speed, do
         if (max_acceleration) *max_acceleration = 0.0;
         return SPH_OK;
     }
+    if (sys->listDirty) TRY(sys->sizeList());
     TRY(sys->writeControl());
     enqueueRates(sys, filter_density != 0);
     CUDA_TRY(cudaGetLastError());
@@ -1169,6 +1263,8 @@ int sph_begin_steps(SphSystem *sys, double time, int64_t step, double last_dt, d
     c.error = 0;
     c.active = (time < until_time && step < max_step) ? 1 : 0;
     c.dt = last_dt;
+    // sizing the table may re-sort (moving the master), so it comes before the buffer is noted
+    if (sys->listDirty) TRY(sys->sizeList());
     sys->beginStep = step;
     sys->beginCur = sys->cur;
     sys->enqueued = 0;
@@ -1402,6 +1498,7 @@ int sph_split(SphSystem *sys, const uint8_t *mask, double reference_density, dou
     sys->mixedH = mixed;
     sys->framed = false;
     sys->graphDirty = true;
+    sys->listDirty = true;
     *split = count;
     return SPH_OK;
 }

@@ -224,6 +224,12 @@ class PairSums:
         """Cells per kernel support of the device's cell list (1: 2h wide; 2: h wide)."""
         check(self._lib.sph_set_cells_per_support(self._handle, int(cells)))
 
+    def setSweepOptions(self, neighborTable: bool = True, threadsPerParticle: int = 1) -> None:
+        """Whether the sweeps read a per-step neighbour table (else they walk the cells; the sums are
+        the same bits either way), and how many threads (1, 2, 4) share each particle's neighbours."""
+        check(self._lib.sph_set_sweep_options(self._handle, int(bool(neighborTable)), int(threadsPerParticle)),
+              'setSweepOptions')
+
     # -- host steps (src/pysurf/sphGpu.py:1998-2113) -- #
     def _vectors(self, values) -> np.ndarray:
         return f64(values, (self.count, self.dimensions))
@@ -472,6 +478,12 @@ class PairSums:
                                     float(untilTime), int(maxStep), float(shortestLength), float(cflNumber),
                                     float(maxTimeStep), int(filterInterval)), 'advance')
         return float(t.value), int(s.value), float(dt.value)
+
+    def neighborTableCapacity(self) -> int:
+        """The neighbour table's row capacity now; 0 when the sweeps walk the cells."""
+        cap = _lib.C.c_int64(0)
+        check(self._lib.sph_neighbor_table(self._handle, _lib.C.byref(cap)))
+        return int(cap.value)
 
     def setStream(self, stream) -> None:
         """The CUDA stream (a cudaStream_t as an int, e.g. torch.cuda.Stream().cuda_stream) the work goes on."""

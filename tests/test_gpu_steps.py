@@ -43,8 +43,9 @@ def caseFromRun(r) -> cases.Case:
                       densityFilterInterval=int(interval), period=period)
 
 
-def deviceRun(case, steps, cellsPerSupport=None):
+def deviceRun(case, steps, cellsPerSupport=None, table=True, threads=1):
     sums = cases.pairSumsFor(case, cellsPerSupport)
+    sums.setSweepOptions(table, threads)
     state = case.state.copy()
     sums.push(state)
     sums.setBoundary(case.boundary, state)
@@ -225,3 +226,50 @@ def test_a_split_beach_steps_like_the_oracle():
     assert time == pytest.approx(stepper.time, rel=1e-4)
     assert np.abs(out['positions'] - ref['positions']).max() < 1e-6
     assert np.abs(out['velocities'] - ref['velocities']).max() < 1e-3
+
+
+@pytest.mark.parametrize('tag', ['plain', 'deltaWendland', 'bedDelta'])
+def test_the_neighbour_table_changes_no_bit(tag):
+    # the table keeps the cell walk's order, so the sums, and the whole run, are the same bits
+    case = caseFromRun(golden('runs.npz', tag))
+    walked, tw, _ = deviceRun(case, 25, table=False)
+    listed, tl, _ = deviceRun(case, 25, table=True)
+    assert tw == tl
+    assert np.array_equal(walked.positions, listed.positions)
+    assert np.array_equal(walked.velocities, listed.velocities)
+    assert np.array_equal(walked.densities, listed.densities)
+
+
+@pytest.mark.parametrize('threads', [2, 4])
+@pytest.mark.parametrize('table', [True, False])
+@pytest.mark.parametrize('tag', ['deltaWendland', 'bedDelta', 'limited'])
+def test_threads_per_particle_follow_the_reference(tag, table, threads):
+    # several threads to a particle change only the order of the float32 sums
+    r = golden('runs.npz', tag)
+    case = caseFromRun(r)
+    steps = int(r['steps'])
+    state, time, _ = deviceRun(case, steps, table=table, threads=threads)
+    assert time == pytest.approx(float(np.sum(r['dts'])), rel=1e-4)
+    assert np.abs(state.positions - r['finalPositions']).max() < 1e-6
+    assert np.abs(state.velocities - r['finalVelocities']).max() < 1e-3
+    assert np.abs(state.densities - r['finalDensities']).max() < 1e-3
+
+
+def test_threads_per_particle_on_the_benchmark_beach():
+    # the 64-ppd beach (122k particles) five steps at one and four threads a particle: the same run to
+    # float32 rounding of the sums (a grid four times longer must find room for every block's maxima)
+    case = cases.solitaryBeach(particlesPerDepth=64)
+    runs = []
+    for threads in (1, 4):
+        sums = cases.pairSumsFor(case)
+        sums.setSweepOptions(True, threads)
+        state = case.state.copy()
+        sums.push(state)
+        sums.setBoundary(case.boundary, state)
+        time, step, dt = sums.advance(0.0, 0, math.inf, 5, case.smoothingLength, case.cflNumber, case.maxTimeStep)
+        sums.pull(state)
+        runs.append((time, state))
+    (t1, a), (t4, b) = runs
+    assert t4 == pytest.approx(t1, rel=1e-9)
+    assert np.abs(a.positions - b.positions).max() < 1e-9
+    assert np.abs(a.velocities - b.velocities).max() < 1e-5

@@ -234,3 +234,29 @@ def test_height_field_enforcement():
     out = s.pullState()
     assert np.allclose(out['positions'], e['enforcedPositions'], rtol=0.0, atol=1e-12)
     assert np.allclose(out['velocities'], e['enforcedVelocities'], rtol=0.0, atol=1e-12)
+
+
+@pytest.mark.parametrize('tag', ['3d_p_wendlandC2', '2d_o_cubicSpline'])
+@pytest.mark.parametrize('threads', [1, 2, 4])
+@pytest.mark.parametrize('table', [True, False])
+def test_every_sweep_form_gives_the_reference_sums(tag, threads, table):
+    # the neighbour table on or off, one to four threads a particle: the same sums to float32 rounding
+    c = golden('clouds.npz', tag)
+    dim = c['positions'].shape[1]
+    g = np.zeros(dim)
+    g[-1] = -9.81
+    s = pairSums(c)
+    s.setSweepOptions(table, threads)
+    s.update(c['positions'], c['masses'], c['isFluid'])
+    close(s.pairAccelerations(c['velocities'], c['densities'], c['pressures'], c0, alpha, 0.3, g), c['accelerations'])
+    s.setViscosityLimiter(True)
+    close(s.velocityGradients(c['strained'], c['densities']), c['velocityGradients'], 2e-5)
+    close(s.pairAccelerations(c['strained'], c['densities'], c['pressures'], c0, alpha, 0.3, g),
+          c['limitedAccelerations'])
+    s.setDiffusion('antuono', 0.1, c0, rho0, 9.81)
+    close(s.densityGradients(c['densities']), c['densityGradients'], 2e-4)
+    close(s.continuityRate(c['velocities'], c['densities']), c['diffusive_antuono'])
+    close(s.wallPressure(c['densities'], c['pressures'], g, rho0, c0), c['wallPressure'])
+    fluid = c['isFluid']
+    close(s.xsphVelocity(c['velocities'], c['densities'], epsilon)[fluid], c['xsph'][fluid])
+    assert np.allclose(s.shepardDensity(c['densities']), c['shepard'], rtol=2e-6, atol=0.0)
