@@ -6,15 +6,18 @@
 //   per-particle constants carried through each re-sort:
 //     m, h (float64), fluid (uint8), orig (int32: the caller's index of the slot)
 //   the sweeps' float32 frame, rebuilt from the master each step:
-//     pa  float4  2D (hx, hy, lx, ly)      3D (hx, hy, hz, hs)
-//     pb  float4  2D (m, hs, dev, -)       3D (lx, ly, lz, m)
-//     kin float4  2D (vx, vy, rho, p)      3D (vx, vy, vz, rho)
-//     aux float2  3D (p, dev)
+//     pa   float4  2D (hx, hy, lx, ly)      3D (hx, hy, hz, hs)
+//     pb   float4  2D (m, hs, dev, V)       3D (lx, ly, lz, m)
+//     kin  float4  2D (vx, vy, rho, P2)     3D (vx, vy, vz, rho)
+//     aux  float4  3D (P2, dev, V, -)
+//     pres float   the pressure p
 //   hi + lo is each float64 coordinate split into a float32 point and its float32 remainder, so a
 //   separation (hi_i - hi_j) + (lo_i - lo_j) keeps the float64 positions' digits without float64
 //   arithmetic (src/pysurf/sphGpu.py:227-242 states the same split).  hs is +h for a fluid
 //   particle and -h for a boundary particle; dev is rho - rho0 in float32, taken in float64
 //   (src/pysurf/sphGpu.py:1031-1038), so neighbours' density differences keep their digits.
+//   V = m / rho and P2 = p / rho^2 are each particle's own, taken once per step instead of once per
+//   pair: the same float32 quotients the pair sums would take.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -73,8 +76,8 @@ struct Params {
 
 // The float32 frame and the float64 master state, current buffers.
 struct Frame {
-    float4 *pa, *pb, *kin;
-    float2 *aux;
+    float4 *pa, *pb, *kin, *aux;
+    float *pres;            // pressure
     int *cell;              // sorted cell index of each slot
     const int *cellStart;   // lower bound of each cell in the sorted order, numCells + 1 entries
     float4 *G0, *G1, *G2;   // velocity gradient rows (2D: G0 = (G00, G01, G10, G11))
@@ -108,38 +111,74 @@ struct Control {
 };
 
 // ------------------------------------------------------------------------------------------
-// Kernels W and dW/dr / r: src/pysurf/sphKernels.py:108-648; src/pysurf/sphGpu.py:139-204.
+// Kernels W and (dW/dr) / r: src/pysurf/sphKernels.py:108-648; src/pysurf/sphGpu.py:139-204.
+// The pair sums only ever take dW/dr divided by r (grad W = (dW/dr) r_ij / r), which for the
+// Wendland C2 is -5 sigma (1 - q/2)^3 / h^2 with no division by r, and for the cubic spline
+// sigma (2.25 q - 3) / h^2 inside q < 1.  The constants depend on h alone, so with one smoothing
+// length they are taken once per thread.
 // ------------------------------------------------------------------------------------------
+
+struct KernelAt {
+    float invH;     // 1 / h
+    float sigma;    // sigma at h
+    float gradC;    // Wendland: -5 sigma / h^2; cubic: sigma / h^2
+    float soft;     // the viscosity's and the diffusion's softening 0.01 h^2
+};
+
+template <int K, int D>
+__device__ __forceinline__ KernelAt kernelAt(float unit, float h)
+{
+    KernelAt k;
+    k.invH = 1.0f / h;
+    float s = unit * k.invH * k.invH;
+    if (D == 3) s *= k.invH;
+    k.sigma = s;
+    k.gradC = (K == 1 ? -5.0f : 1.0f) * s * k.invH * k.invH;
+    k.soft = kViscositySoftening * h * h;
+    return k;
+}
+
+// A pair's kernel constants at h_ij: one set a thread when every particle has the same smoothing
+// length (then h_ij = hMax), else taken per pair.
+template <int K, int D>
+struct Smoothing {
+    KernelAt fixed;
+    float unit;
+    bool mixed;
+    __device__ __forceinline__ explicit Smoothing(const Params &P)
+        : fixed(kernelAt<K, D>(P.sigmaUnit, P.hMax)), unit(P.sigmaUnit), mixed(P.mixedH != 0) {}
+    __device__ __forceinline__ KernelAt at(float h) const { return mixed ? kernelAt<K, D>(unit, h) : fixed; }
+};
+
+// W(q h), q < 2.
+template <int K>
+__device__ __forceinline__ float kernelValue(float q, const KernelAt &k)
+{
+    if (K == 1) {
+        float rest = 1.0f - 0.5f * q, sq = rest * rest;
+        return k.sigma * sq * sq * (2.0f * q + 1.0f);
+    }
+    if (q < 1.0f) return k.sigma * (1.0f - 1.5f * q * q + 0.75f * q * q * q);
+    float rest = 2.0f - q;
+    return k.sigma * 0.25f * rest * rest * rest;
+}
+
+// (dW/dr) / r at r = q h, 0 < q < 2.
+template <int K>
+__device__ __forceinline__ float kernelGradient(float q, const KernelAt &k)
+{
+    if (K == 1) {
+        float rest = 1.0f - 0.5f * q;
+        return k.gradC * rest * rest * rest;
+    }
+    if (q < 1.0f) return k.gradC * (2.25f * q - 3.0f);
+    float rest = 2.0f - q;
+    return __fdividef(-0.75f * k.gradC * rest * rest, q);
+}
 
 __device__ __forceinline__ float sigmaAt(float unit, float h, int dim)
 {
     return dim == 2 ? unit / (h * h) : unit / (h * h * h);
-}
-
-template <int K>
-__device__ __forceinline__ float kernelValue(float q, float sigma)
-{
-    if (K == 1) {
-        if (q >= 2.0f) return 0.0f;
-        float rest = 1.0f - 0.5f * q, sq = rest * rest;
-        return sigma * sq * sq * (2.0f * q + 1.0f);
-    }
-    if (q < 1.0f) return sigma * (1.0f - 1.5f * q * q + 0.75f * q * q * q);
-    if (q < 2.0f) { float rest = 2.0f - q; return sigma * 0.25f * rest * rest * rest; }
-    return 0.0f;
-}
-
-// dW/dr at distance r = q h, for r < 2h.
-template <int K>
-__device__ __forceinline__ float kernelSlope(float q, float h, float sigma)
-{
-    if (K == 1) {
-        float rest = 1.0f - 0.5f * q;
-        return -5.0f * sigma * q * rest * rest * rest / h;
-    }
-    if (q < 1.0f) return sigma * (-3.0f * q + 2.25f * q * q) / h;
-    float rest = 2.0f - q;
-    return sigma * (-0.75f * rest * rest) / h;
 }
 
 __device__ __forceinline__ int clampi(int a, int lo, int hi) { return a < lo ? lo : (a > hi ? hi : a); }
@@ -169,15 +208,7 @@ __device__ __forceinline__ int cellCoordinate(double value, double origin, doubl
 // Frame access per dimension.
 // ------------------------------------------------------------------------------------------
 
-template <int D> struct Pos;
-template <> struct Pos<2> {
-    float hx, hy, lx, ly;
-};
-template <> struct Pos<3> {
-    float hx, hy, hz, lx, ly, lz;
-};
-
-// A particle's signed smoothing length and mass.
+// A particle's signed smoothing length (+h fluid, -h boundary).
 template <int D> __device__ __forceinline__ float signedLength(const Frame &F, int j);
 template <> __device__ __forceinline__ float signedLength<2>(const Frame &F, int j) { return __ldg(&F.pb[j].y); }
 template <> __device__ __forceinline__ float signedLength<3>(const Frame &F, int j) { return __ldg(&F.pa[j].w); }
@@ -186,17 +217,41 @@ template <int D> __device__ __forceinline__ float massOf(const Frame &F, int j);
 template <> __device__ __forceinline__ float massOf<2>(const Frame &F, int j) { return __ldg(&F.pb[j].x); }
 template <> __device__ __forceinline__ float massOf<3>(const Frame &F, int j) { return __ldg(&F.pb[j].w); }
 
-template <int D> __device__ __forceinline__ float pressureOf(const Frame &F, int j);
-template <> __device__ __forceinline__ float pressureOf<2>(const Frame &F, int j) { return __ldg(&F.kin[j].w); }
-template <> __device__ __forceinline__ float pressureOf<3>(const Frame &F, int j) { return __ldg(&F.aux[j].x); }
+template <int D> __device__ __forceinline__ float pressureOf(const Frame &F, int j) { return __ldg(&F.pres[j]); }
+
+// p / rho^2
+template <int D> __device__ __forceinline__ float pressureRatioOf(const Frame &F, int j);
+template <> __device__ __forceinline__ float pressureRatioOf<2>(const Frame &F, int j) { return __ldg(&F.kin[j].w); }
+template <> __device__ __forceinline__ float pressureRatioOf<3>(const Frame &F, int j) { return __ldg(&F.aux[j].x); }
 
 template <int D> __device__ __forceinline__ float deviationOf(const Frame &F, int j);
 template <> __device__ __forceinline__ float deviationOf<2>(const Frame &F, int j) { return __ldg(&F.pb[j].z); }
 template <> __device__ __forceinline__ float deviationOf<3>(const Frame &F, int j) { return __ldg(&F.aux[j].y); }
 
+// m / rho
+template <int D> __device__ __forceinline__ float volumeOf(const Frame &F, int j);
+template <> __device__ __forceinline__ float volumeOf<2>(const Frame &F, int j) { return __ldg(&F.pb[j].w); }
+template <> __device__ __forceinline__ float volumeOf<3>(const Frame &F, int j) { return __ldg(&F.aux[j].z); }
+
 template <int D> __device__ __forceinline__ float densityOf(const Frame &F, int j);
 template <> __device__ __forceinline__ float densityOf<2>(const Frame &F, int j) { return __ldg(&F.kin[j].z); }
 template <> __device__ __forceinline__ float densityOf<3>(const Frame &F, int j) { return __ldg(&F.kin[j].w); }
+
+// Write a slot's density-derived fields: rho, rho - rho0, V = m / rho, p, p / rho^2.
+template <int D>
+__device__ __forceinline__ void storeDensity(const Frame &F, int i, float m, double rho64, double devReference, float p)
+{
+    const float rho = (float)rho64, dev = (float)(rho64 - devReference);
+    const float volume = m / rho, ratio = p / (rho * rho);
+    F.pres[i] = p;
+    if (D == 2) {
+        F.kin[i].z = rho; F.kin[i].w = ratio;
+        F.pb[i].z = dev; F.pb[i].w = volume;
+    } else {
+        F.kin[i].w = rho;
+        F.aux[i] = make_float4(ratio, dev, volume, 0.0f);
+    }
+}
 
 // Velocity (float32) of slot j.
 template <int D> __device__ __forceinline__ void velocityOf(const Frame &F, int j, float v[3])
@@ -205,7 +260,7 @@ template <int D> __device__ __forceinline__ void velocityOf(const Frame &F, int 
     v[0] = k.x; v[1] = k.y; v[2] = D == 3 ? k.z : 0.0f;
 }
 
-// Candidate coordinates (the float32 points alone) and the precise separation.
+// Candidate coordinates (the float32 points alone) and the remainders.
 template <int D> __device__ __forceinline__ void pointOf(const Frame &F, int j, float p[3]);
 template <> __device__ __forceinline__ void pointOf<2>(const Frame &F, int j, float p[3])
 {

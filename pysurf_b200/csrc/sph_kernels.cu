@@ -181,20 +181,24 @@ __global__ void gatherKernel(Params P, int n, const int *perm, const unsigned lo
     float hs = fl ? h : -h;
     float p = (float)taitPressure(P, rho, fl != 0);
     float dev = (float)(rho - P.devReference);
+    float rhoF = (float)rho;
+    float volume = m / rhoF, ratio = p / (rhoF * rhoF);
+    F.pres[s] = p;
     if (P.dim == 2) {
         F.pa[s] = make_float4(hi[0], hi[1], lo[0], lo[1]);
-        F.pb[s] = make_float4(m, hs, dev, 0.0f);
-        F.kin[s] = make_float4((float)v[0], (float)v[1], (float)rho, p);
+        F.pb[s] = make_float4(m, hs, dev, volume);
+        F.kin[s] = make_float4((float)v[0], (float)v[1], rhoF, ratio);
     } else {
         F.pa[s] = make_float4(hi[0], hi[1], hi[2], hs);
         F.pb[s] = make_float4(lo[0], lo[1], lo[2], m);
-        F.kin[s] = make_float4((float)v[0], (float)v[1], (float)v[2], (float)rho);
-        F.aux[s] = make_float2(p, dev);
+        F.kin[s] = make_float4((float)v[0], (float)v[1], (float)v[2], rhoF);
+        F.aux[s] = make_float4(ratio, dev, volume, 0.0f);
     }
 }
 
 // The frame's velocity, density, deviation and pressure from caller-order float64 arrays (the
-// host-step sums take these from the caller each call).  Any of them may be null.
+// host-step sums take these from the caller each call), then V = m / rho and p / rho^2 from the
+// frame's density and pressure.  Any of the arrays may be null.
 __global__ void loadFieldsKernel(Params P, int n, const int *orig, const double *velocities, const double *densities,
                                  const double *pressures, double deviationReference, Frame F)
 {
@@ -207,18 +211,26 @@ __global__ void loadFieldsKernel(Params P, int n, const int *orig, const double 
         k.y = (float)velocities[o * P.dim + 1];
         if (P.dim == 3) k.z = (float)velocities[o * P.dim + 2];
     }
+    float p = pressures ? (float)pressures[o] : F.pres[s];
+    F.pres[s] = p;
     if (P.dim == 2) {
+        float4 b = F.pb[s];
         if (densities) {
             k.z = (float)densities[o];
-            F.pb[s].z = (float)(densities[o] - deviationReference);
+            b.z = (float)(densities[o] - deviationReference);
         }
-        if (pressures) k.w = (float)pressures[o];
+        b.w = b.x / k.z;
+        k.w = p / (k.z * k.z);
+        F.pb[s] = b;
     } else {
+        float4 x = F.aux[s];
         if (densities) {
             k.w = (float)densities[o];
-            F.aux[s].y = (float)(densities[o] - deviationReference);
+            x.y = (float)(densities[o] - deviationReference);
         }
-        if (pressures) F.aux[s].x = (float)pressures[o];
+        x.z = F.pb[s].w / k.w;
+        x.x = p / (k.w * k.w);
+        F.aux[s] = x;
     }
     F.kin[s] = k;
 }

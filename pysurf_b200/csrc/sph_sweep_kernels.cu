@@ -69,15 +69,16 @@ __device__ __forceinline__ bool filterDue(const Control *ctl)
 template <int D, int K>
 struct ShepardVisit {
     static constexpr bool kSkipCoincident = false;
-    const Params &P; const Frame &F;
+    const Frame &F;
+    Smoothing<K, D> S;
     float num, den;
     __device__ bool accept(bool) const { return true; }
     __device__ void operator()(int j, const float *, float r, float h, bool, int)
     {
-        float w = kernelValue<K>(r / h, sigmaAt(P.sigmaUnit, h, D));
-        float mj = massOf<D>(F, j);
-        num += mj * w;
-        den += mj / densityOf<D>(F, j) * w;
+        const KernelAt k = S.at(h);
+        float w = kernelValue<K>(r * k.invH, k);
+        num += massOf<D>(F, j) * w;
+        den += volumeOf<D>(F, j) * w;
     }
 };
 
@@ -92,7 +93,7 @@ __global__ void __launch_bounds__(kBlock) shepardKernel(Params P, Frame F, const
     // the particle itself first, as the reference's sums start (src/pysurf/sphGpu.py:781-783)
     float own = sigmaAt(P.sigmaUnit, hI, D);
     float mi = massOf<D>(F, i);
-    ShepardVisit<D, K> visit{P, F, G.t == 0 ? mi * own : 0.0f, G.t == 0 ? mi / densityOf<D>(F, i) * own : 0.0f};
+    ShepardVisit<D, K> visit{F, Smoothing<K, D>(P), G.t == 0 ? mi * own : 0.0f, G.t == 0 ? volumeOf<D>(F, i) * own : 0.0f};
     forEachNeighbour<D, T>(P, F, i, G.t, hI, visit);
     float num = groupSum<T>(visit.num, G.mask), den = groupSum<T>(visit.den, G.mask);
     if (G.t != 0) return;
@@ -110,13 +111,7 @@ __global__ void applyShepardKernel(Params P, Frame F, const Control *ctl)
     float filtered = F.scalar[i];
     double rho = (double)filtered;
     F.rho[i] = rho;
-    float p = (float)taitPressure(P, rho, true);
-    float dev = (float)(rho - P.devReference);
-    if (D == 2) {
-        F.kin[i].z = filtered; F.kin[i].w = p; F.pb[i].z = dev;
-    } else {
-        F.kin[i].w = filtered; F.aux[i] = make_float2(p, dev);
-    }
+    storeDensity<D>(F, i, massOf<D>(F, i), rho, P.devReference, (float)taitPressure(P, rho, true));
 }
 
 // ------------------------------------------------------------------------------------------
@@ -127,11 +122,13 @@ template <int D, int K>
 struct WallVisit {
     static constexpr bool kSkipCoincident = false;
     const Params &P; const Frame &F;
+    Smoothing<K, D> S;
     float weight, total;
     __device__ bool accept(bool fluidJ) const { return fluidJ; }
     __device__ void operator()(int j, const float *d, float r, float h, bool, int)
     {
-        float w = kernelValue<K>(r / h, sigmaAt(P.sigmaUnit, h, D));
+        const KernelAt k = S.at(h);
+        float w = kernelValue<K>(r * k.invH, k);
         float gd = P.g[0] * d[0] + P.g[1] * d[1] + (D == 3 ? P.g[2] * d[2] : 0.0f);
         weight += w;
         total += w * (pressureOf<D>(F, j) + densityOf<D>(F, j) * gd);
@@ -149,23 +146,24 @@ __global__ void __launch_bounds__(kBlock) wallPressureKernel(Params P, Frame F, 
     if (i >= P.n) return;
     float hs = signedLength<D>(F, i);
     if (hs > 0.0f) return;
-    WallVisit<D, K> visit{P, F, 0.0f, 0.0f};
+    WallVisit<D, K> visit{P, F, Smoothing<K, D>(P), 0.0f, 0.0f};
     forEachNeighbour<D, T>(P, F, i, G.t, -hs, visit);
     float weight = groupSum<T>(visit.weight, G.mask), total = groupSum<T>(visit.total, G.mask);
     if (G.t != 0) return;
     float p = 0.0f;
     if (weight > 0.0f) p = fmaxf(total / weight, 0.0f);
-    double rho = P.rho0 * pow(1.0 + (double)p / P.stiffness, 1.0 / 7.0);
-    float dev = (float)(rho - P.devReference);
     F.scalar[i] = p;
-    if (D == 2) {
-        F.kin[i].w = p;
-        if (writeDensity) { F.kin[i].z = (float)rho; F.pb[i].z = dev; }
-    } else {
-        F.aux[i].x = p;
-        if (writeDensity) { F.kin[i].w = (float)rho; F.aux[i].y = dev; }
+    if (writeDensity) {
+        double rho = P.rho0 * pow(1.0 + (double)p / P.stiffness, 1.0 / 7.0);
+        storeDensity<D>(F, i, massOf<D>(F, i), rho, P.devReference, p);
+        F.rho[i] = rho;
+        return;
     }
-    if (writeDensity) F.rho[i] = rho;
+    // the density stays; the pressure and p / rho^2 take p_w
+    const float rho = densityOf<D>(F, i), ratio = p / (rho * rho);
+    F.pres[i] = p;
+    if (D == 2) F.kin[i].w = ratio;
+    else F.aux[i].x = ratio;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -175,15 +173,16 @@ __global__ void __launch_bounds__(kBlock) wallPressureKernel(Params P, Frame F, 
 template <int D, int K>
 struct GradientVisit {
     static constexpr bool kSkipCoincident = true;
-    const Params &P; const Frame &F;
+    const Frame &F;
+    Smoothing<K, D> kernel;
     bool wantG, wantL, wantRho;
     float vi[3], devI;
     float S[3][3], Mf[3][3], M[3][3], gsum[3];
     __device__ bool accept(bool) const { return true; }
     __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int)
     {
-        float slope = kernelSlope<K>(r / h, h, sigmaAt(P.sigmaUnit, h, D));
-        float w = massOf<D>(F, j) / densityOf<D>(F, j) * slope / r;
+        const KernelAt k = kernel.at(h);
+        float w = volumeOf<D>(F, j) * kernelGradient<K>(r * k.invH, k);
         if (wantG && fluidJ) {
             float vj[3];
             velocityOf<D>(F, j, vj);
@@ -228,7 +227,7 @@ gradientKernel(Params P, Frame F, const Control *ctl, int wantG, int wantL, int 
         if (wantRho) F.gradRho[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         return;
     }
-    GradientVisit<D, K> visit{P, F, wantG != 0, wantL != 0 || wantRho != 0, wantRho != 0};
+    GradientVisit<D, K> visit{F, Smoothing<K, D>(P), wantG != 0, wantL != 0 || wantRho != 0, wantRho != 0};
     velocityOf<D>(F, i, visit.vi);
     visit.devI = deviationOf<D>(F, i);
     for (int a = 0; a < 3; ++a) {
@@ -276,17 +275,19 @@ template <int D, int K>
 struct MomentumVisit {
     static constexpr bool kSkipCoincident = true;
     const Params &P; const Frame &F;
-    float vi[3], rhoI, own;
+    Smoothing<K, D> S;
+    float vi[3], rhoI, own, viscosityScale;   // viscosityScale: -alpha c0
     float Gi[3][3];
     float total[3];
     __device__ bool accept(bool) const { return true; }
     __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int)
     {
+        const KernelAt k = S.at(h);
+        const float q = r * k.invH;
         float vj[3];
         velocityOf<D>(F, j, vj);
         float rel[3] = {vi[0] - vj[0], vi[1] - vj[1], vi[2] - vj[2]};
         float approach = rel[0] * d[0] + rel[1] * d[1] + (D == 3 ? rel[2] * d[2] : 0.0f);
-        float rhoJ = densityOf<D>(F, j);
         float viscosity = 0.0f;
         if (approach < 0.0f && P.limited && fluidJ) {
             float Gj[3][3];
@@ -300,11 +301,11 @@ struct MomentumVisit {
             }
             float limiter = 0.0f;
             if (slopeI * slopeJ > 0.0f) {
-                float ratio = slopeI / slopeJ;
-                limiter = fminf(1.0f, 4.0f * ratio / ((1.0f + ratio) * (1.0f + ratio)));
-                float eta = r / h;
-                if (eta < kCloseDistance) {
-                    float fade = (eta - kCloseDistance) / kFoldWidth;
+                // 4 R / (1 + R)^2 at R = slopeI / slopeJ, as 4 slopeI slopeJ / (slopeI + slopeJ)^2
+                const float sum = slopeI + slopeJ;
+                limiter = fminf(1.0f, 4.0f * slopeI * slopeJ / (sum * sum));
+                if (q < kCloseDistance) {
+                    float fade = (q - kCloseDistance) * (1.0f / kFoldWidth);
                     limiter *= expf(-fade * fade);
                 }
             }
@@ -312,13 +313,14 @@ struct MomentumVisit {
             for (int a = 0; a < D; ++a) approach += (rel[a] - 0.5f * limiter * (rampI[a] + rampJ[a])) * d[a];
         }
         if (approach < 0.0f) {
-            float mu = h * approach / (r * r + kViscositySoftening * h * h);
-            viscosity = -P.alpha * P.c0 * mu / (0.5f * (rhoI + rhoJ));
+            // -alpha c0 h (v_ij . r_ij) / ((r^2 + 0.01 h^2) (rho_i + rho_j) / 2); the denominator is
+            // a positive normal float for any physical pair, which __fdividef takes to 2 ulp
+            viscosity = __fdividef(viscosityScale * h * approach,
+                                   (r * r + k.soft) * (0.5f * (rhoI + densityOf<D>(F, j))));
             if (!fluidJ) viscosity *= P.boundaryFactor;
         }
-        float coefficient = -(own + pressureOf<D>(F, j) / (rhoJ * rhoJ) + viscosity) * massOf<D>(F, j);
-        float slope = kernelSlope<K>(r / h, h, sigmaAt(P.sigmaUnit, h, D));
-        float f = coefficient * slope / r;
+        float coefficient = -(own + pressureRatioOf<D>(F, j) + viscosity) * massOf<D>(F, j);
+        float f = coefficient * kernelGradient<K>(q, k);
         for (int a = 0; a < D; ++a) total[a] += f * d[a];
     }
 };
@@ -358,10 +360,11 @@ __global__ void __launch_bounds__(kBlock) momentumKernel(Params P, Frame F, Cont
         if (hs <= 0.0f) {
             if (G.t == 0) F.acc[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         } else {
-            MomentumVisit<D, K> visit{P, F};
+            MomentumVisit<D, K> visit{P, F, Smoothing<K, D>(P)};
             velocityOf<D>(F, i, visit.vi);
             visit.rhoI = densityOf<D>(F, i);
-            visit.own = pressureOf<D>(F, i) / (visit.rhoI * visit.rhoI);
+            visit.own = pressureRatioOf<D>(F, i);
+            visit.viscosityScale = -P.alpha * P.c0;
             if (P.limited) loadMatrix<D>(F.G0, F.G1, F.G2, i, visit.Gi);
             visit.total[0] = visit.total[1] = visit.total[2] = 0.0f;
             forEachNeighbour<D, T>(P, F, i, G.t, hs, visit);
@@ -460,16 +463,17 @@ template <int D, int K>
 struct ContinuityVisit {
     static constexpr bool kSkipCoincident = true;
     const Params &P; const Frame &F;
+    Smoothing<K, D> S;
     bool boundaryI, diffuses, corrected;
     float vi[3], devI, Li[3][3], gi[3];
     float total;
     __device__ bool accept(bool fluidJ) const { return !(boundaryI && !fluidJ); }
     __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int)
     {
-        float slope = kernelSlope<K>(r / h, h, sigmaAt(P.sigmaUnit, h, D));
+        const KernelAt k = S.at(h);
+        const float grad = kernelGradient<K>(r * k.invH, k);    // (dW/dr) / r
         float vj[3];
         velocityOf<D>(F, j, vj);
-        float mj = massOf<D>(F, j);
         float dot = 0.0f;
         if (corrected) {
             for (int a = 0; a < D; ++a) {
@@ -480,14 +484,14 @@ struct ContinuityVisit {
         } else {
             for (int a = 0; a < D; ++a) dot += (vi[a] - vj[a]) * d[a];
         }
-        total += mj * dot * slope / r;
+        total += massOf<D>(F, j) * dot * grad;
         if (diffuses && fluidJ) {
             float devJ = deviationOf<D>(F, j);
             float difference = devJ - devI;
             if (P.diffusion == 2) {
                 float ratio = 1.0f + 0.5f * (devI + devJ) / P.rho0F;
                 float sq = ratio * ratio;
-                difference -= P.rho0F * P.gravityOverSound * d[D - 1] / (sq * sq * ratio);
+                difference -= __fdividef(P.rho0F * P.gravityOverSound * d[D - 1], sq * sq * ratio);
             } else if (P.diffusion == 3) {
                 float4 gj = __ldg(&F.gradRho[j]);
                 float gjv[3] = {gj.x, gj.y, gj.z};
@@ -495,8 +499,10 @@ struct ContinuityVisit {
                 for (int a = 0; a < D; ++a) t += (gi[a] + gjv[a]) * d[a];
                 difference += 0.5f * t;
             }
-            total += P.diffusionFactor * h * mj / densityOf<D>(F, j) * difference * (-slope * r)
-                   / (r * r + kViscositySoftening * h * h);
+            // 2 delta c0 h V_j (difference) (-(dW/dr) r) / (r^2 + 0.01 h^2), with (dW/dr) r = grad r^2
+            const float r2 = r * r;
+            total += P.diffusionFactor * h * volumeOf<D>(F, j) * difference * (-grad)
+                   * __fdividef(r2, r2 + k.soft);
         }
     }
 };
@@ -510,7 +516,7 @@ __global__ void __launch_bounds__(kBlock) continuityKernel(Params P, Frame F, Co
     const int i = G.i;
     if (i >= P.n) return;
     float hs = signedLength<D>(F, i);
-    ContinuityVisit<D, K> visit{P, F};
+    ContinuityVisit<D, K> visit{P, F, Smoothing<K, D>(P)};
     visit.boundaryI = hs <= 0.0f;
     visit.diffuses = P.diffusion != 0 && !visit.boundaryI;
     visit.corrected = P.corrected && !visit.boundaryI;
@@ -544,12 +550,14 @@ __global__ void __launch_bounds__(kBlock) continuityKernel(Params P, Frame F, Co
 template <int D, int K>
 struct XsphVisit {
     static constexpr bool kSkipCoincident = false;
-    const Params &P; const Frame &F; const float *densities;
+    const Frame &F; const float *densities;
+    Smoothing<K, D> S;
     float vi[3], rhoI, corr[3];
     __device__ bool accept(bool fluidJ) const { return fluidJ; }
     __device__ void operator()(int j, const float *, float r, float h, bool, int)
     {
-        float w = kernelValue<K>(r / h, sigmaAt(P.sigmaUnit, h, D));
+        const KernelAt k = S.at(h);
+        float w = kernelValue<K>(r * k.invH, k);
         float rhoJ = densities ? densities[j] : densityOf<D>(F, j);
         float weight = massOf<D>(F, j) * w / (0.5f * (rhoI + rhoJ));
         float vj[3];
@@ -575,7 +583,7 @@ xsphKernel(Params P, Frame F, Control *ctl, Enforcement E, const float *densitie
         if (G.t == 0) F.vec[i] = make_float4(v[0], v[1], v[2], 0.0f);
         return;
     }
-    XsphVisit<D, K> visit{P, F, densities};
+    XsphVisit<D, K> visit{F, densities, Smoothing<K, D>(P)};
     visit.vi[0] = v[0]; visit.vi[1] = v[1]; visit.vi[2] = v[2];
     visit.rhoI = densities ? densities[i] : densityOf<D>(F, i);
     visit.corr[0] = visit.corr[1] = visit.corr[2] = 0.0f;

@@ -116,8 +116,8 @@ struct SphSystem {
     MasterView master[2]{};
     float4 *pa = nullptr, *pb = nullptr, *kin = nullptr, *G[3] = {}, *L[3] = {}, *gradRho = nullptr, *acc = nullptr,
            *vec = nullptr;
-    float2 *aux = nullptr;
-    float *rate = nullptr, *scalar = nullptr;
+    float4 *aux = nullptr;
+    float *pres = nullptr, *rate = nullptr, *scalar = nullptr;
     int *cell = nullptr, *cellStart = nullptr;
     unsigned long long *keys[2] = {nullptr, nullptr};
     int *vals[2] = {nullptr, nullptr};
@@ -169,7 +169,7 @@ struct SphSystem {
             cudaFree(keys[b]); cudaFree(vals[b]);
             keys[b] = nullptr; vals[b] = nullptr;
         }
-        void *ptrs[] = {pa, pb, kin, G[0], G[1], G[2], L[0], L[1], L[2], gradRho, acc, vec, aux, rate, scalar, cell,
+        void *ptrs[] = {pa, pb, kin, G[0], G[1], G[2], L[0], L[1], L[2], gradRho, acc, vec, aux, pres, rate, scalar, cell,
                         counts, blockMaxima, dStage, dStageU8, dRank, nbr, ncount};
         for (void *p : ptrs) cudaFree(p);
         nbr = ncount = nullptr;
@@ -178,7 +178,7 @@ struct SphSystem {
         listDirty = true;
         pa = pb = kin = gradRho = acc = vec = nullptr;
         for (int a = 0; a < 3; ++a) G[a] = L[a] = nullptr;
-        aux = nullptr; rate = scalar = nullptr; cell = nullptr; counts = nullptr; blockMaxima = nullptr;
+        aux = nullptr; pres = rate = scalar = nullptr; cell = nullptr; counts = nullptr; blockMaxima = nullptr;
         dStage = nullptr; dStageU8 = nullptr; dRank = nullptr;
         capacity = 0;
         return SPH_OK;
@@ -236,6 +236,7 @@ struct SphSystem {
         TRY(deviceAlloc(&pb, cap));
         TRY(deviceAlloc(&kin, cap));
         TRY(deviceAlloc(&aux, cap));
+        TRY(deviceAlloc(&pres, cap));
         for (int a = 0; a < 3; ++a) { TRY(deviceAlloc(&G[a], cap)); TRY(deviceAlloc(&L[a], cap)); }
         TRY(deviceAlloc(&gradRho, cap));
         TRY(deviceAlloc(&acc, cap));
@@ -253,7 +254,8 @@ struct SphSystem {
         TRY(deviceAlloc(&ncount, cap));
         CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(float4) * cap, stream));
         CUDA_TRY(cudaMemsetAsync(kin, 0, sizeof(float4) * cap, stream));
-        CUDA_TRY(cudaMemsetAsync(aux, 0, sizeof(float2) * cap, stream));
+        CUDA_TRY(cudaMemsetAsync(aux, 0, sizeof(float4) * cap, stream));
+        CUDA_TRY(cudaMemsetAsync(pres, 0, sizeof(float) * cap, stream));
         graphDirty = true;
         framed = false;
         return SPH_OK;
@@ -350,7 +352,7 @@ struct SphSystem {
     Frame frame() const
     {
         Frame F{};
-        F.pa = pa; F.pb = pb; F.kin = kin; F.aux = aux;
+        F.pa = pa; F.pb = pb; F.kin = kin; F.aux = aux; F.pres = pres;
         F.cell = cell; F.cellStart = cellStart;
         F.G0 = G[0]; F.G1 = G[1]; F.G2 = G[2];
         F.L0 = L[0]; F.L1 = L[1]; F.L2 = L[2];
