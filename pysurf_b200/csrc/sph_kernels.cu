@@ -1,8 +1,8 @@
 // sph_kernels.cu -- the B200 kernels of the delta-SPH step.
 //
-//   cell list      keys (cell, caller index) -> LSD radix sort -> cell lower bounds -> one gather
-//                  that permutes the float64 master and builds the float32 frame (with the Tait
-//                  pressure and the density deviation fused in)
+//   cell list      counting sort by cell, each cell's slots in caller-index order -> cell lower
+//                  bounds -> one gather that permutes the float64 master and builds the float32
+//                  frame (with the Tait pressure, the density deviation, m / rho and p / rho^2)
 //   sweeps         A  wall pressure      boundary rows over fluid neighbours
 //                  B  gradients          fluid rows: velocity gradient G, correction L, grad rho
 //                  C  momentum           fluid rows: pressure, limited viscosity, gravity; the
@@ -27,9 +27,18 @@ namespace sph {
 // Cell list
 // ------------------------------------------------------------------------------------------
 
-// Each slot's key: its cell in the high bits, the caller's index in the low bits.
-__global__ void cellKeysKernel(Params P, int n, const double *x0, const double *x1, const double *x2,
-                               const int *orig, int origBits, unsigned long long *keys, int *vals, const Control *ctl)
+// A counting sort by cell, in four launches:
+//   count  each slot's cell, and its place among the slots of that cell in the order the atomics
+//          hand places out (an arbitrary order)
+//   scan   the cells' lower bounds from the counts (two launches), which also clears the counts
+//   place  each slot into its cell's range at that place, with its caller index
+//   rank   within each cell, the slots in caller-index order: a slot's rank is the number of its
+//          cellmates with a smaller caller index, so the sorted order is (cell, caller index), a
+//          function of the state alone
+// A cell holds a handful of slots, so the rank's loop over the cell is short; its cost grows with
+// the square of a cell's count, as the sweeps' candidate tests over that cell already do.
+__global__ void cellCountKernel(Params P, int n, const double *x0, const double *x1, const double *x2, int *slotCell,
+                                int *slotWithin, int *cellCount, const Control *ctl)
 {
     if (ctl && !ctl->active) return;
     int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -37,120 +46,124 @@ __global__ void cellKeysKernel(Params P, int n, const double *x0, const double *
     int cx = cellCoordinate(x0[s], P.origin[0], P.cellWidth, P.nc[0]);
     int cy = cellCoordinate(x1[s], P.origin[1], P.cellWidth, P.nc[1]);
     int cz = P.dim == 3 ? cellCoordinate(x2[s], P.origin[2], P.cellWidth, P.nc[2]) : 0;
-    unsigned long long c = (unsigned long long)((cz * P.nc[1] + cy) * P.nc[0] + cx);
-    keys[s] = (c << origBits) | (unsigned long long)(unsigned)orig[s];
-    vals[s] = s;
+    int c = (cz * P.nc[1] + cy) * P.nc[0] + cx;
+    slotCell[s] = c;
+    slotWithin[s] = atomicAdd(&cellCount[c], 1);
 }
 
-// Radix sort, 8-bit digits, least significant first.  A tile is kRadixItems keys per thread of a
-// 256-thread block, taken in rounds of 256 consecutive keys so that ranks stay stable.
-constexpr int kRadixThreads = 256;
-constexpr int kRadixItems = 8;
-constexpr int kRadixTile = kRadixThreads * kRadixItems;
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
 
-__global__ void radixHistogramKernel(const unsigned long long *keys, int n, int shift, unsigned *counts, int blocks,
-                                     const Control *ctl)
+// The block's sum of one value a thread (every thread gets it).
+__device__ __forceinline__ int blockSumInt(int value, int *shared)
 {
-    if (ctl && !ctl->active) return;
-    __shared__ unsigned hist[256];
-    hist[threadIdx.x] = 0;
+    for (int offset = 16; offset > 0; offset >>= 1) value += __shfl_xor_sync(0xFFFFFFFFu, value, offset);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     __syncthreads();
-    int base = blockIdx.x * kRadixTile;
-    for (int k = 0; k < kRadixItems; ++k) {
-        int idx = base + k * kRadixThreads + threadIdx.x;
-        if (idx < n) atomicAdd(&hist[(keys[idx] >> shift) & 0xFF], 1u);
-    }
+    if (lane == 0) shared[warp] = value;
     __syncthreads();
-    counts[threadIdx.x * blocks + blockIdx.x] = hist[threadIdx.x];
+    value = lane < (int)(blockDim.x >> 5) ? shared[lane] : 0;
+    for (int offset = 16; offset > 0; offset >>= 1) value += __shfl_xor_sync(0xFFFFFFFFu, value, offset);
+    return value;
 }
 
-// Exclusive scan of the digit-major counts in one block.
-__global__ void radixScanKernel(unsigned *counts, int total, const Control *ctl)
+// partials[b] = the sum of tile b's counts.
+__global__ void __launch_bounds__(kScanThreads)
+cellScanReduceKernel(const int *cellCount, int total, int *partials, const Control *ctl)
 {
     if (ctl && !ctl->active) return;
-    __shared__ unsigned partial[1024];
-    int t = threadIdx.x;
-    int per = (total + blockDim.x - 1) / blockDim.x;
-    int lo = t * per, hi = min(lo + per, total);
-    unsigned sum = 0;
-    for (int k = lo; k < hi; ++k) sum += counts[k];
-    partial[t] = sum;
-    __syncthreads();
-    for (int offset = 1; offset < blockDim.x; offset <<= 1) {
-        unsigned add = t >= offset ? partial[t - offset] : 0;
-        __syncthreads();
-        partial[t] += add;
-        __syncthreads();
+    __shared__ int shared[32];
+    const int base = blockIdx.x * kScanTile;
+    int sum = 0;
+    for (int k = 0; k < kScanItems; ++k) {
+        int idx = base + k * kScanThreads + threadIdx.x;
+        if (idx < total) sum += cellCount[idx];
     }
-    unsigned running = t > 0 ? partial[t - 1] : 0;
-    for (int k = lo; k < hi; ++k) {
-        unsigned c = counts[k];
-        counts[k] = running;
-        running += c;
-    }
+    sum = blockSumInt(sum, shared);
+    if (threadIdx.x == 0) partials[blockIdx.x] = sum;
 }
 
-__global__ void radixScatterKernel(const unsigned long long *keysIn, const int *valsIn, int n, int shift,
-                                   const unsigned *offsets, int blocks, unsigned long long *keysOut, int *valsOut,
-                                   const Control *ctl)
+// cellStart[c] = the counts' exclusive prefix sum; the counts go back to zero for the next sort.
+__global__ void __launch_bounds__(kScanThreads)
+cellScanApplyKernel(int *cellCount, int total, const int *partials, int *cellStart, const Control *ctl)
 {
     if (ctl && !ctl->active) return;
-    __shared__ unsigned running[256];
-    __shared__ unsigned warpCount[kRadixThreads / 32][256];
-    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
-    running[t] = offsets[t * blocks + blockIdx.x];
-    const int base = blockIdx.x * kRadixTile;
-    for (int k = 0; k < kRadixItems; ++k) {
-        for (int w = 0; w < kRadixThreads / 32; ++w) warpCount[w][t] = 0;
-        __syncthreads();
-        int idx = base + k * kRadixThreads + t;
-        bool valid = idx < n;
-        unsigned long long key = valid ? keysIn[idx] : 0ull;
-        int digit = valid ? (int)((key >> shift) & 0xFF) : 256 + lane;   // invalid lanes match nobody
-        unsigned peers = __match_any_sync(0xFFFFFFFFu, digit);
-        unsigned below = peers & ((1u << lane) - 1u);
-        int rankInWarp = __popc(below);
-        if (valid && below == 0) warpCount[warp][digit] = __popc(peers);
-        __syncthreads();
-        // thread t owns digit t: exclusive prefix over the warps, in place
-        unsigned sum = 0;
-        for (int w = 0; w < kRadixThreads / 32; ++w) {
-            unsigned c = warpCount[w][t];
-            warpCount[w][t] = sum;
-            sum += c;
+    __shared__ int shared[32];
+    // the tiles before this one
+    int before = 0;
+    for (int b = threadIdx.x; b < (int)blockIdx.x; b += kScanThreads) before += partials[b];
+    before = blockSumInt(before, shared);
+    // thread t scans items base + 4t .. base + 4t + 3
+    const int first = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    int item[kScanItems], sum = 0;
+    for (int k = 0; k < kScanItems; ++k) {
+        item[k] = first + k < total ? cellCount[first + k] : 0;
+        sum += item[k];
+    }
+    // exclusive prefix of the threads' sums: within the warp, then over the warps
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int inclusive = sum;
+    for (int offset = 1; offset < 32; offset <<= 1) {
+        int up = __shfl_up_sync(0xFFFFFFFFu, inclusive, offset);
+        if (lane >= offset) inclusive += up;
+    }
+    __syncthreads();
+    if (lane == 31) shared[warp] = inclusive;
+    __syncthreads();
+    if (warp == 0) {
+        int w = lane < kScanThreads / 32 ? shared[lane] : 0, wi = w;
+        for (int offset = 1; offset < 32; offset <<= 1) {
+            int up = __shfl_up_sync(0xFFFFFFFFu, wi, offset);
+            if (lane >= offset) wi += up;
         }
-        __syncthreads();
-        if (valid) {
-            unsigned pos = running[digit] + warpCount[warp][digit] + rankInWarp;
-            keysOut[pos] = key;
-            valsOut[pos] = valsIn[idx];
+        if (lane < kScanThreads / 32) shared[lane] = wi - w;
+    }
+    __syncthreads();
+    int running = before + shared[warp] + inclusive - sum;
+    for (int k = 0; k < kScanItems; ++k) {
+        if (first + k < total) {
+            cellStart[first + k] = running;
+            cellCount[first + k] = 0;
         }
-        __syncthreads();
-        running[t] += sum;
-        __syncthreads();
+        running += item[k];
     }
 }
 
-// cellStart[c] = the first sorted slot whose cell is >= c, for c = 0 .. numCells.
-__global__ void cellStartKernel(const unsigned long long *sortedKeys, int n, int origBits, int numCells,
-                                int *cellStart, const Control *ctl)
+__global__ void cellPlaceKernel(int n, const int *slotCell, const int *slotWithin, const int *orig,
+                                const int *cellStart, int2 *bucket, const Control *ctl)
 {
     if (ctl && !ctl->active) return;
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c > numCells) return;
-    int lo = 0, hi = n;
-    while (lo < hi) {
-        int mid = (lo + hi) >> 1;
-        if ((int)(sortedKeys[mid] >> origBits) < c) lo = mid + 1; else hi = mid;
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    bucket[cellStart[slotCell[s]] + slotWithin[s]] = make_int2(orig[s], s);
+}
+
+// perm[k] = the old slot of sorted slot k; sortedCell[k] = its cell.
+__global__ void cellRankKernel(int n, const int2 *bucket, const int *slotCell, const int *cellStart, int *perm,
+                               int *sortedCell, const Control *ctl)
+{
+    if (ctl && !ctl->active) return;
+    int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const int2 e = bucket[k];
+    const int c = slotCell[e.y];
+    const int start = cellStart[c], end = cellStart[c + 1];
+    // ties (never, with distinct caller indices) fall to the old slot, so the ranks stay a permutation
+    int rank = 0;
+    for (int q = start; q < end; ++q) {
+        const int2 o = bucket[q];
+        rank += o.x < e.x || (o.x == e.x && o.y < e.y);
     }
-    cellStart[c] = lo;
+    perm[start + rank] = e.y;
+    sortedCell[start + rank] = c;
 }
 
 // Permute the master into the new order (from the old buffers) and build the float32 frame:
 // points and remainders (src/pysurf/sphGpu.py:1010-1019), float32 velocity and density
 // (1021-1029), deviation (1031-1038) and the Tait pressure (1058-1070).
-__global__ void gatherKernel(Params P, int n, const int *perm, const unsigned long long *sortedKeys, int origBits,
-                             MasterView from, MasterView to, Frame F, const Control *ctl)
+__global__ void gatherKernel(Params P, int n, const int *perm, MasterView from, MasterView to, Frame F,
+                             const Control *ctl)
 {
     if (ctl && !ctl->active) return;
     int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -172,7 +185,6 @@ __global__ void gatherKernel(Params P, int n, const int *perm, const unsigned lo
     to.h[s] = h64;
     to.fluid[s] = fl;
     to.orig[s] = from.orig[o];
-    F.cell[s] = (int)(sortedKeys[s] >> origBits);
     float hi[3], lo[3];
     for (int a = 0; a < 3; ++a) {
         hi[a] = (float)x[a];
@@ -457,44 +469,26 @@ __global__ void splitKernel(int n, int dim, MasterView M, const uint8_t *chosenB
 
 static inline int blocksFor(long long n, int block) { return (int)((n + block - 1) / block); }
 
-void launchCellKeys(const Params &P, int n, const MasterView &M, int origBits, unsigned long long *keys, int *vals,
-                    const Control *ctl, cudaStream_t st)
+int scanTiles(int total) { return blocksFor(total, kScanTile); }
+
+void launchCellSort(const Params &P, int n, const MasterView &M, const CellSortBuffers &B, int *cellStart,
+                    int *sortedCell, const Control *ctl, cudaStream_t st)
 {
     if (n == 0) return;
-    cellKeysKernel<<<blocksFor(n, 256), 256, 0, st>>>(P, n, M.x[0], M.x[1], M.x[2], M.orig, origBits, keys, vals, ctl);
+    const int total = P.nc[0] * P.nc[1] * P.nc[2] + 1, tiles = scanTiles(total);
+    cellCountKernel<<<blocksFor(n, 256), 256, 0, st>>>(P, n, M.x[0], M.x[1], M.x[2], B.slotCell, B.slotWithin,
+                                                       B.cellCount, ctl);
+    cellScanReduceKernel<<<tiles, kScanThreads, 0, st>>>(B.cellCount, total, B.partials, ctl);
+    cellScanApplyKernel<<<tiles, kScanThreads, 0, st>>>(B.cellCount, total, B.partials, cellStart, ctl);
+    cellPlaceKernel<<<blocksFor(n, 256), 256, 0, st>>>(n, B.slotCell, B.slotWithin, M.orig, cellStart, B.bucket, ctl);
+    cellRankKernel<<<blocksFor(n, 256), 256, 0, st>>>(n, B.bucket, B.slotCell, cellStart, B.perm, sortedCell, ctl);
 }
 
-int radixBlocks(int n) { return blocksFor(n, kRadixTile); }
-
-void launchRadixSort(int n, int bits, unsigned long long *keys, int *vals, unsigned long long *keysAlt, int *valsAlt,
-                     unsigned *counts, const Control *ctl, cudaStream_t st, unsigned long long **keysOut,
-                     int **valsOut)
-{
-    int blocks = radixBlocks(n);
-    unsigned long long *kin = keys, *kout = keysAlt;
-    int *vin = vals, *vout = valsAlt;
-    for (int shift = 0; shift < bits && n > 0; shift += 8) {
-        radixHistogramKernel<<<blocks, kRadixThreads, 0, st>>>(kin, n, shift, counts, blocks, ctl);
-        radixScanKernel<<<1, 1024, 0, st>>>(counts, 256 * blocks, ctl);
-        radixScatterKernel<<<blocks, kRadixThreads, 0, st>>>(kin, vin, n, shift, counts, blocks, kout, vout, ctl);
-        unsigned long long *tk = kin; kin = kout; kout = tk;
-        int *tv = vin; vin = vout; vout = tv;
-    }
-    *keysOut = kin;
-    *valsOut = vin;
-}
-
-void launchCellStart(const unsigned long long *sortedKeys, int n, int origBits, int numCells, int *cellStart,
-                     const Control *ctl, cudaStream_t st)
-{
-    cellStartKernel<<<blocksFor(numCells + 1, 256), 256, 0, st>>>(sortedKeys, n, origBits, numCells, cellStart, ctl);
-}
-
-void launchGather(const Params &P, int n, const int *perm, const unsigned long long *sortedKeys, int origBits,
-                  const MasterView &from, const MasterView &to, const Frame &F, const Control *ctl, cudaStream_t st)
+void launchGather(const Params &P, int n, const int *perm, const MasterView &from, const MasterView &to,
+                  const Frame &F, const Control *ctl, cudaStream_t st)
 {
     if (n == 0) return;
-    gatherKernel<<<blocksFor(n, 256), 256, 0, st>>>(P, n, perm, sortedKeys, origBits, from, to, F, ctl);
+    gatherKernel<<<blocksFor(n, 256), 256, 0, st>>>(P, n, perm, from, to, F, ctl);
 }
 
 void launchLoadFields(const Params &P, int n, const int *orig, const double *v, const double *rho, const double *p,

@@ -50,16 +50,19 @@ struct LaunchArgs {
 };
 
 void launchStage(const LaunchArgs &A, Stage stage);
-void launchCellKeys(const Params &P, int n, const MasterView &M, int origBits, unsigned long long *keys, int *vals,
-                    const Control *ctl, cudaStream_t st);
-int radixBlocks(int n);
-void launchRadixSort(int n, int bits, unsigned long long *keys, int *vals, unsigned long long *keysAlt, int *valsAlt,
-                     unsigned *counts, const Control *ctl, cudaStream_t st, unsigned long long **keysOut,
-                     int **valsOut);
-void launchCellStart(const unsigned long long *sortedKeys, int n, int origBits, int numCells, int *cellStart,
-                     const Control *ctl, cudaStream_t st);
-void launchGather(const Params &P, int n, const int *perm, const unsigned long long *sortedKeys, int origBits,
-                  const MasterView &from, const MasterView &to, const Frame &F, const Control *ctl, cudaStream_t st);
+// The counting sort's scratch: slotCell, slotWithin, perm (n entries), bucket (n pairs), cellCount
+// (numCells + 1 entries, all zero between sorts), partials (scanTiles(numCells + 1) entries).
+struct CellSortBuffers {
+    int *slotCell, *slotWithin, *perm, *cellCount, *partials;
+    int2 *bucket;
+};
+int scanTiles(int total);
+// Sorts the slots of M by (cell, caller index): cellStart (numCells + 1 lower bounds), perm and the
+// sorted slots' cells.
+void launchCellSort(const Params &P, int n, const MasterView &M, const CellSortBuffers &B, int *cellStart,
+                    int *sortedCell, const Control *ctl, cudaStream_t st);
+void launchGather(const Params &P, int n, const int *perm, const MasterView &from, const MasterView &to,
+                  const Frame &F, const Control *ctl, cudaStream_t st);
 void launchLoadFields(const Params &P, int n, const int *orig, const double *v, const double *rho, const double *p,
                       double deviationReference, const Frame &F, cudaStream_t st);
 void launchLoadMaster(int n, int dim, const double *x, const double *v, const double *rho, const double *m,

@@ -57,13 +57,6 @@ double sigmaUnit(int kind, int dim)
     return dim == 2 ? 10.0 / (7.0 * pi) : 1.0 / pi;
 }
 
-int bitsFor(long long value)
-{
-    int bits = 1;
-    while ((1ll << bits) <= value) ++bits;
-    return bits;
-}
-
 template <class T>
 int deviceAlloc(T **ptr, size_t count)
 {
@@ -119,9 +112,7 @@ struct SphSystem {
     float4 *aux = nullptr;
     float *pres = nullptr, *rate = nullptr, *scalar = nullptr;
     int *cell = nullptr, *cellStart = nullptr;
-    unsigned long long *keys[2] = {nullptr, nullptr};
-    int *vals[2] = {nullptr, nullptr};
-    unsigned *counts = nullptr;
+    CellSortBuffers sortBuffers = {};
     double *blockMaxima = nullptr;
     Control *ctl = nullptr;
     // Caller-order float64 staging on the device, kStageSlots rows of capacity doubles:
@@ -166,11 +157,9 @@ struct SphSystem {
             for (int a = 0; a < 3; ++a) { cudaFree(M.x[a]); cudaFree(M.v[a]); }
             cudaFree(M.rho); cudaFree(M.m); cudaFree(M.h); cudaFree(M.fluid); cudaFree(M.orig);
             M = MasterView{};
-            cudaFree(keys[b]); cudaFree(vals[b]);
-            keys[b] = nullptr; vals[b] = nullptr;
         }
         void *ptrs[] = {pa, pb, kin, G[0], G[1], G[2], L[0], L[1], L[2], gradRho, acc, vec, aux, pres, rate, scalar, cell,
-                        counts, blockMaxima, dStage, dStageU8, dRank, nbr, ncount};
+                        sortBuffers.slotCell, sortBuffers.slotWithin, sortBuffers.perm, sortBuffers.bucket, blockMaxima, dStage, dStageU8, dRank, nbr, ncount};
         for (void *p : ptrs) cudaFree(p);
         nbr = ncount = nullptr;
         nbrEntries = 0;
@@ -178,7 +167,9 @@ struct SphSystem {
         listDirty = true;
         pa = pb = kin = gradRho = acc = vec = nullptr;
         for (int a = 0; a < 3; ++a) G[a] = L[a] = nullptr;
-        aux = nullptr; pres = rate = scalar = nullptr; cell = nullptr; counts = nullptr; blockMaxima = nullptr;
+        aux = nullptr; pres = rate = scalar = nullptr; cell = nullptr; blockMaxima = nullptr;
+        sortBuffers.slotCell = sortBuffers.slotWithin = sortBuffers.perm = nullptr;
+        sortBuffers.bucket = nullptr;
         dStage = nullptr; dStageU8 = nullptr; dRank = nullptr;
         capacity = 0;
         return SPH_OK;
@@ -244,8 +235,10 @@ struct SphSystem {
         TRY(deviceAlloc(&rate, cap));
         TRY(deviceAlloc(&scalar, cap));
         TRY(deviceAlloc(&cell, cap));
-        for (int b = 0; b < 2; ++b) { TRY(deviceAlloc(&keys[b], cap)); TRY(deviceAlloc(&vals[b], cap)); }
-        TRY(deviceAlloc(&counts, (size_t)256 * radixBlocks(cap)));
+        TRY(deviceAlloc(&sortBuffers.slotCell, cap));
+        TRY(deviceAlloc(&sortBuffers.slotWithin, cap));
+        TRY(deviceAlloc(&sortBuffers.perm, cap));
+        TRY(deviceAlloc(&sortBuffers.bucket, cap));
         // one (speed, acceleration) pair per block of the momentum sweep, at up to 4 threads a particle
         TRY(deviceAlloc(&blockMaxima, (size_t)2 * ((4ll * cap + kBlock - 1) / kBlock)));
         TRY(deviceAlloc(&dStage, (size_t)kStageSlots * cap));
@@ -289,7 +282,15 @@ struct SphSystem {
         numCells = (int)total;
         if (numCells + 1 > cellStartCapacity) {
             cudaFree(cellStart);
+            cudaFree(sortBuffers.cellCount);
+            cudaFree(sortBuffers.partials);
+            cellStart = sortBuffers.cellCount = sortBuffers.partials = nullptr;
+            cellStartCapacity = 0;
             TRY(deviceAlloc(&cellStart, numCells + 1));
+            TRY(deviceAlloc(&sortBuffers.cellCount, numCells + 1));
+            TRY(deviceAlloc(&sortBuffers.partials, scanTiles(numCells + 1)));
+            // the counts are zero between sorts: each sort's scan clears what its count added
+            CUDA_TRY(cudaMemsetAsync(sortBuffers.cellCount, 0, sizeof(int) * (numCells + 1), stream));
             cellStartCapacity = numCells + 1;
         }
         // the reference's hash grid shape (src/pysurf/sphGpu.py:1466-1478)
@@ -387,20 +388,13 @@ struct SphSystem {
     {
         if (n == 0) return;
         Params P = params();
-        int origBits = bitsFor(std::max(n - 1, 1));
-        int cellBits = bitsFor(std::max(numCells - 1, 1));
-        int bits = origBits + cellBits;
-        launchCellKeys(P, n, master[cur], origBits, keys[0], vals[0], control, stream);
-        unsigned long long *sortedKeys;
-        int *perm;
-        launchRadixSort(n, bits, keys[0], vals[0], keys[1], vals[1], counts, control, stream, &sortedKeys, &perm);
-        launchCellStart(sortedKeys, n, origBits, numCells, cellStart, control, stream);
+        launchCellSort(P, n, master[cur], sortBuffers, cellStart, cell, control, stream);
         int next = 1 - cur;
         Frame F = frame();
         const MasterView &to = master[next];
         for (int a = 0; a < 3; ++a) { F.x[a] = to.x[a]; F.v[a] = to.v[a]; }
         F.rho = to.rho; F.m = to.m; F.h = to.h; F.fluid = to.fluid; F.orig = to.orig;
-        launchGather(P, n, perm, sortedKeys, origBits, master[cur], to, F, control, stream);
+        launchGather(P, n, sortBuffers.perm, master[cur], to, F, control, stream);
         cur = next;
         framed = true;
         cellsFresh = true;
@@ -572,6 +566,8 @@ int sph_destroy(SphSystem *sys)
     }
     sys->freeArrays();
     cudaFree(sys->cellStart);
+    cudaFree(sys->sortBuffers.cellCount);
+    cudaFree(sys->sortBuffers.partials);
     cudaFree(sys->dMaxCount);
     cudaFree(sys->ctl);
     cudaFree(sys->bedX);
