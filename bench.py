@@ -47,7 +47,7 @@ def parseArgs():
     p.add_argument('--impl', default='b200', choices=['b200', 'reference'])
     p.add_argument('--ppd', type=int, default=64)
     p.add_argument('--cells', type=int, default=None, help='cells per kernel support in the device cell list')
-    p.add_argument('--threads', type=int, default=None, help='threads per particle in the sweeps (1, 2, 4)')
+    p.add_argument('--threads', type=int, default=None, help='threads per particle in the sweeps (1, 2, 4, 8)')
     p.add_argument('--no-table', action='store_true', help='walk the cells in every sweep (no neighbour table)')
     p.add_argument('--no-e2e', action='store_true')
     p.add_argument('--no-cpu', action='store_true')

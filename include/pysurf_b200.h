@@ -60,7 +60,7 @@ int sph_set_cells_per_support(SphSystem *sys, int cells);
  * once, after the cell list, in a table sized to the largest count seen at push/update plus a
  * quarter, when it fits in half the free device memory; a particle whose count outgrows its row
  * walks the cells, with the same summation order.  0 always walks the cells.
- * threads_per_particle 1, 2 or 4 threads share each particle's neighbours (sums combined by
+ * threads_per_particle 1, 2, 4 or 8 threads share each particle's neighbours (sums combined by
  * shuffles in a fixed order). */
 int sph_set_sweep_options(SphSystem *sys, int neighbor_table, int threads_per_particle);
 /* The neighbour table's row capacity now (0: the sweeps walk the cells). */

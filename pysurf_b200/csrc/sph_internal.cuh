@@ -26,6 +26,12 @@
 namespace sph {
 
 constexpr int kBlock = 128;                 // threads per sweep block
+#ifndef SPH_SWEEP_MIN_BLOCKS
+#define SPH_SWEEP_MIN_BLOCKS 8
+#endif
+// resident sweep blocks an SM: 8 blocks of 128 caps a sweep at 64 registers, for the warps that hide
+// its neighbours' load latency
+constexpr int kSweepMinBlocks = SPH_SWEEP_MIN_BLOCKS;
 constexpr float kViscositySoftening = 0.01f;   // mu_ij's r^2 + 0.01 h^2 (src/pysurf/sphSolver.py:213)
 constexpr float kCloseDistance = 0.3f;      // limiter fade (src/pysurf/sphSolver.py:220-221)
 constexpr float kFoldWidth = 0.2f;
@@ -68,8 +74,8 @@ struct Params {
     int wallExtrapolated;
     float xsphEpsilon;
     double gravity64[3];
-    // neighbour table: up to listCap entries a particle, entry k of slot i at k * listStride + i;
-    // listCap 0: no table, the sweeps walk the cells
+    // neighbour table: up to listCap entries a particle (a multiple of 4), entry k of slot i at
+    // 4 ((k / 4) listStride + i) + k % 4; listCap 0: no table, the sweeps walk the cells
     int listCap;
     int listStride;
 };
@@ -87,7 +93,7 @@ struct Frame {
     float *rate;            // d rho / dt
     float *scalar;          // scratch per particle (Shepard, wall pressure outputs)
     float4 *vec;            // scratch per particle (XSPH transport velocity)
-    int *nbr;               // neighbour table (column-major), top bit: a pair across the periodic seam
+    int *nbr;               // neighbour table (chunks of four), top bit: a pair across the periodic seam
     int *ncount;            // each slot's neighbour count (may exceed the table's capacity)
     // master (current buffers)
     double *x[3], *v[3], *rho, *m, *h;
@@ -236,6 +242,36 @@ template <> __device__ __forceinline__ float volumeOf<3>(const Frame &F, int j) 
 template <int D> __device__ __forceinline__ float densityOf(const Frame &F, int j);
 template <> __device__ __forceinline__ float densityOf<2>(const Frame &F, int j) { return __ldg(&F.kin[j].z); }
 template <> __device__ __forceinline__ float densityOf<3>(const Frame &F, int j) { return __ldg(&F.kin[j].w); }
+
+// A neighbour's values from its rows, each row loaded once a pair: pa (A), pb (B), kin (K) and, in
+// 3D, aux (X).
+template <int D> __device__ __forceinline__ float4 auxRow(const Frame &F, int j)
+{
+    return D == 3 ? __ldg(&F.aux[j]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+template <int D> __device__ __forceinline__ float signedLengthIn(const float4 &A, const float4 &B)
+{ return D == 2 ? B.y : A.w; }
+template <int D> __device__ __forceinline__ float massIn(const float4 &B) { return D == 2 ? B.x : B.w; }
+template <int D> __device__ __forceinline__ float volumeIn(const float4 &B, const float4 &X)
+{ return D == 2 ? B.w : X.z; }
+template <int D> __device__ __forceinline__ float deviationIn(const float4 &B, const float4 &X)
+{ return D == 2 ? B.z : X.y; }
+template <int D> __device__ __forceinline__ float densityIn(const float4 &K) { return D == 2 ? K.z : K.w; }
+template <int D> __device__ __forceinline__ float pressureRatioIn(const float4 &K, const float4 &X)
+{ return D == 2 ? K.w : X.x; }
+template <int D> __device__ __forceinline__ void pointIn(const float4 &A, float p[3])
+{
+    p[0] = A.x; p[1] = A.y; p[2] = D == 3 ? A.z : 0.0f;
+}
+template <int D> __device__ __forceinline__ void remainderIn(const float4 &A, const float4 &B, float l[3])
+{
+    if (D == 2) { l[0] = A.z; l[1] = A.w; l[2] = 0.0f; }
+    else { l[0] = B.x; l[1] = B.y; l[2] = B.z; }
+}
+template <int D> __device__ __forceinline__ void velocityIn(const float4 &K, float v[3])
+{
+    v[0] = K.x; v[1] = K.y; v[2] = D == 3 ? K.z : 0.0f;
+}
 
 // Write a slot's density-derived fields: rho, rho - rho0, V = m / rho, p, p / rho^2.
 template <int D>

@@ -45,7 +45,7 @@ struct LaunchArgs {
     int wantG, wantL, wantRho;
     float floorDet;
     const float *densities; // Xsph: the densities it divides by; null for the frame's
-    int threads;            // threads per particle in the sweeps: 1, 2 or 4
+    int threads;            // threads per particle in the sweeps: 1, 2, 4 or 8
     int *maxCount;          // List: the largest neighbour count goes here (atomic max), when given
 };
 

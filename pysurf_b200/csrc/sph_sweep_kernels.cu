@@ -28,30 +28,76 @@ namespace sph {
 // The neighbour table
 // ------------------------------------------------------------------------------------------
 
-struct RecordVisit {
-    static constexpr bool kSkipCoincident = false;
-    int *column;
-    int stride, cap, count;
-    __device__ bool accept(bool) const { return true; }
-    __device__ void operator()(int j, const float *, float, float, bool, int image)
-    {
-        if (count < cap) column[(size_t)count * stride] = image ? (j | (int)0x80000000) : j;
-        ++count;
-    }
-};
-
-// Each slot's neighbours in the walk's order; the count is the whole count even when the row is
-// full (the sweeps then walk the cells for that slot).  maxCount: the largest count, when given.
-template <int D>
+// Each slot's neighbours in the walk's order (forEachNeighbour's, with its tests), from a group of
+// L lanes: lane t tests candidates t, t + L, ... of each run of the stencil, and the group's ballot
+// places the accepted ones in order.  The count is the whole count even when the row is full (the
+// sweeps then walk the cells for that slot).  maxCount: the largest count, when given.
+template <int D, int L>
 __global__ void __launch_bounds__(kBlock) listKernel(Params P, Frame F, const Control *ctl, int *maxCount)
 {
     if (ctl && !ctl->active) return;
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= P.n) return;
-    RecordVisit visit{F.nbr + i, P.listStride, P.listCap, 0};
-    forEachNeighbour<D, 1>(P, F, i, 0, fabsf(signedLength<D>(F, i)), visit, false);
-    F.ncount[i] = visit.count;
-    if (maxCount) atomicMax(maxCount, visit.count);
+    const Group<L> G = groupOf<L>();
+    const int i = G.i;
+    if (i >= P.n) return;           // a group's lanes share i, so groups leave whole
+    const int t = G.t;
+    const int shift = (threadIdx.x & 31) & ~(L - 1);
+    const unsigned lower = (1u << t) - 1u;
+    const float hI = fabsf(signedLength<D>(F, i));
+    float pi[3], li[3];
+    pointOf<D>(F, i, pi);
+    remainderOf<D>(F, i, li);
+    const float reach = P.mixedH ? hI + P.hMax : 2.0f * P.hMax;
+    const float limit = kCandidateMargin * reach * reach;
+    double shift64 = 0.0;
+    bool seam = false;
+    if (D == 3 && P.period > 0.0 && (pi[1] < reach || pi[1] > P.periodF - reach)) {
+        seam = true;
+        shift64 = pi[1] < 0.5f * P.periodF ? P.period : -P.period;
+    }
+    const int nx = P.nc[0], ny = P.nc[1], ncs = P.ncs;
+    const int c = F.cell[i];
+    const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
+    const int x0 = max(cx - ncs, 0), x1 = min(cx + ncs, nx - 1);
+    const int z0 = D == 3 ? max(cz - ncs, 0) : 0, z1 = D == 3 ? min(cz + ncs, P.nc[2] - 1) : 0;
+    const int cyImage = seam ? cellCoordinate((double)pi[1] + (double)li[1] + shift64, P.origin[1], P.cellWidth, ny) : cy;
+    int *column = F.nbr + 4 * (size_t)i;
+    int count = 0;
+    for (int image = 0; image < (seam ? 2 : 1); ++image) {
+        const int yc = image == 0 ? cy : cyImage;
+        const float offset = image ? (float)shift64 : 0.0f;
+        for (int zz = z0; zz <= z1; ++zz)
+            for (int yy = max(yc - ncs, 0); yy <= min(yc + ncs, ny - 1); ++yy) {
+                const int row = (zz * ny + yy) * nx;
+                const int first = __ldg(&F.cellStart[row + x0]), end = __ldg(&F.cellStart[row + x1 + 1]);
+                for (int base = first; base < end; base += L) {
+                    const int j = base + t;
+                    bool accepted = false;
+                    if (j < end && j != i) {
+                        const float4 A = __ldg(&F.pa[j]);
+                        float pj[3];
+                        pointIn<D>(A, pj);
+                        if (coarseDistance2<D>(pi, pj, offset) < limit) {
+                            const float4 B = D == 3 || P.mixedH ? __ldg(&F.pb[j]) : A;
+                            float lj[3], d[3];
+                            remainderIn<D>(A, B, lj);
+                            const float r2 = separation2<D>(P, pi, li, pj, lj, offset, image, shift64, d);
+                            const float h = P.mixedH ? 0.5f * (hI + fabsf(signedLengthIn<D>(A, B))) : P.hMax;
+                            accepted = r2 < support2(h);
+                        }
+                    }
+                    const unsigned bits = (__ballot_sync(G.mask, accepted) >> shift) & ((L >= 32 ? 0u : 1u << L) - 1u);
+                    if (accepted) {
+                        const int k = count + __popc(bits & lower);
+                        if (k < P.listCap)
+                            column[((size_t)(k >> 2) * P.listStride) * 4 + (k & 3)] = image ? (j | (int)0x80000000) : j;
+                    }
+                    count += __popc(bits);
+                }
+            }
+    }
+    if (t != 0) return;
+    F.ncount[i] = count;
+    if (maxCount) atomicMax(maxCount, count);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -73,17 +119,18 @@ struct ShepardVisit {
     Smoothing<K, D> S;
     float num, den;
     __device__ bool accept(bool) const { return true; }
-    __device__ void operator()(int j, const float *, float r, float h, bool, int)
+    __device__ void operator()(int j, const float *, float r, float h, bool, int, const float4 &B)
     {
         const KernelAt k = S.at(h);
+        const float4 X = auxRow<D>(F, j);
         float w = kernelValue<K>(r * k.invH, k);
-        num += massOf<D>(F, j) * w;
-        den += volumeOf<D>(F, j) * w;
+        num += massIn<D>(B) * w;
+        den += volumeIn<D>(B, X) * w;
     }
 };
 
 template <int D, int K, int T>
-__global__ void __launch_bounds__(kBlock) shepardKernel(Params P, Frame F, const Control *ctl)
+__global__ void __launch_bounds__(kBlock, kSweepMinBlocks) shepardKernel(Params P, Frame F, const Control *ctl)
 {
     if (!filterDue(ctl)) return;
     const Group<T> G = groupOf<T>();
@@ -125,7 +172,7 @@ struct WallVisit {
     Smoothing<K, D> S;
     float weight, total;
     __device__ bool accept(bool fluidJ) const { return fluidJ; }
-    __device__ void operator()(int j, const float *d, float r, float h, bool, int)
+    __device__ void operator()(int j, const float *d, float r, float h, bool, int, const float4 &)
     {
         const KernelAt k = S.at(h);
         float w = kernelValue<K>(r * k.invH, k);
@@ -138,7 +185,8 @@ struct WallVisit {
 // Boundary rows only write their own entries and only fluid entries are read, so the frame is
 // updated in place.  writeDensity: the master float64 density takes Tait^-1(p_w) too.
 template <int D, int K, int T>
-__global__ void __launch_bounds__(kBlock) wallPressureKernel(Params P, Frame F, const Control *ctl, int writeDensity)
+__global__ void __launch_bounds__(kBlock, kSweepMinBlocks)
+wallPressureKernel(Params P, Frame F, const Control *ctl, int writeDensity)
 {
     if (ctl && !ctl->active) return;
     const Group<T> G = groupOf<T>();
@@ -179,10 +227,11 @@ struct GradientVisit {
     float vi[3], devI;
     float S[3][3], Mf[3][3], M[3][3], gsum[3];
     __device__ bool accept(bool) const { return true; }
-    __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int)
+    __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int, const float4 &B)
     {
         const KernelAt k = kernel.at(h);
-        float w = volumeOf<D>(F, j) * kernelGradient<K>(r * k.invH, k);
+        const float4 X = auxRow<D>(F, j);
+        float w = volumeIn<D>(B, X) * kernelGradient<K>(r * k.invH, k);
         if (wantG && fluidJ) {
             float vj[3];
             velocityOf<D>(F, j, vj);
@@ -196,7 +245,7 @@ struct GradientVisit {
             for (int a = 0; a < D; ++a)
                 for (int b = 0; b < D; ++b) M[a][b] += -w * d[a] * d[b];
         if (wantRho) {
-            float t = w * (deviationOf<D>(F, j) - devI);
+            float t = w * (deviationIn<D>(B, X) - devI);
             for (int a = 0; a < D; ++a) gsum[a] += t * d[a];
         }
     }
@@ -210,7 +259,7 @@ __device__ __forceinline__ void groupSumMatrix(float M[3][3], unsigned mask)
 }
 
 template <int D, int K, int T>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, kSweepMinBlocks)
 gradientKernel(Params P, Frame F, const Control *ctl, int wantG, int wantL, int wantRho, float floorDet)
 {
     if (ctl && !ctl->active) return;
@@ -280,12 +329,13 @@ struct MomentumVisit {
     float Gi[3][3];
     float total[3];
     __device__ bool accept(bool) const { return true; }
-    __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int)
+    __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int, const float4 &B)
     {
         const KernelAt k = S.at(h);
         const float q = r * k.invH;
+        const float4 Kj = __ldg(&F.kin[j]);
         float vj[3];
-        velocityOf<D>(F, j, vj);
+        velocityIn<D>(Kj, vj);
         float rel[3] = {vi[0] - vj[0], vi[1] - vj[1], vi[2] - vj[2]};
         float approach = rel[0] * d[0] + rel[1] * d[1] + (D == 3 ? rel[2] * d[2] : 0.0f);
         float viscosity = 0.0f;
@@ -316,10 +366,11 @@ struct MomentumVisit {
             // -alpha c0 h (v_ij . r_ij) / ((r^2 + 0.01 h^2) (rho_i + rho_j) / 2); the denominator is
             // a positive normal float for any physical pair, which __fdividef takes to 2 ulp
             viscosity = __fdividef(viscosityScale * h * approach,
-                                   (r * r + k.soft) * (0.5f * (rhoI + densityOf<D>(F, j))));
+                                   (r * r + k.soft) * (0.5f * (rhoI + densityIn<D>(Kj))));
             if (!fluidJ) viscosity *= P.boundaryFactor;
         }
-        float coefficient = -(own + pressureRatioOf<D>(F, j) + viscosity) * massOf<D>(F, j);
+        const float ratioJ = D == 2 ? Kj.w : __ldg(&F.aux[j].x);
+        float coefficient = -(own + ratioJ + viscosity) * massIn<D>(B);
         float f = coefficient * kernelGradient<K>(q, k);
         for (int a = 0; a < D; ++a) total[a] += f * d[a];
     }
@@ -347,7 +398,8 @@ __device__ __forceinline__ double cflTimeStep(double h, double c0, double vmax, 
 }
 
 template <int D, int K, int T>
-__global__ void __launch_bounds__(kBlock) momentumKernel(Params P, Frame F, Control *ctl, double *blockMaxima)
+__global__ void __launch_bounds__(kBlock, kSweepMinBlocks)
+momentumKernel(Params P, Frame F, Control *ctl, double *blockMaxima)
 {
     __shared__ double shared[kBlock / 32];
     __shared__ bool last;
@@ -468,7 +520,7 @@ struct ContinuityVisit {
     float vi[3], devI, Li[3][3], gi[3];
     float total;
     __device__ bool accept(bool fluidJ) const { return !(boundaryI && !fluidJ); }
-    __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int)
+    __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int, const float4 &B)
     {
         const KernelAt k = S.at(h);
         const float grad = kernelGradient<K>(r * k.invH, k);    // (dW/dr) / r
@@ -484,9 +536,10 @@ struct ContinuityVisit {
         } else {
             for (int a = 0; a < D; ++a) dot += (vi[a] - vj[a]) * d[a];
         }
-        total += massOf<D>(F, j) * dot * grad;
+        total += massIn<D>(B) * dot * grad;
         if (diffuses && fluidJ) {
-            float devJ = deviationOf<D>(F, j);
+            const float4 X = auxRow<D>(F, j);
+            float devJ = deviationIn<D>(B, X);
             float difference = devJ - devI;
             if (P.diffusion == 2) {
                 float ratio = 1.0f + 0.5f * (devI + devJ) / P.rho0F;
@@ -501,7 +554,7 @@ struct ContinuityVisit {
             }
             // 2 delta c0 h V_j (difference) (-(dW/dr) r) / (r^2 + 0.01 h^2), with (dW/dr) r = grad r^2
             const float r2 = r * r;
-            total += P.diffusionFactor * h * volumeOf<D>(F, j) * difference * (-grad)
+            total += P.diffusionFactor * h * volumeIn<D>(B, X) * difference * (-grad)
                    * __fdividef(r2, r2 + k.soft);
         }
     }
@@ -509,7 +562,8 @@ struct ContinuityVisit {
 
 // mode 0: the rate only; 1: advance the density; 2: advance, drift and enforce.
 template <int D, int K, int T>
-__global__ void __launch_bounds__(kBlock) continuityKernel(Params P, Frame F, Control *ctl, Enforcement E, int mode)
+__global__ void __launch_bounds__(kBlock, kSweepMinBlocks)
+continuityKernel(Params P, Frame F, Control *ctl, Enforcement E, int mode)
 {
     if (ctl && !ctl->active) return;
     const Group<T> G = groupOf<T>();
@@ -554,12 +608,12 @@ struct XsphVisit {
     Smoothing<K, D> S;
     float vi[3], rhoI, corr[3];
     __device__ bool accept(bool fluidJ) const { return fluidJ; }
-    __device__ void operator()(int j, const float *, float r, float h, bool, int)
+    __device__ void operator()(int j, const float *, float r, float h, bool, int, const float4 &B)
     {
         const KernelAt k = S.at(h);
         float w = kernelValue<K>(r * k.invH, k);
         float rhoJ = densities ? densities[j] : densityOf<D>(F, j);
-        float weight = massOf<D>(F, j) * w / (0.5f * (rhoI + rhoJ));
+        float weight = massIn<D>(B) * w / (0.5f * (rhoI + rhoJ));
         float vj[3];
         velocityOf<D>(F, j, vj);
         for (int a = 0; a < D; ++a) corr[a] += weight * (vj[a] - vi[a]);
@@ -569,7 +623,7 @@ struct XsphVisit {
 // densities: the float32 densities the sum divides by (null: the frame's).  mode 0: the transport
 // velocity into F.vec only; 2: drift with it and enforce.
 template <int D, int K, int T>
-__global__ void __launch_bounds__(kBlock)
+__global__ void __launch_bounds__(kBlock, kSweepMinBlocks)
 xsphKernel(Params P, Frame F, Control *ctl, Enforcement E, const float *densities, int mode)
 {
     if (ctl && !ctl->active) return;
@@ -604,6 +658,12 @@ xsphKernel(Params P, Frame F, Control *ctl, Enforcement E, const float *densitie
 
 static inline int blocksFor(long long n, int block) { return (int)((n + block - 1) / block); }
 
+#ifndef SPH_LIST_LANES_2D
+#define SPH_LIST_LANES_2D 8
+#endif
+constexpr int kListLanes2 = SPH_LIST_LANES_2D;
+constexpr int kListLanes3 = 4;
+
 template <int D, int K, int T>
 static void launchT(const LaunchArgs &A, Stage stage)
 {
@@ -624,8 +684,11 @@ static void launchT(const LaunchArgs &A, Stage stage)
     case Stage::Continuity: continuityKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.flag); break;
     case Stage::Xsph: xsphKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.densities, A.flag); break;
     case Stage::List:
-        if (D == 2) listKernel<2><<<pointwise, kBlock, 0, st>>>(P, F, A.ctl, A.maxCount);
-        else listKernel<3><<<pointwise, kBlock, 0, st>>>(P, F, A.ctl, A.maxCount);
+        // lanes a slot for the table: the 2D stencil's runs are longer
+        if (D == 2) listKernel<2, kListLanes2><<<blocksFor((long long)P.n * kListLanes2, kBlock), kBlock, 0, st>>>(
+            P, F, A.ctl, A.maxCount);
+        else listKernel<3, kListLanes3><<<blocksFor((long long)P.n * kListLanes3, kBlock), kBlock, 0, st>>>(
+            P, F, A.ctl, A.maxCount);
         break;
     }
 }
@@ -633,7 +696,8 @@ static void launchT(const LaunchArgs &A, Stage stage)
 template <int D, int K>
 static void launchDK(const LaunchArgs &A, Stage stage)
 {
-    if (A.threads >= 4) launchT<D, K, 4>(A, stage);
+    if (A.threads >= 8) launchT<D, K, 8>(A, stage);
+    else if (A.threads == 4) launchT<D, K, 4>(A, stage);
     else if (A.threads == 2) launchT<D, K, 2>(A, stage);
     else launchT<D, K, 1>(A, stage);
 }

@@ -7,15 +7,17 @@
 // precise separation (hi_i - hi_j) + (lo_i - lo_j).
 //
 // Each step the table kernel walks the cells once and records, per particle, the neighbours the
-// walk accepts, in the walk's order, in a column-major table (entry k of particle i at
-// k * stride + i, so a warp's reads of entry k are contiguous).  The sweeps then read the table
+// walk accepts, in the walk's order, in a table of 16-byte chunks: entries 4c .. 4c + 3 of particle
+// i form chunk c, stored at c * stride + i, so a lane takes four neighbours with one load and a
+// warp's loads of chunk c are contiguous.  The sweeps then read the table
 // instead of walking the cells: no candidate that fails the distance test is visited again, so
 // a warp's lanes stay busy.  A particle with more neighbours than its row holds walks the cells
 // instead.  Table and walk feed one loop body, the visitor called from one place, so a sweep
 // gives the same bits either way.
 //
-// T threads serve one particle: lane t of the group takes the particle's neighbours t, t + T,
-// t + 2T, ... (counted in the walk's order), and the group sums its partial sums with a
+// T threads serve one particle: lane t of the group takes the particle's neighbours in chunks t,
+// t + T, t + 2T, ... (neighbour k, counted in the walk's order, is in chunk k / 4), and the group
+// sums its partial sums with a
 // butterfly of shuffles, which gives every lane the same bits (each level adds two values whose
 // order does not matter).  T = 1 is the plain one-thread-per-particle sweep.
 //
@@ -60,13 +62,62 @@ __device__ __forceinline__ float groupSum(float value, unsigned mask)
     return value;
 }
 
+// The coarse test's squared distance between float32 points, and a pair's separation and squared
+// distance.  Each takes its roundings from explicit intrinsics, so that the table kernel and the
+// walk, compiled apart, reach the same decision on a pair at the edge of the support.  The support
+// test is r^2 < (2 h)^2, so a rejected candidate takes no square root; it parts from the
+// reference's r < 2 h only where the two roundings straddle 2 h, where W and grad W vanish.
+template <int D>
+__device__ __forceinline__ float coarseDistance2(const float pi[3], const float pj[3], float offset)
+{
+    const float cx = __fsub_rn(pi[0], pj[0]), cy = __fsub_rn(__fadd_rn(pi[1], offset), pj[1]);
+    float r2 = __fadd_rn(__fmul_rn(cx, cx), __fmul_rn(cy, cy));
+    if (D == 3) {
+        const float cz = __fsub_rn(pi[2], pj[2]);
+        r2 = __fadd_rn(r2, __fmul_rn(cz, cz));
+    }
+    return r2;
+}
+
+// d = x_i - x_j from the points and remainders (image: across the periodic seam, in float64); r^2.
+template <int D>
+__device__ __forceinline__ float separation2(const Params &P, const float pi[3], const float li[3], const float pj[3],
+                                            const float lj[3], float offset, int image, double shift64, float d[3])
+{
+    if (!P.precise) {
+        // separationPrecision 'float32': the points alone (src/pysurf/sphGpu.py:227-242)
+        d[0] = __fsub_rn(pi[0], pj[0]);
+        d[1] = __fsub_rn(__fadd_rn(pi[1], offset), pj[1]);
+        d[2] = D == 3 ? __fsub_rn(pi[2], pj[2]) : 0.0f;
+    } else if (!image) {
+        for (int a = 0; a < D; ++a) d[a] = __fadd_rn(__fsub_rn(pi[a], pj[a]), __fsub_rn(li[a], lj[a]));
+        if (D == 2) d[2] = 0.0f;
+    } else {
+        for (int a = 0; a < D; ++a)
+            d[a] = (float)(((double)pi[a] + (double)li[a]) - ((double)pj[a] + (double)lj[a]));
+        d[1] = (float)((((double)pi[1] + (double)li[1]) + shift64) - ((double)pj[1] + (double)lj[1]));
+        if (D == 2) d[2] = 0.0f;
+    }
+    float r2 = __fadd_rn(__fmul_rn(d[0], d[0]), __fmul_rn(d[1], d[1]));
+    if (D == 3) r2 = __fadd_rn(r2, __fmul_rn(d[2], d[2]));
+    return r2;
+}
+
+// (2 h)^2, the support test's bound.
+__device__ __forceinline__ float support2(float h)
+{
+    const float w = __fmul_rn(2.0f, h);
+    return __fmul_rn(w, w);
+}
+
 // The candidates of slot i, one at a time: its table row when the row holds them all, else the
 // cells of its stencil (then twice for an image search across a periodic seam).
 template <int D>
 struct Candidates {
     // table
-    const int *column;
+    const int4 *column;
     int stride, count, k, step;
+    int4 chunk;         // the entries still to visit of the current chunk, first in x
     // walk
     bool walking;
     int images, image, cyImage, cy, ncs, nx, ny, x0, x1, z0, z1, zz, yy, j, end;
@@ -92,8 +143,11 @@ struct Candidates {
     {
         if (!walking) {
             if (k >= count) return false;
-            const int entry = __ldg(column + (size_t)k * stride);
-            k += step;
+            if ((k & 3) == 0) chunk = __ldg(column + (size_t)(k >> 2) * stride);
+            const int entry = chunk.x;
+            chunk.x = chunk.y; chunk.y = chunk.z; chunk.z = chunk.w;
+            // the chunk's last entry passes to this lane's next chunk
+            k = (k & 3) == 3 ? k + 1 + 4 * (step - 1) : k + 1;
             jOut = entry & 0x7FFFFFFF;
             imageOut = entry < 0 ? 1 : 0;
             return true;
@@ -121,10 +175,10 @@ struct Candidates {
     }
 };
 
-// Visit the neighbours of slot i.  Every neighbour j != i with r < 2 h_ij (the table's criterion)
-// is counted in the walk's order; lane t of T takes those whose count is t mod T (the table row
-// of a lane is read with step T from entry t).  Of those, the visitor gets (j, d, r, h_ij, fluidJ,
-// image) when Visitor::accept(fluidJ), and r >= 1e-12 where Visitor::kSkipCoincident.
+// Visit the neighbours of slot i.  Every neighbour j != i with r^2 < (2 h_ij)^2 (the table's
+// criterion) is counted in the walk's order; lane t of T takes those whose count k has k / 4 = t
+// mod T (the table's chunks t, t + T, ...).  Of those, the visitor gets (j, d, r, h_ij, fluidJ,
+// image, pb row of j) when Visitor::accept(fluidJ), and r >= 1e-12 where Visitor::kSkipCoincident.
 // useTable: false forces the walk (the table kernel itself).
 template <int D, int T, class Visitor>
 __device__ __forceinline__ void forEachNeighbour(const Params &P, const Frame &F, int i, int t, float hI,
@@ -146,10 +200,10 @@ __device__ __forceinline__ void forEachNeighbour(const Params &P, const Frame &F
     const int count = useTable && P.listCap > 0 ? __ldg(&F.ncount[i]) : 0;
     C.walking = !(useTable && P.listCap > 0 && count <= P.listCap);
     if (!C.walking) {
-        C.column = F.nbr + i;
+        C.column = reinterpret_cast<const int4 *>(F.nbr) + i;
         C.stride = P.listStride;
         C.count = count;
-        C.k = t;
+        C.k = 4 * t;
         C.step = T;
     } else {
         C.nx = P.nc[0];
@@ -173,46 +227,30 @@ __device__ __forceinline__ void forEachNeighbour(const Params &P, const Frame &F
     int counted = 0, j = 0, image = 0;
     while (C.next(j, image)) {
         const float offset = image ? (float)shift64 : 0.0f;     // the search's origin: particle or image
+        const float4 A = __ldg(&F.pa[j]);
         float pj[3];
-        pointOf<D>(F, j, pj);
-        if (C.walking) {
-            const float cxv = pi[0] - pj[0];
-            const float cyv = (pi[1] + offset) - pj[1];
-            const float czv = D == 3 ? pi[2] - pj[2] : 0.0f;
-            if (cxv * cxv + cyv * cyv + czv * czv >= limit || j == i) continue;
-        }
-        const float hs = signedLength<D>(F, j);
+        pointIn<D>(A, pj);
+        if (C.walking && (coarseDistance2<D>(pi, pj, offset) >= limit || j == i)) continue;
+        const float4 B = __ldg(&F.pb[j]);
+        const float hs = signedLengthIn<D>(A, B);
         const bool fluidJ = hs > 0.0f;
         // a lone lane may skip a rejected neighbour before its separation; a group counts every one
         if ((T == 1 || !C.walking) && !visit.accept(fluidJ)) continue;
         float lj[3];
-        remainderOf<D>(F, j, lj);
+        remainderIn<D>(A, B, lj);
         float d[3];
-        if (!P.precise) {
-            // separationPrecision 'float32': the points alone (src/pysurf/sphGpu.py:227-242)
-            d[0] = pi[0] - pj[0];
-            d[1] = (pi[1] + offset) - pj[1];
-            d[2] = D == 3 ? pi[2] - pj[2] : 0.0f;
-        } else if (!image) {
-            d[0] = (pi[0] - pj[0]) + (li[0] - lj[0]);
-            d[1] = (pi[1] - pj[1]) + (li[1] - lj[1]);
-            d[2] = D == 3 ? (pi[2] - pj[2]) + (li[2] - lj[2]) : 0.0f;
-        } else {
-            for (int a = 0; a < D; ++a)
-                d[a] = (float)(((double)pi[a] + (double)li[a]) - ((double)pj[a] + (double)lj[a]));
-            d[1] = (float)((((double)pi[1] + (double)li[1]) + shift64) - ((double)pj[1] + (double)lj[1]));
-        }
-        const float r = sqrtf(d[0] * d[0] + d[1] * d[1] + (D == 3 ? d[2] * d[2] : 0.0f));
+        const float r2 = separation2<D>(P, pi, li, pj, lj, offset, image, shift64, d);
         const float h = P.mixedH ? 0.5f * (hI + fabsf(hs)) : P.hMax;
         if (C.walking) {
-            if (r >= 2.0f * h) continue;
+            if (r2 >= support2(h)) continue;
             if (T > 1) {
-                if (counted++ % T != t) continue;
+                if ((counted++ >> 2) % T != t) continue;
                 if (!visit.accept(fluidJ)) continue;
             }
         }
+        const float r = __fsqrt_rn(r2);
         if (Visitor::kSkipCoincident && r < 1.0e-12f) continue;
-        visit(j, d, r, h, fluidJ, image);
+        visit(j, d, r, h, fluidJ, image, B);
     }
 }
 

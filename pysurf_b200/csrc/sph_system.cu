@@ -158,8 +158,9 @@ struct SphSystem {
             cudaFree(M.rho); cudaFree(M.m); cudaFree(M.h); cudaFree(M.fluid); cudaFree(M.orig);
             M = MasterView{};
         }
-        void *ptrs[] = {pa, pb, kin, G[0], G[1], G[2], L[0], L[1], L[2], gradRho, acc, vec, aux, pres, rate, scalar, cell,
-                        sortBuffers.slotCell, sortBuffers.slotWithin, sortBuffers.perm, sortBuffers.bucket, blockMaxima, dStage, dStageU8, dRank, nbr, ncount};
+        void *ptrs[] = {pa, pb, kin, G[0], G[1], G[2], L[0], L[1], L[2], gradRho, acc, vec, aux, pres, rate,
+                        scalar, cell, sortBuffers.slotCell, sortBuffers.slotWithin, sortBuffers.perm,
+                        sortBuffers.bucket, blockMaxima, dStage, dStageU8, dRank, nbr, ncount};
         for (void *p : ptrs) cudaFree(p);
         nbr = ncount = nullptr;
         nbrEntries = 0;
@@ -239,8 +240,8 @@ struct SphSystem {
         TRY(deviceAlloc(&sortBuffers.slotWithin, cap));
         TRY(deviceAlloc(&sortBuffers.perm, cap));
         TRY(deviceAlloc(&sortBuffers.bucket, cap));
-        // one (speed, acceleration) pair per block of the momentum sweep, at up to 4 threads a particle
-        TRY(deviceAlloc(&blockMaxima, (size_t)2 * ((4ll * cap + kBlock - 1) / kBlock)));
+        // one (speed, acceleration) pair per block of the momentum sweep, at up to 8 threads a particle
+        TRY(deviceAlloc(&blockMaxima, (size_t)2 * ((8ll * cap + kBlock - 1) / kBlock)));
         TRY(deviceAlloc(&dStage, (size_t)kStageSlots * cap));
         TRY(deviceAlloc(&dStageU8, cap));
         TRY(deviceAlloc(&dRank, cap));
@@ -600,8 +601,9 @@ int sph_set_sweep_options(SphSystem *sys, int neighbor_table, int threads_per_pa
 {
     CHECK_SYS(sys);
     if (neighbor_table != 0 && neighbor_table != 1) return fail(SPH_ERR_INVALID, "neighbor_table must be 0 or 1");
-    if (threads_per_particle != 1 && threads_per_particle != 2 && threads_per_particle != 4)
-        return fail(SPH_ERR_INVALID, "threads per particle must be 1, 2 or 4");
+    if (threads_per_particle != 1 && threads_per_particle != 2 && threads_per_particle != 4 &&
+        threads_per_particle != 8)
+        return fail(SPH_ERR_INVALID, "threads per particle must be 1, 2, 4 or 8");
     sys->tableMode = neighbor_table;
     sys->threads = threads_per_particle;
     sys->listDirty = true;

@@ -226,7 +226,7 @@ class PairSums:
 
     def setSweepOptions(self, neighborTable: bool = True, threadsPerParticle: int = 1) -> None:
         """Whether the sweeps read a per-step neighbour table (else they walk the cells; the sums are
-        the same bits either way), and how many threads (1, 2, 4) share each particle's neighbours."""
+        the same bits either way), and how many threads (1, 2, 4, 8) share each particle's neighbours."""
         check(self._lib.sph_set_sweep_options(self._handle, int(bool(neighborTable)), int(threadsPerParticle)),
               'setSweepOptions')
 

@@ -237,10 +237,10 @@ def test_height_field_enforcement():
 
 
 @pytest.mark.parametrize('tag', ['3d_p_wendlandC2', '2d_o_cubicSpline'])
-@pytest.mark.parametrize('threads', [1, 2, 4])
+@pytest.mark.parametrize('threads', [1, 2, 4, 8])
 @pytest.mark.parametrize('table', [True, False])
 def test_every_sweep_form_gives_the_reference_sums(tag, threads, table):
-    # the neighbour table on or off, one to four threads a particle: the same sums to float32 rounding
+    # the neighbour table on or off, one to eight threads a particle: the same sums to float32 rounding
     c = golden('clouds.npz', tag)
     dim = c['positions'].shape[1]
     g = np.zeros(dim)
