@@ -7,6 +7,8 @@ reference itself built (tests/golden/beach.npz).
     damBreak            a 1 x 2 m column in a 4 x 3 m tank, 3 wall layers, jittered lattice
     solitaryBeach       a first-order solitary wave over a plane beach, the deltaSph scheme
                         (src/pysurf/BreakingWave.py:658-760 with src/pysurf/waveMakers.py:282-329)
+    ridgeWave3D         a solitary wave crossing a Gaussian ridge at 25 degrees in a walled 3D tank
+                        (src/pysurf/BreakingWave3D.py:630-700, src/pysurf/sphBoundaries.py:498-595)
 
 Each returns a ``Case``: the particle state, the boundary, and the solver configuration the
 reference's ``SimulationConfig``/``WcsphSolver`` would hold for it.
@@ -18,7 +20,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from pysurf_b200.state import BedBoundary, ContainerBoundary, ParticleState, Profile
+from pysurf_b200.state import BedBoundary, ContainerBoundary, HeightFieldBoundary, HeightTable, ParticleState, Profile
 
 GRAVITY = 9.80665            # src/pysurf/constants.py:29
 FRESHWATER = 998.2           # src/pysurf/constants.py:33
@@ -251,6 +253,127 @@ def solitaryBeach(particlesPerDepth: int = 64, depth: float = 1.0, height: float
                 maxTimeStep=1.0,
                 info={'depth': depth, 'H/d': height / depth, 'crestX': crestX, 'toeX': toeX, 'slope': slope,
                       'length': length, 'ppd': particlesPerDepth, 'layers': layers})
+
+
+def gaussianRidge(depth: float = 1.0, ridgeHeight: float = 0.6, ridgeWidth: float = 3.0, angle: float = 25.0,
+                  length: float = 40.0, width: float = 10.0, ridgeX: float = 20.0):
+    """The bed z_b(x, y) = ridgeHeight d exp(-xi^2 / (2 sigma^2)) of a Gaussian ridge whose axis crosses
+    (ridgeX, width / 2) at `angle` degrees to the y axis (the crest line of a wave travelling along +x),
+    xi the distance from the axis (the bed of HeightField.fromFunction, src/pysurf/bathymetry.py:480-517).
+    Returns (elevation(x, y), gradient(x, y) -> (dz/dx, dz/dy))."""
+    a = math.radians(angle)
+    ca, sa = math.cos(a), math.sin(a)
+    peak, sigma2 = ridgeHeight * depth, (ridgeWidth * depth) ** 2
+
+    def distance(x, y):
+        return (np.asarray(x, dtype=float) - ridgeX) * ca - (np.asarray(y, dtype=float) - 0.5 * width) * sa
+
+    def elevation(x, y):
+        xi = distance(x, y)
+        return peak * np.exp(-xi * xi / (2.0 * sigma2))
+
+    def gradient(x, y):
+        xi = distance(x, y)
+        dz = -elevation(x, y) * xi / sigma2
+        return dz * ca, -dz * sa
+
+    return elevation, gradient
+
+
+def heightTable(elevation, bounds, gridSpacing: float, stillWaterLevel: float, padding: int = 2) -> HeightTable:
+    """A height field sampled on a grid `padding` cells past its bounds, as the device's cubic
+    convolution reads it (src/pysurf/bathymetry.py:480-517)."""
+    startX, endX, startY, endY = bounds
+    x = startX + gridSpacing * np.arange(-padding, int(math.ceil((endX - startX) / gridSpacing)) + padding + 1)
+    y = startY + gridSpacing * np.arange(-padding, int(math.ceil((endY - startY) / gridSpacing)) + padding + 1)
+    gx, gy = np.meshgrid(x, y, indexing='xy')
+    return HeightTable(x, y, elevation(gx, gy), tuple(bounds), stillWaterLevel)
+
+
+def heightFieldPositions(elevation, gradient, bounds, spacing: float, layers: int, wallTop: float,
+                         floor: float) -> np.ndarray:
+    """Boundary particles of a height-field tank (src/pysurf/sphBoundaries.py:498-595): the bed's layers
+    on the lattice's columns, each offset along the local normal by (layer + 1/2) s, then walls on all
+    four sides whose columns stand behind their planes at (layer + 1/2) s, on the fluid lattice's
+    heights from below the bed's deepest layer to `wallTop`; the side walls run past the end walls."""
+    startX, endX, startY, endY = bounds
+    xs = np.arange(startX + 0.5 * spacing, endX, spacing)
+    ys = np.arange(startY + 0.5 * spacing, endY, spacing)
+    gx, gy = (g.ravel() for g in np.meshgrid(xs, ys, indexing='xy'))
+    zx, zy = gradient(gx, gy)
+    norm = np.sqrt(1.0 + zx * zx + zy * zy)
+    normal = np.column_stack([-zx / norm, -zy / norm, 1.0 / norm])
+    surface = np.column_stack([gx, gy, elevation(gx, gy)])
+    blocks = [surface - (layer + 0.5) * spacing * normal for layer in range(layers)]
+    heights = np.arange(floor - (layers + 1) * spacing + 0.5 * spacing, wallTop, spacing)
+
+    def wall(lineX, lineY):
+        bottom = elevation(np.clip(lineX, startX, endX), np.clip(lineY, startY, endY)) - layers * spacing
+        x, y = np.repeat(lineX, heights.size), np.repeat(lineY, heights.size)
+        z = np.tile(heights, lineX.size)
+        keep = z > np.repeat(bottom, heights.size)
+        return np.column_stack([x[keep], y[keep], z[keep]])
+
+    offsets = (np.arange(layers) + 0.5) * spacing
+    for offset in offsets:
+        blocks.append(wall(np.full(ys.size, startX - offset), ys))
+        blocks.append(wall(np.full(ys.size, endX + offset), ys))
+    along = np.concatenate([startX - offsets[::-1], xs, endX + offsets])
+    for offset in offsets:
+        blocks.append(wall(along, np.full(along.size, startY - offset)))
+        blocks.append(wall(along, np.full(along.size, endY + offset)))
+    return np.vstack(blocks)
+
+
+def ridgeWave3D(particlesPerDepth: int = 32, depth: float = 1.0, height: float = 0.5, crestX: float = 8.0,
+                ridgeHeight: float = 0.6, ridgeWidth: float = 3.0, angle: float = 25.0, length: float = 40.0,
+                width: float = 10.0, ridgeX: float = 20.0, smoothingRatio: float = 3.0,
+                layers: int | None = None) -> Case:
+    """A first-order solitary wave of H/d = 0.5 crossing a Gaussian ridge (0.6 d high, sigma = 3 d, its axis
+    at 25 degrees to the crest) in a 40 d x 10 d tank with walls on all sides, 32 particles per depth, run
+    with the deltaSph scheme of src/pysurf/BreakingWave3D.py:656-662 (Wendland C2 at h = 3 dx, hydrostatic
+    diffusion, the continuity correction, extrapolated walls, the viscosity limiter, density floor 0.9 rho0).
+    The fluid fills the lattice's cells from the bed to the wave's surface (the layout of
+    src/pysurf/BreakingWave3D.py:630-700 without start packing); crest-zone splitting is a separate step."""
+    s = depth / particlesPerDepth
+    layers = max(3, math.ceil(2.0 * smoothingRatio - 1e-9)) if layers is None else layers
+    bounds = (0.0, length, 0.0, width)
+    elevation, gradient = gaussianRidge(depth, ridgeHeight, ridgeWidth, angle, length, width, ridgeX)
+    floor = 0.0
+    wallTop = depth + 3.0 * height
+    table = heightTable(elevation, bounds, 0.5 * s, depth)
+    boundary = HeightFieldBoundary(table, s, nLayers=layers, wallTop=wallTop)
+    # fluid: lattice cells from the bed to the surface d + eta(x)
+    xs = np.arange(0.5 * s, length, s)
+    ys = np.arange(0.5 * s, width, s)
+    zs = np.arange(floor + 0.5 * s, depth + height + s, s)
+    gx, gy, gz = (g.ravel() for g in np.meshgrid(xs, ys, zs, indexing='ij'))
+    bedZ = elevation(gx, gy)
+    surface = depth + solitaryWaveProfile(gx, height, depth, crestX)
+    keep = (gz >= bedZ + (0.5 - 1e-9) * s) & (gz < surface)
+    fluid = np.column_stack([gx[keep], gy[keep], gz[keep]])
+    x, z, bed = fluid[:, 0], fluid[:, 2], bedZ[keep]
+    celerity = solitaryWaveSpeed(height, depth)
+    kappa = solitaryWaveDecay(height, depth)
+    eta = solitaryWaveProfile(x, height, depth, crestX)
+    etaSlope = -2.0 * kappa * eta * np.tanh(kappa * (x - crestX))
+    u = celerity * eta / (depth + eta)
+    w = -(z - bed) * celerity * depth * etaSlope / (depth + eta) ** 2
+    velocities = np.column_stack([u, np.zeros_like(u), w])
+    rho0 = FRESHWATER
+    walls = heightFieldPositions(elevation, gradient, bounds, s, layers, wallTop, floor)
+    state = ParticleState.assemble(fluid, walls, s, rho0, velocities)
+    c0 = 10.0 * celerity
+    top = depth + solitaryWaveProfile(state.positions[:, 0], height, depth, crestX)
+    state.densities = hydrostaticDensity(top - state.positions[:, 2], rho0, c0)
+    margin = (layers + 2.0) * s
+    return Case('ridgeWave3D', state, boundary, 3, s, smoothingRatio * s, 'wendlandC2',
+                np.array([-margin, -margin, floor - margin]), np.array([length + margin, width + margin, wallTop]),
+                rho0, c0, np.array([0.0, 0.0, -GRAVITY]), alpha=0.01, densityFloor=0.9 * rho0,
+                densityDiffusion='hydrostatic', wallExtrapolated=True, continuityCorrection=True,
+                viscosityLimiter=True, cflNumber=0.25, maxTimeStep=1.0,
+                info={'depth': depth, 'H/d': height / depth, 'crestX': crestX, 'ridge': [ridgeHeight, ridgeWidth, angle],
+                      'tank': [length, width], 'ppd': particlesPerDepth, 'layers': layers})
 
 
 def pairSumsFor(case: Case, cellsPerSupport: int | None = None, device: int = 0):

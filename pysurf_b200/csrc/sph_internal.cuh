@@ -29,9 +29,14 @@ constexpr int kBlock = 128;                 // threads per sweep block
 #ifndef SPH_SWEEP_MIN_BLOCKS
 #define SPH_SWEEP_MIN_BLOCKS 8
 #endif
-// resident sweep blocks an SM: 8 blocks of 128 caps a sweep at 64 registers, for the warps that hide
-// its neighbours' load latency
-constexpr int kSweepMinBlocks = SPH_SWEEP_MIN_BLOCKS;
+#ifndef SPH_SWEEP_MIN_BLOCKS_3D
+#define SPH_SWEEP_MIN_BLOCKS_3D 6
+#endif
+// Resident sweep blocks an SM, which caps a sweep's registers: in 2D 8 blocks of 128 (64 registers)
+// give the warps that hide the neighbours' load latency; the 3D sweeps' 3 x 3 sums want about 105
+// registers, and 6 blocks (80 registers, a few spilled) ran faster than 4 (none spilled) or 5.
+template <int D>
+constexpr int sweepMinBlocks() { return D == 2 ? SPH_SWEEP_MIN_BLOCKS : SPH_SWEEP_MIN_BLOCKS_3D; }
 constexpr float kViscositySoftening = 0.01f;   // mu_ij's r^2 + 0.01 h^2 (src/pysurf/sphSolver.py:213)
 constexpr float kCloseDistance = 0.3f;      // limiter fade (src/pysurf/sphSolver.py:220-221)
 constexpr float kFoldWidth = 0.2f;

@@ -28,11 +28,21 @@ namespace sph {
 // The neighbour table
 // ------------------------------------------------------------------------------------------
 
+#ifndef SPH_LIST_TRIM
+#define SPH_LIST_TRIM 1
+#endif
+
 // Each slot's neighbours in the walk's order (forEachNeighbour's, with its tests), from a group of
 // L lanes: lane t tests candidates t, t + L, ... of each run of the stencil, and the group's ballot
 // places the accepted ones in order.  The count is the whole count even when the row is full (the
 // sweeps then walk the cells for that slot).  maxCount: the largest count, when given.
-template <int D, int L>
+//
+// A stencil row is trimmed to the cells within the search's reach of the particle, taken in cell
+// units from the particle's place in its cell (a particle outside the grid, whose cell is clamped,
+// searches its whole stencil).  The reach carries slack over the coarse test's bound, so every
+// candidate the coarse test passes stays: the accepted neighbours and their order are those of the
+// whole stencil.  PRECISE: separations from point and remainder; MIXED: smoothing lengths differ.
+template <int D, int L, bool PRECISE, bool MIXED>
 __global__ void __launch_bounds__(kBlock) listKernel(Params P, Frame F, const Control *ctl, int *maxCount)
 {
     if (ctl && !ctl->active) return;
@@ -42,12 +52,14 @@ __global__ void __launch_bounds__(kBlock) listKernel(Params P, Frame F, const Co
     const int t = G.t;
     const int shift = (threadIdx.x & 31) & ~(L - 1);
     const unsigned lower = (1u << t) - 1u;
-    const float hI = fabsf(signedLength<D>(F, i));
+    const float4 Ai = __ldg(&F.pa[i]), Bi = __ldg(&F.pb[i]);
+    const float hI = fabsf(signedLengthIn<D>(Ai, Bi));
     float pi[3], li[3];
-    pointOf<D>(F, i, pi);
-    remainderOf<D>(F, i, li);
-    const float reach = P.mixedH ? hI + P.hMax : 2.0f * P.hMax;
+    pointIn<D>(Ai, pi);
+    remainderIn<D>(Ai, Bi, li);
+    const float reach = MIXED ? hI + P.hMax : 2.0f * P.hMax;
     const float limit = kCandidateMargin * reach * reach;
+    const float support = MIXED ? 0.0f : support2(P.hMax);
     double shift64 = 0.0;
     bool seam = false;
     if (D == 3 && P.period > 0.0 && (pi[1] < reach || pi[1] > P.periodF - reach)) {
@@ -60,15 +72,35 @@ __global__ void __launch_bounds__(kBlock) listKernel(Params P, Frame F, const Co
     const int x0 = max(cx - ncs, 0), x1 = min(cx + ncs, nx - 1);
     const int z0 = D == 3 ? max(cz - ncs, 0) : 0, z1 = D == 3 ? min(cz + ncs, P.nc[2] - 1) : 0;
     const int cyImage = seam ? cellCoordinate((double)pi[1] + (double)li[1] + shift64, P.origin[1], P.cellWidth, ny) : cy;
+    // the particle's place in its cell, in cell widths, and the reach in cell widths with slack
+    const float invW = (float)(1.0 / P.cellWidth);
+    const float fx = (float)(((double)pi[0] - P.origin[0]) / P.cellWidth) - (float)cx;
+    const float fz = D == 3 ? (float)(((double)pi[2] - P.origin[2]) / P.cellWidth) - (float)cz : 0.5f;
+    const float R = (1.001f * sqrtf(limit) + 5.0e-7f * (fabsf(pi[0]) + fabsf(pi[1]) + fabsf(pi[2]))) * invW + 1.0e-3f;
     int *column = F.nbr + 4 * (size_t)i;
     int count = 0;
     for (int image = 0; image < (seam ? 2 : 1); ++image) {
         const int yc = image == 0 ? cy : cyImage;
         const float offset = image ? (float)shift64 : 0.0f;
-        for (int zz = z0; zz <= z1; ++zz)
+        const float fy = (float)(((double)pi[1] + (image ? shift64 : 0.0) - P.origin[1]) / P.cellWidth) - (float)yc;
+        const bool trim = SPH_LIST_TRIM && fx >= 0.0f && fx < 1.0f && fy >= 0.0f && fy < 1.0f && fz >= 0.0f &&
+                          fz < 1.0f;
+        for (int zz = z0; zz <= z1; ++zz) {
+            const int oz = zz - cz;
+            const float dz = oz > 0 ? (float)oz - fz : (oz < 0 ? fz - (float)(oz + 1) : 0.0f);
             for (int yy = max(yc - ncs, 0); yy <= min(yc + ncs, ny - 1); ++yy) {
+                int xa = x0, xb = x1;
+                if (trim) {
+                    const int oy = yy - yc;
+                    const float dy = oy > 0 ? (float)oy - fy : (oy < 0 ? fy - (float)(oy + 1) : 0.0f);
+                    const float rem = R * R - dy * dy - dz * dz;
+                    if (rem < 0.0f) continue;
+                    const float ext = sqrtf(rem);
+                    xa = max(x0, cx + (int)floorf(fx - ext));
+                    xb = min(x1, cx + (int)floorf(fx + ext));
+                }
                 const int row = (zz * ny + yy) * nx;
-                const int first = __ldg(&F.cellStart[row + x0]), end = __ldg(&F.cellStart[row + x1 + 1]);
+                const int first = __ldg(&F.cellStart[row + xa]), end = __ldg(&F.cellStart[row + xb + 1]);
                 for (int base = first; base < end; base += L) {
                     const int j = base + t;
                     bool accepted = false;
@@ -76,13 +108,17 @@ __global__ void __launch_bounds__(kBlock) listKernel(Params P, Frame F, const Co
                         const float4 A = __ldg(&F.pa[j]);
                         float pj[3];
                         pointIn<D>(A, pj);
-                        if (coarseDistance2<D>(pi, pj, offset) < limit) {
-                            const float4 B = D == 3 || P.mixedH ? __ldg(&F.pb[j]) : A;
-                            float lj[3], d[3];
-                            remainderIn<D>(A, B, lj);
-                            const float r2 = separation2<D>(P, pi, li, pj, lj, offset, image, shift64, d);
-                            const float h = P.mixedH ? 0.5f * (hI + fabsf(signedLengthIn<D>(A, B))) : P.hMax;
-                            accepted = r2 < support2(h);
+                        const float coarse = coarseDistance2<D>(pi, pj, offset);
+                        if (coarse < limit) {
+                            const float4 B = (D == 3 && PRECISE) || MIXED ? __ldg(&F.pb[j]) : A;
+                            float r2 = coarse;      // the float32 points' separation is the coarse one
+                            if (PRECISE) {
+                                float lj[3], d[3];
+                                remainderIn<D>(A, B, lj);
+                                r2 = separation2<D, 1>(P, pi, li, pj, lj, offset, image, shift64, d);
+                            }
+                            const float bound = MIXED ? support2(0.5f * (hI + fabsf(signedLengthIn<D>(A, B)))) : support;
+                            accepted = r2 < bound;
                         }
                     }
                     const unsigned bits = (__ballot_sync(G.mask, accepted) >> shift) & ((L >= 32 ? 0u : 1u << L) - 1u);
@@ -94,6 +130,7 @@ __global__ void __launch_bounds__(kBlock) listKernel(Params P, Frame F, const Co
                     count += __popc(bits);
                 }
             }
+        }
     }
     if (t != 0) return;
     F.ncount[i] = count;
@@ -130,7 +167,7 @@ struct ShepardVisit {
 };
 
 template <int D, int K, int T>
-__global__ void __launch_bounds__(kBlock, kSweepMinBlocks) shepardKernel(Params P, Frame F, const Control *ctl)
+__global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>()) shepardKernel(Params P, Frame F, const Control *ctl)
 {
     if (!filterDue(ctl)) return;
     const Group<T> G = groupOf<T>();
@@ -185,7 +222,7 @@ struct WallVisit {
 // Boundary rows only write their own entries and only fluid entries are read, so the frame is
 // updated in place.  writeDensity: the master float64 density takes Tait^-1(p_w) too.
 template <int D, int K, int T>
-__global__ void __launch_bounds__(kBlock, kSweepMinBlocks)
+__global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>())
 wallPressureKernel(Params P, Frame F, const Control *ctl, int writeDensity)
 {
     if (ctl && !ctl->active) return;
@@ -259,7 +296,7 @@ __device__ __forceinline__ void groupSumMatrix(float M[3][3], unsigned mask)
 }
 
 template <int D, int K, int T>
-__global__ void __launch_bounds__(kBlock, kSweepMinBlocks)
+__global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>())
 gradientKernel(Params P, Frame F, const Control *ctl, int wantG, int wantL, int wantRho, float floorDet)
 {
     if (ctl && !ctl->active) return;
@@ -398,7 +435,7 @@ __device__ __forceinline__ double cflTimeStep(double h, double c0, double vmax, 
 }
 
 template <int D, int K, int T>
-__global__ void __launch_bounds__(kBlock, kSweepMinBlocks)
+__global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>())
 momentumKernel(Params P, Frame F, Control *ctl, double *blockMaxima)
 {
     __shared__ double shared[kBlock / 32];
@@ -562,7 +599,7 @@ struct ContinuityVisit {
 
 // mode 0: the rate only; 1: advance the density; 2: advance, drift and enforce.
 template <int D, int K, int T>
-__global__ void __launch_bounds__(kBlock, kSweepMinBlocks)
+__global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>())
 continuityKernel(Params P, Frame F, Control *ctl, Enforcement E, int mode)
 {
     if (ctl && !ctl->active) return;
@@ -623,7 +660,7 @@ struct XsphVisit {
 // densities: the float32 densities the sum divides by (null: the frame's).  mode 0: the transport
 // velocity into F.vec only; 2: drift with it and enforce.
 template <int D, int K, int T>
-__global__ void __launch_bounds__(kBlock, kSweepMinBlocks)
+__global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>())
 xsphKernel(Params P, Frame F, Control *ctl, Enforcement E, const float *densities, int mode)
 {
     if (ctl && !ctl->active) return;
@@ -664,6 +701,20 @@ static inline int blocksFor(long long n, int block) { return (int)((n + block - 
 constexpr int kListLanes2 = SPH_LIST_LANES_2D;
 constexpr int kListLanes3 = 4;
 
+// The table kernel: lanes a slot (the 2D stencil's runs are longer), and its precision and
+// smoothing-length forms.
+template <int D>
+static void launchList(const LaunchArgs &A)
+{
+    constexpr int L = D == 2 ? kListLanes2 : kListLanes3;
+    const int grid = blocksFor((long long)A.P.n * L, kBlock);
+    cudaStream_t st = A.stream;
+    if (A.P.precise && !A.P.mixedH) listKernel<D, L, true, false><<<grid, kBlock, 0, st>>>(A.P, A.F, A.ctl, A.maxCount);
+    else if (A.P.precise) listKernel<D, L, true, true><<<grid, kBlock, 0, st>>>(A.P, A.F, A.ctl, A.maxCount);
+    else if (!A.P.mixedH) listKernel<D, L, false, false><<<grid, kBlock, 0, st>>>(A.P, A.F, A.ctl, A.maxCount);
+    else listKernel<D, L, false, true><<<grid, kBlock, 0, st>>>(A.P, A.F, A.ctl, A.maxCount);
+}
+
 template <int D, int K, int T>
 static void launchT(const LaunchArgs &A, Stage stage)
 {
@@ -683,13 +734,7 @@ static void launchT(const LaunchArgs &A, Stage stage)
     case Stage::Kick: kickKernel<D><<<pointwise, kBlock, 0, st>>>(P, F, A.ctl); break;
     case Stage::Continuity: continuityKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.flag); break;
     case Stage::Xsph: xsphKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.densities, A.flag); break;
-    case Stage::List:
-        // lanes a slot for the table: the 2D stencil's runs are longer
-        if (D == 2) listKernel<2, kListLanes2><<<blocksFor((long long)P.n * kListLanes2, kBlock), kBlock, 0, st>>>(
-            P, F, A.ctl, A.maxCount);
-        else listKernel<3, kListLanes3><<<blocksFor((long long)P.n * kListLanes3, kBlock), kBlock, 0, st>>>(
-            P, F, A.ctl, A.maxCount);
-        break;
+    case Stage::List: launchList<D>(A); break;
     }
 }
 

@@ -80,11 +80,12 @@ __device__ __forceinline__ float coarseDistance2(const float pi[3], const float 
 }
 
 // d = x_i - x_j from the points and remainders (image: across the periodic seam, in float64); r^2.
-template <int D>
+// PRECISE 1 or 0 fixes the form at compile time, -1 takes it from P.precise.
+template <int D, int PRECISE = -1>
 __device__ __forceinline__ float separation2(const Params &P, const float pi[3], const float li[3], const float pj[3],
                                             const float lj[3], float offset, int image, double shift64, float d[3])
 {
-    if (!P.precise) {
+    if (PRECISE == 0 || (PRECISE < 0 && !P.precise)) {
         // separationPrecision 'float32': the points alone (src/pysurf/sphGpu.py:227-242)
         d[0] = __fsub_rn(pi[0], pj[0]);
         d[1] = __fsub_rn(__fadd_rn(pi[1], offset), pj[1]);
