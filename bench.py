@@ -1,13 +1,14 @@
 """Benchmark: fluid particle-updates/s of the deltaSph step on the 2D solitary wave over a 1:15 beach.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--ppd 64]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--case beach|ridge] [--ppd P]
 
 Workload: the first-order solitary wave of H/d = 0.45 at x0 = 10 d over a 1:15 beach from
 x = 15 d, 60 d long, 64 particles per depth (pysurf_b200.cases.solitaryBeach), stepped by the
 deltaSph scheme (Wendland C2 at h = 3 dx, hydrostatic delta-SPH diffusion, the continuity
 correction, extrapolated walls, the viscosity limiter, density floor 0.9 rho0).  A step is one
 full device-resident step: cell list, wall pressure, gradients, momentum, time step, kick,
-continuity, density update, drift and bed enforcement.
+continuity, density update, drift and bed enforcement.  --case ridge steps the 3D Gaussian-ridge
+tank instead (pysurf_b200.cases.ridgeWave3D, 24 particles per depth by default).
 
 value      fluid particles x steps / device time of exactly K steps (CUDA events on the stream the
            kernels run on, an L2 flush of 256 MiB between steps outside the timed spans), max over
@@ -16,7 +17,9 @@ value      fluid particles x steps / device time of exactly K steps (CUDA events
 e2e        the same metric through the public API with host buffers: each step pushes the whole
            state from pinned host memory, steps once and pulls the state back.
 roofline   the dominant kernel (momentum) against the measured HBM copy bandwidth, with the
-           step's algorithmic bytes per fluid particle-update (53 B in 2D) per launch.
+           step's algorithmic bytes per fluid particle-update (53 B in 2D, 69 B in 3D) per launch.
+pair_flops the three sweeps' float32 work, 150 flop a directed pair, against the nominal FP32 SIMT
+           peak: the gather sweeps are bound by latency and issue, not by HBM.
 --impl reference   the float64 C restatement of the reference's step (oracle/, OpenMP over every
            host core) on the same workload, timed per step.
 """
@@ -35,7 +38,11 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-ALGORITHMIC_BYTES_2D = 53       # per fluid particle-update: x 8+4, v 8, rho 4, m 4, kind 1 read; x, v, rho written
+# algorithmic bytes per fluid particle-update: read x (offset + cell), v, rho, m, kind; write x, v, rho
+ALGORITHMIC_BYTES = {2: 53, 3: 69}
+FLOP_PER_PAIR = 150             # float32 flop per directed pair per step over the three sweeps (gradients,
+                                # momentum with the limiter, continuity with diffusion)
+FP32_SIMT_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12   # nominal: 148 SMs x 128 FP32 lanes x FMA x 1965 MHz
 METRIC = 'particle-updates/s'
 
 
@@ -45,7 +52,9 @@ def parseArgs():
     p.add_argument('--steps', type=int, default=40)
     p.add_argument('--warmup', type=int, default=5)
     p.add_argument('--impl', default='b200', choices=['b200', 'reference'])
-    p.add_argument('--ppd', type=int, default=64)
+    p.add_argument('--case', default='beach', choices=['beach', 'ridge'],
+                   help='beach: the 2D solitary wave on a 1:15 beach (the headline); ridge: the 3D Gaussian ridge')
+    p.add_argument('--ppd', type=int, default=None, help='particles per depth (64 beach, 24 ridge)')
     p.add_argument('--cells', type=int, default=None, help='cells per kernel support in the device cell list')
     p.add_argument('--threads', type=int, default=None, help='threads per particle in the sweeps (1, 2, 4, 8)')
     p.add_argument('--no-table', action='store_true', help='walk the cells in every sweep (no neighbour table)')
@@ -54,14 +63,65 @@ def parseArgs():
     return p.parse_args()
 
 
+def buildCase(args):
+    from pysurf_b200 import cases
+    if args.case == 'ridge':
+        return cases.ridgeWave3D(args.ppd or 24)
+    return cases.solitaryBeach(args.ppd or 64)
+
+
 def config(case, flush: bool = True) -> dict:
     info = dict(case.info)
-    return {'workload': 'solitary wave H/d 0.45 on a 1:15 plane beach, 2D, deltaSph scheme (Wendland C2 h=3dx, '
-                        'hydrostatic delta-SPH 0.1, continuity correction, extrapolated walls, viscosity limiter)',
-            'particles_per_depth': info['ppd'], 'fluid_particles': case.fluidCount,
-            'boundary_particles': int(case.state.nParticles - case.fluidCount), 'bed_layers': info['layers'],
-            'smoothing_length_over_dx': round(case.smoothingLength / case.spacing, 6), 'domain_length_d': info['length'],
+    scheme = ('deltaSph scheme (Wendland C2 h=3dx, hydrostatic delta-SPH 0.1, continuity correction, extrapolated '
+              'walls, viscosity limiter)')
+    if case.dimensions == 2:
+        workload = f'solitary wave H/d 0.45 on a 1:15 plane beach, 2D, {scheme}'
+        extent = {'domain_length_d': info['length']}
+    else:
+        workload = (f'solitary wave H/d 0.5 over a Gaussian ridge (0.6 d, sigma 3 d, axis at 25 degrees) in a '
+                    f'40 d x 10 d tank, 3D, {scheme}')
+        extent = {'tank_d': info['tank']}
+    return {'workload': workload, 'particles_per_depth': info['ppd'], 'fluid_particles': case.fluidCount,
+            'boundary_particles': int(case.state.nParticles - case.fluidCount), 'boundary_layers': info['layers'],
+            'smoothing_length_over_dx': round(case.smoothingLength / case.spacing, 6), **extent,
             'l2': 'flushed (256 MiB write) between timed steps' if flush else 'resident'}
+
+
+def meanNeighbours(case, sample: int = 20000) -> float:
+    """Neighbours within 2h of a fluid particle at the start, the mean over a seeded sample, for the
+    pair-flop figure."""
+    import numpy as np
+    from scipy.spatial import cKDTree
+    positions = case.state.positions
+    fluid = np.flatnonzero(case.state.isFluid)
+    chosen = np.random.default_rng(0).choice(fluid, size=min(sample, fluid.size), replace=False)
+    counts = cKDTree(positions).query_ball_point(positions[chosen], 2.0 * case.smoothingLength, return_length=True)
+    return float(np.mean(counts) - 1.0)
+
+
+def oracleStepper(case):
+    """The float64 C restatement of the device step (oracle/) set up for the case."""
+    from oracle import oracle
+    boundary = case.boundary
+    if type(boundary).__name__ == 'BedBoundary':
+        bed = boundary.bathymetry
+        enforcement = ('bed', oracle.bedParams(bed.x, bed.z, 0.25 * case.spacing, False, 0.0, True, bed.startX, 0.0,
+                                               bed.endX))
+    else:
+        field, clearance = boundary.field, 0.25 * boundary.spacing
+        startX, endX, startY, endY = field.bounds
+        enforcement = ('field', oracle.fieldParams(field.z, field.x[0], field.y[0], field.spacingX, field.spacingY,
+                                                   clearance, startY + clearance, endY - clearance, True,
+                                                   startX + clearance, endX - clearance))
+    return oracle.Stepper(case.dimensions, case.kernelType, case.smoothingLength, case.referenceDensity,
+                          case.soundSpeed, case.alpha, case.gravity, 0.0, 0.0, case.densityFloor,
+                          case.densityDiffusion, case.diffusionDelta, True, False, True, True, case.cflNumber,
+                          case.maxTimeStep, 0.0, 0, enforcement)
+
+
+def sweepConfig(sums, table: bool, threads: int) -> dict:
+    return {'cells_per_support': sums.cellsPerSupport, 'threads_per_particle': threads, 'neighbour_table': table,
+            'table_row_capacity': sums.neighborTableCapacity()}
 
 
 def clockSampler(device: int):
@@ -113,9 +173,10 @@ def measuredPeaks() -> dict:
     return {'hbm_gbs': 6650.0, 'source': 'fallback'}
 
 
-def profiledTraffic() -> float | None:
-    """dram bytes per momentum launch from the committed ncu summary, if one is there."""
-    path = os.path.join(ROOT, 'profiles', 'momentum_solitaryBeach64.md')
+def profiledTraffic(case) -> float | None:
+    """dram bytes per momentum launch from the committed ncu summary of this workload, if one is there."""
+    name = 'momentum_solitaryBeach64.md' if case.dimensions == 2 else f'momentum_ridgeWave3D{case.info["ppd"]}.md'
+    path = os.path.join(ROOT, 'profiles', name)
     if not os.path.exists(path):
         return None
     match = re.search(r'traffic_bytes_per_launch:\s*([0-9.eE+]+)', open(path).read())
@@ -125,13 +186,7 @@ def profiledTraffic() -> float | None:
 def cpuBaseline(case, seconds: float = 12.0) -> dict:
     """The float64 oracle's step on the same workload, on every host core, for about `seconds`."""
     import numpy as np
-    from oracle import oracle
-    bed = case.boundary.bathymetry
-    stepper = oracle.Stepper(2, case.kernelType, case.smoothingLength, case.referenceDensity, case.soundSpeed,
-                             case.alpha, case.gravity, 0.0, 0.0, case.densityFloor, case.densityDiffusion,
-                             case.diffusionDelta, True, False, True, True, case.cflNumber, case.maxTimeStep, 0.0, 0,
-                             ('bed', oracle.bedParams(bed.x, bed.z, 0.25 * case.spacing, False, 0.0, True, bed.startX,
-                                                      0.0, bed.endX)))
+    stepper = oracleStepper(case)
     state = {k: np.array(getattr(case.state, k), copy=True) for k in ('positions', 'velocities', 'densities',
                                                                        'masses', 'isFluid')}
     stepper(state)                          # warm-up: page in, first neighbour list
@@ -153,16 +208,9 @@ def referenceArm(args) -> None:
     rank = int(os.environ.get('RANK', '0'))
     if rank != 0:
         return
-    from pysurf_b200 import cases
-    case = cases.solitaryBeach(args.ppd)
+    case = buildCase(args)
     import numpy as np
-    from oracle import oracle
-    bed = case.boundary.bathymetry
-    stepper = oracle.Stepper(2, case.kernelType, case.smoothingLength, case.referenceDensity, case.soundSpeed,
-                             case.alpha, case.gravity, 0.0, 0.0, case.densityFloor, case.densityDiffusion,
-                             case.diffusionDelta, True, False, True, True, case.cflNumber, case.maxTimeStep, 0.0, 0,
-                             ('bed', oracle.bedParams(bed.x, bed.z, 0.25 * case.spacing, False, 0.0, True, bed.startX,
-                                                      0.0, bed.endX)))
+    stepper = oracleStepper(case)
     state = {k: np.array(getattr(case.state, k), copy=True) for k in ('positions', 'velocities', 'densities',
                                                                        'masses', 'isFluid')}
     for _ in range(args.warmup):
@@ -203,14 +251,15 @@ def main() -> None:
     if world > 1:
         dist.init_process_group('nccl', timeout=timedelta(seconds=300), device_id=torch.device('cuda', local))
 
-    case = cases.solitaryBeach(args.ppd)
+    case = buildCase(args)
     sums = cases.pairSumsFor(case, args.cells, device=local)
-    sums.setSweepOptions(not args.no_table, args.threads or 1)
+    sums.setSweepOptions(not args.no_table, args.threads or 4)
     stream = torch.cuda.Stream()
     sums.setStream(stream.cuda_stream)
     state = case.state.copy()
     sums.push(state)
     sums.setBoundary(case.boundary, state)
+    neighbours = meanNeighbours(case)
     h, cfl, maxdt = case.smoothingLength, case.cflNumber, case.maxTimeStep
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device='cuda')     # 256 MiB, twice the L2
 
@@ -252,22 +301,29 @@ def main() -> None:
     dominant = max(stages, key=stages.get)
     peaks = measuredPeaks()
     kernelMs = stages[dominant]
-    achieved = ALGORITHMIC_BYTES_2D * case.fluidCount / (kernelMs / 1e3) / 1e9
+    unitBytes = ALGORITHMIC_BYTES[case.dimensions]
+    achieved = unitBytes * case.fluidCount / (kernelMs / 1e3) / 1e9
+    pairFlop = case.fluidCount * neighbours * FLOP_PER_PAIR
+    simt = {'flop_per_pair': FLOP_PER_PAIR, 'neighbours_per_fluid_particle': neighbours,
+            'achieved_tflops': pairFlop / (totalMs / args.steps / 1e3) / 1e12, 'peak_tflops': FP32_SIMT_TFLOPS,
+            'peak_source': 'nominal FP32 SIMT: 148 SMs x 128 lanes x 2 flop x 1965 MHz'}
+    simt['frac'] = simt['achieved_tflops'] / FP32_SIMT_TFLOPS
     roofline = {'bound': 'hbm', 'kernel': dominant, 'achieved': achieved, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
-                'frac': achieved / peaks['hbm_gbs'], 'traffic': profiledTraffic(), 'peak_source': peaks['source'],
-                'kernel_ms': kernelMs, 'step_hbm_frac': ALGORITHMIC_BYTES_2D * case.fluidCount /
+                'frac': achieved / peaks['hbm_gbs'], 'traffic': profiledTraffic(case), 'peak_source': peaks['source'],
+                'kernel_ms': kernelMs, 'bytes_per_update': unitBytes, 'step_hbm_frac': unitBytes * case.fluidCount /
                 (totalMs / args.steps / 1e3) / 1e9 / peaks['hbm_gbs']}
 
     # end to end through the public API with host buffers: push, one step, pull, every step
     e2e = None
     if not args.no_e2e:
-        n, dim = case.state.nParticles, 2
+        n, dim = case.state.nParticles, case.dimensions
         pinned = {name: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
                   for name, shape in (('positions', (n, dim)), ('velocities', (n, dim)), ('densities', (n,)),
                                       ('masses', (n,)), ('pressures', (n,)), ('accelerations', (n, dim)))}
         sums.pull(state)
+        flags = torch.empty(n, dtype=torch.bool, pin_memory=True).numpy()
         host = type(state)(pinned['positions'], pinned['velocities'], pinned['accelerations'], pinned['densities'],
-                           pinned['pressures'], pinned['masses'], torch.empty(n, dtype=torch.bool, pin_memory=True).numpy())
+                           pinned['pressures'], pinned['masses'], flags)
         for name in ('positions', 'velocities', 'densities', 'masses', 'pressures', 'accelerations'):
             getattr(host, name)[:] = getattr(state, name)
         host.isFluid[:] = state.isFluid
@@ -305,9 +361,10 @@ def main() -> None:
         line = {'metric': METRIC, 'value': value, 'unit': METRIC, 'n_gpus': world, 'steps': args.steps,
                 'warmup': args.warmup, 'ms_per_step': totalMs / args.steps, 'higher_is_better': True,
                 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32 sums, f64 state', 'data': 'synthetic',
-                'config': dict(config(case), parallelism=f'replicas{world}' if world > 1 else 'single'),
+                'config': dict(config(case), parallelism=f'replicas{world}' if world > 1 else 'single',
+                               **sweepConfig(sums, not args.no_table, args.threads or 4)),
                 'clocks': clocks, 'e2e': e2e, 'gpu_launches': launchesPerStep * args.steps,
-                'roofline': roofline, 'stages_ms': stages, 'cpu_baseline': cpu,
+                'roofline': roofline, 'pair_flops': simt, 'stages_ms': stages, 'cpu_baseline': cpu,
                 'simulated_time_s': t}
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -54,14 +54,15 @@ int sph_version(void);
 /* The hash grid's shape the reference's sortParticles reads (PairSums.gridShape,
  * src/pysurf/sphGpu.py:1466-1478 gridDimensions). */
 int sph_grid_shape(const SphSystem *sys, int64_t shape[3]);
-/* Cells per support of the internal cell list (1: cells 2h wide, 2: cells h wide). */
+/* Cells per support of the internal cell list (1: cells 2h wide, 2: cells h wide, ...; the
+ * default 3, cells 2h / 3 wide, offers the fewest candidates for the stencil's cost). */
 int sph_set_cells_per_support(SphSystem *sys, int cells);
 /* How the sweeps find neighbours: neighbor_table 1 (the default) records each step's neighbours
  * once, after the cell list, in a table sized to the largest count seen at push/update plus a
- * quarter, when it fits in half the free device memory; a particle whose count outgrows its row
- * walks the cells, with the same summation order.  0 always walks the cells.
- * threads_per_particle 1, 2, 4 or 8 threads share each particle's neighbours (sums combined by
- * shuffles in a fixed order). */
+ * quarter, when it fits in three quarters of the free device memory; a particle whose count
+ * outgrows its row walks the cells, with the same summation order.  0 always walks the cells.
+ * threads_per_particle 1, 2, 4 (the default) or 8 threads share each particle's neighbours (sums
+ * combined by shuffles in a fixed order). */
 int sph_set_sweep_options(SphSystem *sys, int neighbor_table, int threads_per_particle);
 /* The neighbour table's row capacity now (0: the sweeps walk the cells). */
 int sph_neighbor_table(const SphSystem *sys, int64_t *row_capacity);

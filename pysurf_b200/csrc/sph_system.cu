@@ -82,7 +82,7 @@ struct SphSystem {
     double domainMin[3] = {0, 0, 0}, domainMax[3] = {0, 0, 0};
     double period = 0.0;
     int precise = 1;
-    int ncs = 1;
+    int ncs = 3;                // cells per support: 2h / 3 wide cells trim the candidates
     int64_t gridShape[3] = {1, 1, 1};
     // physics (setPhysics) and the sums' switches
     double rho0 = 1000.0, c0 = 1.0, alpha = 0.0, boundaryFactor = 0.0, gravity[3] = {0, 0, 0};
@@ -131,7 +131,7 @@ struct SphSystem {
     int listCap = 0;
     int tableMode = 1;          // 0 never build the table, 1 build it when it fits the budget
     bool listDirty = true;      // the table's size must be taken again before the next step
-    int threads = 1;            // threads per particle in the sweeps
+    int threads = 4;            // threads per particle in the sweeps
     int cellStartCapacity = 0;
     // execution
     cudaStream_t stream = nullptr;
@@ -406,7 +406,8 @@ struct SphSystem {
     }
 
     // Take the neighbour table's size from the current cell list: the largest count now, with room
-    // to grow by a quarter, if it fits in half the free device memory; otherwise no table.  Syncs.
+    // to grow by a quarter, if it fits in three quarters of the free device memory; otherwise no
+    // table.  Syncs.
     int sizeList()
     {
         listDirty = false;
@@ -434,7 +435,7 @@ struct SphSystem {
             cudaFree(nbr);
             nbr = nullptr;
             nbrEntries = 0;
-            if (entries * sizeof(int) > freeBytes / 2 || deviceAlloc(&nbr, entries) != SPH_OK) {
+            if (entries * sizeof(int) > freeBytes / 4 * 3 || deviceAlloc(&nbr, entries) != SPH_OK) {
                 nbr = nullptr;
                 cap = 0;
                 cudaGetLastError();

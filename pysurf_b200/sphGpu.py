@@ -152,6 +152,7 @@ class PairSums:
         shape = np.zeros(3, dtype=np.int64)
         check(self._lib.sph_grid_shape(self._handle, shape.ctypes.data_as(_lib._pi64)))
         self.gridShape = tuple(int(c) for c in shape)
+        self.cellsPerSupport = 3
         self._enforcement = None
 
     def __del__(self):
@@ -221,10 +222,11 @@ class PairSums:
         self.shiftingEnabled = False
 
     def setCellsPerSupport(self, cells: int) -> None:
-        """Cells per kernel support of the device's cell list (1: 2h wide; 2: h wide)."""
+        """Cells per kernel support of the device's cell list (1: 2h wide; 2: h wide; the default 3: 2h/3 wide)."""
         check(self._lib.sph_set_cells_per_support(self._handle, int(cells)))
+        self.cellsPerSupport = int(cells)
 
-    def setSweepOptions(self, neighborTable: bool = True, threadsPerParticle: int = 1) -> None:
+    def setSweepOptions(self, neighborTable: bool = True, threadsPerParticle: int = 4) -> None:
         """Whether the sweeps read a per-step neighbour table (else they walk the cells; the sums are
         the same bits either way), and how many threads (1, 2, 4, 8) share each particle's neighbours."""
         check(self._lib.sph_set_sweep_options(self._handle, int(bool(neighborTable)), int(threadsPerParticle)),

@@ -43,9 +43,11 @@ def caseFromRun(r) -> cases.Case:
                       densityFilterInterval=int(interval), period=period)
 
 
-def deviceRun(case, steps, cellsPerSupport=None, table=True, threads=1):
+def deviceRun(case, steps, cellsPerSupport=None, table=True, threads=None):
+    # threads None keeps the backend's default, which hostDrivenRun's PairSums also runs with
     sums = cases.pairSumsFor(case, cellsPerSupport)
-    sums.setSweepOptions(table, threads)
+    if threads is not None or not table:
+        sums.setSweepOptions(table, threads or 4)
     state = case.state.copy()
     sums.push(state)
     sums.setBoundary(case.boundary, state)
