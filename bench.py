@@ -174,13 +174,22 @@ def measuredPeaks() -> dict:
 
 
 def profiledTraffic(case) -> float | None:
-    """dram bytes per momentum launch from the committed ncu summary of this workload, if one is there."""
-    name = 'momentum_solitaryBeach64.md' if case.dimensions == 2 else f'momentum_ridgeWave3D{case.info["ppd"]}.md'
+    """DRAM bytes per momentum launch from the committed ncu summary of this workload.  The 3D
+    workload is captured at 8 ppd (the bench's size is too large to capture); its traffic, which
+    grows with the fluid rows, is scaled to this case by the fluid count."""
+    name = 'momentum_solitaryBeach64.md' if case.dimensions == 2 else 'momentum_ridgeWave3D8.md'
     path = os.path.join(ROOT, 'profiles', name)
     if not os.path.exists(path):
         return None
-    match = re.search(r'traffic_bytes_per_launch:\s*([0-9.eE+]+)', open(path).read())
-    return float(match.group(1)) if match else None
+    text = open(path).read()
+    match = re.search(r'traffic_bytes_per_launch:\s*([0-9.eE+]+)', text)
+    if not match:
+        return None
+    traffic = float(match.group(1))
+    fluid = re.search(r'fluid_particles:\s*([0-9]+)', text)
+    if case.dimensions == 3 and fluid:
+        traffic *= case.fluidCount / float(fluid.group(1))
+    return traffic
 
 
 def cpuBaseline(case, seconds: float = 12.0) -> dict:
