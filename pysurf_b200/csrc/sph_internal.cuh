@@ -117,8 +117,11 @@ struct Control {
     int hostDt;                 // dt comes from the host (residentIntegrate), not the maxima
     int filterNow;              // host-driven steps: this step filters the density (Shepard)
     long long filterInterval;   // device loop: filter every this many steps, 0 for none
-    unsigned int ticket;        // last-block-done counter of the maxima reduction
+    unsigned int ticket;        // last-warp-done counter of the maxima reduction
     int error;                  // DeviceError flags
+    // the maxima reduction's running values: the bits of non-negative doubles, which order as the
+    // doubles do, so an integer atomicMax takes their maximum in any order; zero between steps
+    unsigned long long vmaxBits, amaxBits;
 };
 
 // ------------------------------------------------------------------------------------------

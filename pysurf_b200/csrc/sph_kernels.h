@@ -39,7 +39,7 @@ struct LaunchArgs {
     Frame F;
     cudaStream_t stream;
     Control *ctl;
-    double *blockMaxima;
+    int maxima;             // Momentum: fold the fluid maxima into ctl and take the time step
     Enforcement E;
     int flag;               // Wall: write the density too; Continuity / Xsph: the epilogue's mode
     int wantG, wantL, wantRho;

@@ -413,20 +413,6 @@ struct MomentumVisit {
     }
 };
 
-__device__ __forceinline__ double blockMax(double value, double *shared)
-{
-    for (int offset = 16; offset > 0; offset >>= 1) value = fmax(value, __shfl_down_sync(0xFFFFFFFFu, value, offset));
-    int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    __syncthreads();
-    if (lane == 0) shared[warp] = value;
-    __syncthreads();
-    if (warp == 0) {
-        value = lane < (int)(blockDim.x >> 5) ? shared[lane] : 0.0;
-        for (int offset = 16; offset > 0; offset >>= 1) value = fmax(value, __shfl_down_sync(0xFFFFFFFFu, value, offset));
-    }
-    return value;
-}
-
 __device__ __forceinline__ double cflTimeStep(double h, double c0, double vmax, double amax, double cfl, double maxdt)
 {
     double dt = cfl * h / (c0 + vmax);
@@ -434,12 +420,46 @@ __device__ __forceinline__ double cflTimeStep(double h, double c0, double vmax, 
     return fmin(dt, maxdt);
 }
 
+__device__ __forceinline__ double warpMax(double value)
+{
+    for (int offset = 16; offset > 0; offset >>= 1) value = fmax(value, __shfl_xor_sync(0xFFFFFFFFu, value, offset));
+    return value;
+}
+
+// The step's fluid maxima without a block barrier: each warp folds its lanes' values and lane 0
+// raises the running maxima (atomicMax on the bits of non-negative doubles, which is order-free);
+// the last warp to finish takes the time step in float64 and clears the running values.
+__device__ __forceinline__ void foldMaxima(Control *ctl, double speed, double accel, int warps)
+{
+    // non-negative, and a NaN counts as 0 as fmax would take it
+    speed = warpMax(speed > 0.0 ? speed : 0.0);
+    accel = warpMax(accel > 0.0 ? accel : 0.0);
+    if ((threadIdx.x & 31) != 0) return;
+    atomicMax(&ctl->vmaxBits, (unsigned long long)__double_as_longlong(speed));
+    atomicMax(&ctl->amaxBits, (unsigned long long)__double_as_longlong(accel));
+    __threadfence();
+    if (atomicAdd(&ctl->ticket, 1u) != (unsigned)(warps - 1)) return;
+    __threadfence();
+    const double vmax = __longlong_as_double((long long)atomicMax(&ctl->vmaxBits, 0ull));
+    const double amax = __longlong_as_double((long long)atomicMax(&ctl->amaxBits, 0ull));
+    ctl->vmax = vmax;
+    ctl->amax = amax;
+    ctl->vmaxBits = 0;
+    ctl->amaxBits = 0;
+    ctl->ticket = 0;
+    if (!ctl->hostDt) {
+        const double dt = cflTimeStep(ctl->hMin, ctl->soundSpeed, vmax, amax, ctl->cfl, ctl->maxTimeStep);
+        if (!(dt > 0.0) || !isfinite(dt)) ctl->error |= kErrTimeStep;
+        ctl->dt = dt;
+    }
+}
+
+// maxima: fold the fluid maxima into ctl and take the time step (the device steps); 0 for the
+// host-step sums.
 template <int D, int K, int T>
 __global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>())
-momentumKernel(Params P, Frame F, Control *ctl, double *blockMaxima)
+momentumKernel(Params P, Frame F, Control *ctl, int maxima)
 {
-    __shared__ double shared[kBlock / 32];
-    __shared__ bool last;
     if (ctl && !ctl->active) return;
     const Group<T> G = groupOf<T>();
     const int i = G.i;
@@ -469,37 +489,7 @@ momentumKernel(Params P, Frame F, Control *ctl, double *blockMaxima)
             }
         }
     }
-    if (!blockMaxima) return;
-    double bs = blockMax(speed, shared);
-    double ba = blockMax(accel, shared);
-    if (threadIdx.x == 0) {
-        blockMaxima[2 * blockIdx.x] = bs;
-        blockMaxima[2 * blockIdx.x + 1] = ba;
-        __threadfence();
-        unsigned ticket = atomicAdd(&ctl->ticket, 1u);
-        last = ticket == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!last) return;
-    // The last block reduces every block's maxima (max is order-free, so this is deterministic)
-    __threadfence();
-    double vmax = 0.0, amax = 0.0;
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
-        vmax = fmax(vmax, ((volatile double *)blockMaxima)[2 * b]);
-        amax = fmax(amax, ((volatile double *)blockMaxima)[2 * b + 1]);
-    }
-    vmax = blockMax(vmax, shared);
-    amax = blockMax(amax, shared);
-    if (threadIdx.x == 0) {
-        ctl->vmax = vmax;
-        ctl->amax = amax;
-        ctl->ticket = 0;
-        if (!ctl->hostDt) {
-            double dt = cflTimeStep(ctl->hMin, ctl->soundSpeed, vmax, amax, ctl->cfl, ctl->maxTimeStep);
-            if (!(dt > 0.0) || !isfinite(dt)) ctl->error |= kErrTimeStep;
-            ctl->dt = dt;
-        }
-    }
+    if (maxima) foldMaxima(ctl, speed, accel, (int)(gridDim.x * (blockDim.x >> 5)));
 }
 
 // v += a dt on the fluid (src/pysurf/sphGpu.py:1084-1109); the frame takes the kicked velocity.
@@ -730,7 +720,7 @@ static void launchT(const LaunchArgs &A, Stage stage)
     case Stage::Gradients:
         gradientKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.wantG, A.wantL, A.wantRho, A.floorDet);
         break;
-    case Stage::Momentum: momentumKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.blockMaxima); break;
+    case Stage::Momentum: momentumKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.maxima); break;
     case Stage::Kick: kickKernel<D><<<pointwise, kBlock, 0, st>>>(P, F, A.ctl); break;
     case Stage::Continuity: continuityKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.flag); break;
     case Stage::Xsph: xsphKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.densities, A.flag); break;

@@ -113,7 +113,6 @@ struct SphSystem {
     float *pres = nullptr, *rate = nullptr, *scalar = nullptr;
     int *cell = nullptr, *cellStart = nullptr;
     CellSortBuffers sortBuffers = {};
-    double *blockMaxima = nullptr;
     Control *ctl = nullptr;
     // Caller-order float64 staging on the device, kStageSlots rows of capacity doubles:
     //   inputs   0-2 vectors, 3 densities, 4 pressures (loadState: 0-2 x, 3-5 v, 6 rho, 7 m, 8 h)
@@ -160,7 +159,7 @@ struct SphSystem {
         }
         void *ptrs[] = {pa, pb, kin, G[0], G[1], G[2], L[0], L[1], L[2], gradRho, acc, vec, aux, pres, rate,
                         scalar, cell, sortBuffers.slotCell, sortBuffers.slotWithin, sortBuffers.perm,
-                        sortBuffers.bucket, blockMaxima, dStage, dStageU8, dRank, nbr, ncount};
+                        sortBuffers.bucket, dStage, dStageU8, dRank, nbr, ncount};
         for (void *p : ptrs) cudaFree(p);
         nbr = ncount = nullptr;
         nbrEntries = 0;
@@ -168,7 +167,7 @@ struct SphSystem {
         listDirty = true;
         pa = pb = kin = gradRho = acc = vec = nullptr;
         for (int a = 0; a < 3; ++a) G[a] = L[a] = nullptr;
-        aux = nullptr; pres = rate = scalar = nullptr; cell = nullptr; blockMaxima = nullptr;
+        aux = nullptr; pres = rate = scalar = nullptr; cell = nullptr;
         sortBuffers.slotCell = sortBuffers.slotWithin = sortBuffers.perm = nullptr;
         sortBuffers.bucket = nullptr;
         dStage = nullptr; dStageU8 = nullptr; dRank = nullptr;
@@ -240,8 +239,6 @@ struct SphSystem {
         TRY(deviceAlloc(&sortBuffers.slotWithin, cap));
         TRY(deviceAlloc(&sortBuffers.perm, cap));
         TRY(deviceAlloc(&sortBuffers.bucket, cap));
-        // one (speed, acceleration) pair per block of the momentum sweep, at up to 8 threads a particle
-        TRY(deviceAlloc(&blockMaxima, (size_t)2 * ((8ll * cap + kBlock - 1) / kBlock)));
         TRY(deviceAlloc(&dStage, (size_t)kStageSlots * cap));
         TRY(deviceAlloc(&dStageU8, cap));
         TRY(deviceAlloc(&dRank, cap));
@@ -373,7 +370,7 @@ struct SphSystem {
         A.F = frame();
         A.stream = stream;
         A.ctl = control;
-        A.blockMaxima = control ? blockMaxima : nullptr;
+        A.maxima = control ? 1 : 0;
         A.E = enforcement;
         A.floorDet = (float)pow(0.25, dim);
         A.threads = threads;
@@ -1173,6 +1170,7 @@ int sph_resident_rates(SphSystem *sys, int filter_density, double *max_speed, do
     c.ticket = 0;
     c.error = 0;
     c.vmax = c.amax = 0.0;
+    c.vmaxBits = c.amaxBits = 0;
     if (sys->n == 0) {
         if (max_speed) *max_speed = 0.0;
         if (max_acceleration) *max_acceleration = 0.0;
@@ -1261,6 +1259,7 @@ int sph_begin_steps(SphSystem *sys, double time, int64_t step, double last_dt, d
     c.filterNow = 0;
     c.hostDt = 0;
     c.ticket = 0;
+    c.vmaxBits = c.amaxBits = 0;
     c.error = 0;
     c.active = (time < until_time && step < max_step) ? 1 : 0;
     c.dt = last_dt;
