@@ -152,11 +152,12 @@ __device__ __forceinline__ bool filterDue(const Control *ctl)
 template <int D, int K>
 struct ShepardVisit {
     static constexpr bool kSkipCoincident = false;
+    static constexpr bool kKinetic = false;
     const Frame &F;
     Smoothing<K, D> S;
     float num, den;
     __device__ bool accept(bool) const { return true; }
-    __device__ void operator()(int j, const float *, float r, float h, bool, int, const float4 &B)
+    __device__ void operator()(int j, const float *, float r, float h, bool, int, const float4 &B, const float4 &)
     {
         const KernelAt k = S.at(h);
         const float4 X = auxRow<D>(F, j);
@@ -177,7 +178,8 @@ __global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>()) shepardKernel(Par
     // the particle itself first, as the reference's sums start (src/pysurf/sphGpu.py:781-783)
     float own = sigmaAt(P.sigmaUnit, hI, D);
     float mi = massOf<D>(F, i);
-    ShepardVisit<D, K> visit{F, Smoothing<K, D>(P), G.t == 0 ? mi * own : 0.0f, G.t == 0 ? volumeOf<D>(F, i) * own : 0.0f};
+    ShepardVisit<D, K> visit{F, Smoothing<K, D>(P), G.t == 0 ? mi * own : 0.0f,
+                             G.t == 0 ? volumeOf<D>(F, i) * own : 0.0f};
     forEachNeighbour<D, T>(P, F, i, G.t, hI, visit);
     float num = groupSum<T>(visit.num, G.mask), den = groupSum<T>(visit.den, G.mask);
     if (G.t != 0) return;
@@ -205,17 +207,18 @@ __global__ void applyShepardKernel(Params P, Frame F, const Control *ctl)
 template <int D, int K>
 struct WallVisit {
     static constexpr bool kSkipCoincident = false;
+    static constexpr bool kKinetic = true;
     const Params &P; const Frame &F;
     Smoothing<K, D> S;
     float weight, total;
     __device__ bool accept(bool fluidJ) const { return fluidJ; }
-    __device__ void operator()(int j, const float *d, float r, float h, bool, int, const float4 &)
+    __device__ void operator()(int j, const float *d, float r, float h, bool, int, const float4 &, const float4 &Kj)
     {
         const KernelAt k = S.at(h);
         float w = kernelValue<K>(r * k.invH, k);
         float gd = P.g[0] * d[0] + P.g[1] * d[1] + (D == 3 ? P.g[2] * d[2] : 0.0f);
         weight += w;
-        total += w * (pressureOf<D>(F, j) + densityOf<D>(F, j) * gd);
+        total += w * (pressureOf<D>(F, j) + densityIn<D>(Kj) * gd);
     }
 };
 
@@ -258,20 +261,22 @@ wallPressureKernel(Params P, Frame F, const Control *ctl, int writeDensity)
 template <int D, int K>
 struct GradientVisit {
     static constexpr bool kSkipCoincident = true;
+    static constexpr bool kKinetic = true;
     const Frame &F;
     Smoothing<K, D> kernel;
     bool wantG, wantL, wantRho;
     float vi[3], devI;
     float S[3][3], Mf[3][3], M[3][3], gsum[3];
     __device__ bool accept(bool) const { return true; }
-    __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int, const float4 &B)
+    __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int, const float4 &B,
+                               const float4 &Kj)
     {
         const KernelAt k = kernel.at(h);
         const float4 X = auxRow<D>(F, j);
         float w = volumeIn<D>(B, X) * kernelGradient<K>(r * k.invH, k);
         if (wantG && fluidJ) {
             float vj[3];
-            velocityOf<D>(F, j, vj);
+            velocityIn<D>(Kj, vj);
             for (int a = 0; a < D; ++a)
                 for (int b = 0; b < D; ++b) {
                     S[a][b] += w * (vj[a] - vi[a]) * d[b];
@@ -360,17 +365,18 @@ gradientKernel(Params P, Frame F, const Control *ctl, int wantG, int wantL, int 
 template <int D, int K>
 struct MomentumVisit {
     static constexpr bool kSkipCoincident = true;
+    static constexpr bool kKinetic = true;
     const Params &P; const Frame &F;
     Smoothing<K, D> S;
     float vi[3], rhoI, own, viscosityScale;   // viscosityScale: -alpha c0
     float Gi[3][3];
     float total[3];
     __device__ bool accept(bool) const { return true; }
-    __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int, const float4 &B)
+    __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int, const float4 &B,
+                               const float4 &Kj)
     {
         const KernelAt k = S.at(h);
         const float q = r * k.invH;
-        const float4 Kj = __ldg(&F.kin[j]);
         float vj[3];
         velocityIn<D>(Kj, vj);
         float rel[3] = {vi[0] - vj[0], vi[1] - vj[1], vi[2] - vj[2]};
@@ -541,18 +547,20 @@ __device__ __forceinline__ void driftAndEnforce(const Params &P, const Frame &F,
 template <int D, int K>
 struct ContinuityVisit {
     static constexpr bool kSkipCoincident = true;
+    static constexpr bool kKinetic = true;
     const Params &P; const Frame &F;
     Smoothing<K, D> S;
     bool boundaryI, diffuses, corrected;
     float vi[3], devI, Li[3][3], gi[3];
     float total;
     __device__ bool accept(bool fluidJ) const { return !(boundaryI && !fluidJ); }
-    __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int, const float4 &B)
+    __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int, const float4 &B,
+                               const float4 &Kj)
     {
         const KernelAt k = S.at(h);
         const float grad = kernelGradient<K>(r * k.invH, k);    // (dW/dr) / r
         float vj[3];
-        velocityOf<D>(F, j, vj);
+        velocityIn<D>(Kj, vj);
         float dot = 0.0f;
         if (corrected) {
             for (int a = 0; a < D; ++a) {
@@ -631,18 +639,19 @@ continuityKernel(Params P, Frame F, Control *ctl, Enforcement E, int mode)
 template <int D, int K>
 struct XsphVisit {
     static constexpr bool kSkipCoincident = false;
+    static constexpr bool kKinetic = true;
     const Frame &F; const float *densities;
     Smoothing<K, D> S;
     float vi[3], rhoI, corr[3];
     __device__ bool accept(bool fluidJ) const { return fluidJ; }
-    __device__ void operator()(int j, const float *, float r, float h, bool, int, const float4 &B)
+    __device__ void operator()(int j, const float *, float r, float h, bool, int, const float4 &B, const float4 &Kj)
     {
         const KernelAt k = S.at(h);
         float w = kernelValue<K>(r * k.invH, k);
-        float rhoJ = densities ? densities[j] : densityOf<D>(F, j);
+        float rhoJ = densities ? densities[j] : densityIn<D>(Kj);
         float weight = massIn<D>(B) * w / (0.5f * (rhoI + rhoJ));
         float vj[3];
-        velocityOf<D>(F, j, vj);
+        velocityIn<D>(Kj, vj);
         for (int a = 0; a < D; ++a) corr[a] += weight * (vj[a] - vi[a]);
     }
 };

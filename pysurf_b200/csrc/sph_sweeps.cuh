@@ -179,7 +179,8 @@ struct Candidates {
 // Visit the neighbours of slot i.  Every neighbour j != i with r^2 < (2 h_ij)^2 (the table's
 // criterion) is counted in the walk's order; lane t of T takes those whose count k has k / 4 = t
 // mod T (the table's chunks t, t + T, ...).  Of those, the visitor gets (j, d, r, h_ij, fluidJ,
-// image, pb row of j) when Visitor::accept(fluidJ), and r >= 1e-12 where Visitor::kSkipCoincident.
+// image, pb row of j, kin row of j when Visitor::kKinetic) when Visitor::accept(fluidJ), and
+// r >= 1e-12 where Visitor::kSkipCoincident.
 // useTable: false forces the walk (the table kernel itself).
 template <int D, int T, class Visitor>
 __device__ __forceinline__ void forEachNeighbour(const Params &P, const Frame &F, int i, int t, float hI,
@@ -233,6 +234,8 @@ __device__ __forceinline__ void forEachNeighbour(const Params &P, const Frame &F
         pointIn<D>(A, pj);
         if (C.walking && (coarseDistance2<D>(pi, pj, offset) >= limit || j == i)) continue;
         const float4 B = __ldg(&F.pb[j]);
+        // the kinematic row too, with the others, when the visitor reads it
+        const float4 Kj = Visitor::kKinetic ? __ldg(&F.kin[j]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         const float hs = signedLengthIn<D>(A, B);
         const bool fluidJ = hs > 0.0f;
         // a lone lane may skip a rejected neighbour before its separation; a group counts every one
@@ -251,7 +254,7 @@ __device__ __forceinline__ void forEachNeighbour(const Params &P, const Frame &F
         }
         const float r = __fsqrt_rn(r2);
         if (Visitor::kSkipCoincident && r < 1.0e-12f) continue;
-        visit(j, d, r, h, fluidJ, image, B);
+        visit(j, d, r, h, fluidJ, image, B, Kj);
     }
 }
 
