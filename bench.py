@@ -247,18 +247,13 @@ def main() -> None:
         return
     import numpy as np
     import torch
-    import torch.distributed as dist
-    from datetime import timedelta
 
-    from pysurf_b200 import cases
-    from pysurf_b200._lib import C
+    from pysurf_b200 import cases, replicas
 
-    rank = int(os.environ.get('RANK', '0'))
-    world = int(os.environ.get('WORLD_SIZE', '1'))
-    local = int(os.environ.get('LOCAL_RANK', '0'))
+    ranks = replicas.ranksFromEnvironment()
+    rank, world, local = ranks.rank, ranks.world, ranks.local
     torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group('nccl', timeout=timedelta(seconds=300), device_id=torch.device('cuda', local))
+    replicas.initialize(ranks, 'nccl')
 
     case = buildCase(args)
     sums = cases.pairSumsFor(case, args.cells, device=local)
@@ -281,8 +276,7 @@ def main() -> None:
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     stageMs = []
-    if world > 1:
-        dist.barrier()
+    replicas.barrier(ranks)
     torch.cuda.synchronize()
     sampler = clockSampler(local)
     for k in range(args.steps):
@@ -297,12 +291,8 @@ def main() -> None:
     clocks = sampler()
     t, s, dt = sums.finishSteps()
     stepMs = [a.elapsed_time(b) for a, b in zip(starts, stops)]
-    totalMs = float(sum(stepMs))
-    if world > 1:
-        worst = torch.tensor([totalMs], device='cuda', dtype=torch.float64)
-        dist.all_reduce(worst, op=dist.ReduceOp.MAX)
-        totalMs = float(worst.item())
-        dist.barrier()
+    totalMs = replicas.maxOverRanks(float(sum(stepMs)), ranks)
+    replicas.barrier(ranks)
     value = world * case.fluidCount * args.steps / (totalMs / 1e3)
 
     names = sums.stageNames()
@@ -353,11 +343,7 @@ def main() -> None:
         end.synchronize()
         e2eMs = max(begin.elapsed_time(end), 0.0)
         wallMs = (time.perf_counter() - wall) * 1e3
-        e2eMs = max(e2eMs, wallMs)
-        if world > 1:
-            worst = torch.tensor([e2eMs], device='cuda', dtype=torch.float64)
-            dist.all_reduce(worst, op=dist.ReduceOp.MAX)
-            e2eMs = float(worst.item())
+        e2eMs = replicas.maxOverRanks(max(e2eMs, wallMs), ranks)
         e2e = {'value': world * case.fluidCount * e2eSteps / (e2eMs / 1e3), 'unit': METRIC,
                'h2d_bytes_per_step': bytesIn, 'd2h_bytes_per_step': bytesOut, 'steps': e2eSteps,
                'ms_per_step': e2eMs / e2eSteps}
@@ -376,8 +362,7 @@ def main() -> None:
                 'roofline': roofline, 'pair_flops': simt, 'stages_ms': stages, 'cpu_baseline': cpu,
                 'simulated_time_s': t}
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.destroy_process_group()
+    replicas.finalize(ranks)
 
 
 if __name__ == '__main__':
