@@ -58,6 +58,8 @@ def parseArgs():
     p.add_argument('--cells', type=int, default=None, help='cells per kernel support in the device cell list')
     p.add_argument('--threads', type=int, default=None, help='threads per particle in the sweeps (1, 2, 4, 8)')
     p.add_argument('--no-table', action='store_true', help='walk the cells in every sweep (no neighbour table)')
+    p.add_argument('--to-breaking', action='store_true',
+                   help='run the beach from its start to the breaking point and report the time it takes')
     p.add_argument('--no-e2e', action='store_true')
     p.add_argument('--no-cpu', action='store_true')
     return p.parse_args()
@@ -240,10 +242,41 @@ def referenceArm(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def toBreaking(args) -> None:
+    """The beach from its start to the breaking point on one GPU: the device steps, with the
+    breaking tracker reading the pulled fluid positions every 0.01 sqrt(d / g) (what the reference's
+    facade does, src/pysurf/BreakingWave.py:885-912); wall time from push to the breaking point."""
+    import torch
+    from pysurf_b200 import breaking, cases
+    case = buildCase(args)
+    sums = cases.pairSumsFor(case, args.cells)
+    sums.setSweepOptions(not args.no_table, args.threads or 4)
+    state = case.state.copy()
+    torch.cuda.synchronize()
+    start = time.perf_counter()
+    sums.push(state)
+    sums.setBoundary(case.boundary, state)
+    tracker, simulated, steps = breaking.runToBreaking(case, sums, endTime=12.0)
+    torch.cuda.synchronize()
+    wall = time.perf_counter() - start
+    point = tracker.breakingPoint
+    line = {'metric': 'seconds to the breaking point', 'value': wall, 'unit': 's', 'n_gpus': 1,
+            'higher_is_better': False, 'data': 'synthetic', 'config': config(case, flush=False),
+            'steps': steps, 'simulated_time_s': simulated, 'tracker_updates': len(tracker.times),
+            'particle_updates_per_s': case.fluidCount * steps / wall,
+            'breaking': None if point is None else {
+                'time_s': point.time, 'crest_x': point.crestX, 'Hb_over_d': point.crestHeight / case.info['depth'],
+                'hb_over_d': point.depth / case.info['depth'], 'lean': point.lean}}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     args = parseArgs()
     if args.impl == 'reference':
         referenceArm(args)
+        return
+    if args.to_breaking:
+        toBreaking(args)
         return
     import numpy as np
     import torch

@@ -1,0 +1,225 @@
+"""Where a 2D wave breaks on a beach: the breaking tracker of the reference's 2D facade.
+
+The reference reads the wave from the fluid's positions every 0.01 sqrt(d / g) of simulated time
+(src/pysurf/BreakingWave.py:885-912) with `BreakingTracker` (src/pysurf/waveBreaking.py:709-906).
+This module restates its 'cells' face measure, the one its first-order (lattice) start uses:
+
+    surfaceProfile  the free surface column by column: the highest fluid particle of each column one
+                    spacing wide, plus half a spacing (waveBreaking.py:129-162)
+    troughAhead     the lowest surface shoreward of the crest, after a three-column running median
+                    (waveBreaking.py:164-204)
+    faceLean        how far the crest's shoreward face leans past vertical, read in cells one spacing
+                    square above still water (waveBreaking.py:559-634)
+    waterlineX      the landward tip of the water sheet on the bed (waveBreaking.py:636-656)
+    BreakingTracker the crest's history and the breaking point: the first of `persistence`
+                    consecutive updates with the face leaning a spacing or more, with the crest past
+                    `searchFromX` (waveBreaking.py:709-906, the 'cells' branch)
+
+`runToBreaking` steps a `PairSums` on the device to the breaking point, pulling the fluid's
+positions at each tracker update.  The arithmetic is float64 numpy on the pulled positions, as the
+reference's is, so a device run and a float64 run of the same case are read by the same code.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+def surfaceProfile(positions: np.ndarray, x0: float, x1: float, width: float) -> tuple[np.ndarray, np.ndarray]:
+    """Column centres over [x0, x1) and each column's surface: its highest particle plus half a
+    column; NaN where a column holds no particle."""
+    count = max(1, int(math.ceil((x1 - x0) / width)))
+    centers = x0 + (np.arange(count) + 0.5) * width
+    column = np.floor((positions[:, 0] - x0) / width).astype(np.int64)
+    inside = (column >= 0) & (column < count)
+    top = np.full(count, -np.inf)
+    if inside.any():
+        np.maximum.at(top, column[inside], positions[inside, 1])
+    return centers, np.where(np.isfinite(top), top + 0.5 * width, np.nan)
+
+
+def troughAhead(centers: np.ndarray, elevation: np.ndarray, crestX: float, reach: float = np.inf) -> float:
+    """The least surface among the wet columns from the crest shoreward, up to the first dry column
+    or `reach` past the crest, after a running median over three columns with the ends reflected;
+    NaN when the first column ahead is dry."""
+    ahead = np.flatnonzero((centers > crestX) & (centers <= crestX + reach))
+    levels = np.asarray(elevation, dtype=float)[ahead]
+    dry = np.flatnonzero(~np.isfinite(levels))
+    if dry.size:
+        levels = levels[:dry[0]]
+    if levels.size == 0:
+        return float('nan')
+    if levels.size < 3:
+        return float(levels.max())
+    padded = np.concatenate([levels[1:2], levels, levels[-2:-1]])
+    windows = np.stack([padded[:-2], padded[1:-1], padded[2:]])
+    return float(np.median(windows, axis=0).min())
+
+
+def faceLean(positions: np.ndarray, crestX: float, stillWaterLevel: float, spacing: float, reach: float,
+             shoreLimit: float = np.inf) -> float:
+    """How far the crest's shoreward face leans forward of vertical [m]: negative sloping back, zero
+    vertical, positive curling over; -inf when fewer than two bands show a face.
+
+    The window runs from half a spacing behind the crest to `reach` ahead of it (or `shoreLimit`),
+    above still water plus half a spacing, in cells one spacing square.  A particle marks the four
+    cells its own square (a spacing across, centred on it) overlaps.  In each band the face is the
+    shoreward end of the run of marked cells that starts in one of the first two columns; bands whose
+    run reaches the window's end are left out.  The lean is the most any band's face stands
+    shoreward of the face of a band below it."""
+    start = crestX - 0.5 * spacing
+    end = min(crestX + reach, shoreLimit)
+    base = stillWaterLevel + 0.5 * spacing
+    x, z = positions[:, 0], positions[:, 1]
+    near = (x >= start - 0.5 * spacing) & (x < end + 0.5 * spacing) & (z > base - 0.5 * spacing)
+    if not near.any():
+        return -np.inf
+    column0 = np.floor((x[near] - 0.5 * spacing - start) / spacing).astype(np.int64)
+    band0 = np.floor((z[near] - 0.5 * spacing - base) / spacing).astype(np.int64)
+    columns = max(1, int(math.ceil((end - start) / spacing)))
+    marked = np.zeros((int(band0.max()) + 2, columns), dtype=bool)
+    for dc in (0, 1):
+        for db in (0, 1):
+            c, b = column0 + dc, band0 + db
+            keep = (c >= 0) & (c < columns) & (b >= 0)
+            marked[b[keep], c[keep]] = True
+    faces = []
+    for band in marked:
+        first = np.flatnonzero(band[:2])
+        if first.size == 0:
+            continue
+        run = band[first[0]:]
+        gaps = np.flatnonzero(~run)
+        if gaps.size == 0:
+            continue
+        faces.append(start + (first[0] + gaps[0]) * spacing)
+    if len(faces) < 2:
+        return -np.inf
+    faces = np.asarray(faces)
+    below = np.minimum.accumulate(faces)
+    return float((faces[1:] - below[:-1]).max())
+
+
+def waterlineX(positions: np.ndarray, bed, wetHeight: float, minimumParticles: int = 3) -> float:
+    """The landward tip of the water on the bed: the `minimumParticles`-th most landward particle
+    within `wetHeight` of the bed (so a lone droplet ahead of the sheet does not set it); NaN with
+    fewer."""
+    onBed = positions[positions[:, 1] - bed.elevation(positions[:, 0]) < wetHeight]
+    if len(onBed) < minimumParticles:
+        return float('nan')
+    return float(np.partition(onBed[:, 0], len(onBed) - minimumParticles)[len(onBed) - minimumParticles])
+
+
+@dataclass
+class BreakingPoint:
+    """The update the breaking point was read at: time, face lean, crest position and height above
+    still water (Hb), still water depth under the crest (hb), and the trough ahead."""
+    time: float
+    lean: float
+    crestX: float
+    crestHeight: float
+    depth: float
+    faceX: float = float('nan')
+    faceDepth: float = float('nan')
+    troughHeight: float = float('nan')
+
+    @property
+    def breakingIndex(self) -> float:
+        """Hb / hb."""
+        return self.crestHeight / self.depth if self.depth > 0.0 else float('inf')
+
+    @property
+    def waveHeight(self) -> float:
+        """Crest elevation less the trough's."""
+        return self.crestHeight - self.troughHeight
+
+
+@dataclass
+class BreakingTracker:
+    """The crest's history and the breaking point of a wave on a bed profile (the 'cells' measure):
+    the first of `persistence` consecutive updates whose face leans at least `leanThreshold`
+    spacings (less half a spacing, so rounding does not decide a tie), with the crest past
+    `searchFromX`."""
+    bed: object
+    spacing: float
+    leanThreshold: float = 1.0
+    faceReach: float = 1.0
+    searchFromX: float = -np.inf
+    persistence: int = 3
+    times: list = field(default_factory=list)
+    crestX: list = field(default_factory=list)
+    crestHeight: list = field(default_factory=list)
+    lean: list = field(default_factory=list)
+    waterline: list = field(default_factory=list)
+    breakingPoint: BreakingPoint | None = None
+    maxRunup: float = float('nan')
+    _candidate: BreakingPoint | None = field(default=None, repr=False)
+    _streak: int = field(default=0, repr=False)
+
+    @property
+    def breakingFinal(self) -> bool:
+        return self.breakingPoint is not None
+
+    def update(self, time: float, positions: np.ndarray) -> None:
+        """Read the wave from the fluid's positions (N, 2) at `time`."""
+        bed, s = self.bed, self.spacing
+        swl = bed.stillWaterLevel
+        centers, elevation = surfaceProfile(positions, bed.startX, bed.endX, s)
+        top = int(np.nanargmax(elevation))
+        crestX, crestHeight = float(centers[top]), float(elevation[top] - swl)
+        lean = faceLean(positions, crestX, swl, s, self.faceReach)
+        steep = lean > (self.leanThreshold - 0.5) * s
+        trough = troughAhead(centers, elevation, crestX, 2.0 * self.faceReach) - swl
+        tip = waterlineX(positions, bed, 2.0 * s)
+        if np.isfinite(tip):
+            runup = float(bed.elevation(tip) - swl)
+            self.maxRunup = runup if not np.isfinite(self.maxRunup) else max(self.maxRunup, runup)
+        self.times.append(time)
+        self.crestX.append(crestX)
+        self.crestHeight.append(crestHeight)
+        self.lean.append(lean)
+        self.waterline.append(tip)
+        if self.breakingPoint is not None:
+            return
+        if crestX >= self.searchFromX and steep:
+            if self._streak == 0:
+                self._candidate = BreakingPoint(time, lean, crestX, crestHeight, float(bed.depth(crestX)),
+                                                troughHeight=trough)
+            self._streak += 1
+            if self._streak >= self.persistence:
+                self.breakingPoint = self._candidate
+        else:
+            self._streak, self._candidate = 0, None
+
+
+def trackerFor(case) -> BreakingTracker:
+    """The facade's tracker for a beach case: face reach one depth, breaking looked for from the
+    toe on (src/pysurf/BreakingWave.py:763-765)."""
+    info = case.info
+    return BreakingTracker(case.boundary.bathymetry, case.spacing, faceReach=float(info['depth']),
+                           searchFromX=float(info['toeX']))
+
+
+def runToBreaking(case, sums, endTime: float, trackInterval: float = 0.01, maxSteps: int = 1 << 40):
+    """Step the case on the device from its start until the tracker's breaking point is final or
+    `endTime`, updating the tracker every `trackInterval` sqrt(d / g) of simulated time from the
+    pulled fluid positions (src/pysurf/BreakingWave.py:885-912).  `sums` holds the pushed state.
+    Returns (tracker, time, steps)."""
+    depth = float(case.info['depth'])
+    interval = trackInterval * math.sqrt(depth / 9.80665)
+    tracker = trackerFor(case)
+    fluid = np.asarray(case.state.isFluid, dtype=bool)
+    positions = None
+    time, step, dt = 0.0, 0, 0.0
+    nextTrack = interval
+    while time < endTime and not tracker.breakingFinal and step < maxSteps:
+        target = min(nextTrack, endTime)
+        time, step, dt = sums.advance(time, step, target, maxSteps, case.smoothingLength, case.cflNumber,
+                                      case.maxTimeStep, case.densityFilterInterval, dt)
+        if time >= nextTrack:
+            positions = sums.pullPositions(positions)
+            tracker.update(time, positions[fluid])
+            nextTrack += interval
+    return tracker, time, step

@@ -457,6 +457,15 @@ class PairSums:
             if value is not array:
                 array[:] = value
 
+    def pullPositions(self, out: np.ndarray | None = None) -> np.ndarray:
+        """The positions alone, in the caller's order (a tracker's read): into `out` when given."""
+        n, dim = self.count, self.dimensions
+        if out is None or out.shape != (n, dim) or out.dtype != np.float64 or not out.flags['C_CONTIGUOUS']:
+            out = np.empty((n, dim))
+        if n:
+            check(self._lib.sph_pull(self._handle, dptr(out), None, None, None, None, None, None, None), 'pull')
+        return out
+
     def residentRates(self, filterDensity: bool) -> tuple:
         """The first half of a device step; returns the largest fluid speed and acceleration."""
         speed, accel = _lib.C.c_double(0.0), _lib.C.c_double(0.0)

@@ -84,6 +84,10 @@ class Profile:
     def elevation(self, x):
         return np.interp(x, self.x, self.z)
 
+    def depth(self, x):
+        """Still water depth max(0, swl - z_b(x)) (src/pysurf/bathymetry.py:227-231)."""
+        return np.maximum(0.0, self.stillWaterLevel - self.elevation(x))
+
 
 @dataclass
 class BedBoundary:

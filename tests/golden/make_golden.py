@@ -407,17 +407,78 @@ def makeBeach():
     np.savez_compressed(os.path.join(HERE, 'beach.npz'), **out)
 
 
+def breakingShapes(bed, s, seed=5):
+    """Fluid position sets that exercise the breaking measures: a still beach, a steep crest, a lip
+    leaning one and three spacings over the face, and the same jittered."""
+    rng = np.random.default_rng(seed)
+    swl = bed.stillWaterLevel
+    x = np.arange(0.5 * s, 40.0, s)
+    z = np.arange(0.5 * s, 2.0, s)
+    gx, gz = np.meshgrid(x, z, indexing='xy')
+    gx, gz = gx.ravel(), gz.ravel()
+    bedZ = np.interp(gx, bed.x, bed.z)
+    shapes = {}
+    for name, crest, height, lip in (('still', 20.0, 0.0, 0), ('steep', 22.0, 0.45, 0), ('lip1', 24.0, 0.5, 1),
+                                     ('lip3', 25.0, 0.55, 3)):
+        surface = swl + height * np.exp(-((gx - crest) / 1.2) ** 2 * np.where(gx > crest, 6.0, 1.0))
+        keep = (gz >= bedZ + 0.5 * s) & (gz < surface)
+        points = np.column_stack([gx[keep], gz[keep]])
+        if lip:
+            # a tongue of water leaning `lip` spacings ahead of the face near the crest's top
+            top = swl + height
+            tongue = [(crest + 0.4 + (k + 1) * s, top - (j + 0.5) * s) for k in range(lip + 3) for j in range(3)]
+            points = np.vstack([points, np.asarray(tongue)])
+        shapes[name] = points
+        shapes[name + '_jitter'] = points + rng.uniform(-0.2 * s, 0.2 * s, points.shape)
+    return shapes
+
+
+def makeBreaking():
+    """The breaking measures of src/pysurf/waveBreaking.py ('cells' face) on synthetic fluid shapes over a
+    1:15 beach, and a tracker fed a sequence of them."""
+    from pysurf.bathymetry import Bathymetry
+    from pysurf.waveBreaking import (BreakingTracker, freeSurfaceProfile, frontFaceLean, troughAhead,
+                                     waterlineX)
+    out = {}
+    s = 1.0 / 16.0
+    beach = Bathymetry.planeBeach(depth=1.0, toeX=15.0, slope=1.0 / 15.0, endX=60.0)
+    out['bed/x'], out['bed/z'] = np.asarray(beach.x), np.asarray(beach.z)
+    shapes = breakingShapes(beach, s)
+    for name, points in shapes.items():
+        centers, elevation = freeSurfaceProfile(points, beach.startX, beach.endX, s)
+        crest = int(np.nanargmax(elevation))
+        crestX = float(centers[crest])
+        out[f'{name}/positions'] = points
+        out[f'{name}/centers'] = centers
+        out[f'{name}/elevation'] = elevation
+        out[f'{name}/lean'] = np.array(frontFaceLean(points, crestX, beach.stillWaterLevel, s, 1.0))
+        out[f'{name}/trough'] = np.array(troughAhead(centers, elevation, crestX, 2.0))
+        out[f'{name}/waterline'] = np.array(waterlineX(points, beach, 2.0 * s))
+    tracker = BreakingTracker(beach, s, faceReach=1.0, searchFromX=15.0)
+    sequence = ['still', 'steep', 'lip1', 'steep', 'lip1', 'lip1_jitter', 'lip1', 'lip3', 'steep']
+    for k, name in enumerate(sequence):
+        tracker.update(0.1 * (k + 1), shapes[name])
+    out['sequence'] = np.array(sequence)
+    point = tracker.breakingPoint
+    out['tracker/crestX'] = np.asarray(tracker.crestX)
+    out['tracker/crestHeight'] = np.asarray(tracker.crestHeight)
+    out['tracker/lean'] = np.asarray(tracker.lean)
+    out['tracker/waterline'] = np.asarray(tracker.waterline)
+    out['tracker/maxRunup'] = np.array(tracker.maxRunup)
+    out['tracker/point'] = np.array([point.time, point.lean, point.crestX, point.crestHeight, point.depth,
+                                     point.troughHeight]) if point is not None else np.full(6, np.nan)
+    np.savez_compressed(os.path.join(HERE, 'breaking.npz'), **out)
+
+
 def main():
     root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('PYSURF_REFERENCE', '')
     if not root or not os.path.isdir(root):
-        raise SystemExit('Give the reference checkout: make_golden.py /path/to/reference')
+        raise SystemExit('Give the reference checkout: make_golden.py /path/to/reference [fixture ...]')
     loadReference(root)
-    makeCellKeys()
-    makeClouds()
-    makeEnforcement()
-    makeSplit()
-    makeBeach()
-    makeRuns()
+    makers = {'cellkeys': makeCellKeys, 'clouds': makeClouds, 'enforce': makeEnforcement, 'split': makeSplit,
+              'beach': makeBeach, 'runs': makeRuns, 'breaking': makeBreaking}
+    for name in (sys.argv[2:] or list(makers)):
+        makers[name]()
     for name in sorted(os.listdir(HERE)):
         if name.endswith('.npz'):
             print(name, os.path.getsize(os.path.join(HERE, name)))
