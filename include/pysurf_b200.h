@@ -169,6 +169,29 @@ int sph_neighbor_list(SphSystem *sys, double radius, int64_t *offsets, int32_t *
  * and the rest appended in the caller's order.  *split returns how many split. */
 int sph_split(SphSystem *sys, const uint8_t *mask, double reference_density, double length_ratio, int64_t *split);
 
+/* ---- The breaking tracker's reads of the fluid (2D) -----------------------------------------
+ *
+ * The reference's BreakingTracker (src/pysurf/waveBreaking.py:709-906) reads the fluid's pulled
+ * positions every 0.01 sqrt(d / g) of simulated time (src/pysurf/BreakingWave.py:885-912).  These
+ * replace that pull with the three small things an update needs, computed on the device with the
+ * reference's float64 arithmetic term by term, so they equal the host's reads of pulled positions.
+ *
+ * sph_surface_tops: tops[c] = the largest height of a fluid particle in column
+ *   floor((x - x0) / width) = c, c < count; -inf for an empty column (freeSurfaceProfile,
+ *   src/pysurf/waveBreaking.py:129-162, before its half-column offset).
+ * sph_face_cells: marks (bands rows of columns bytes) = 1 where a fluid particle with
+ *   low_x <= x < high_x and z > low_z marks the cell (band0 + db, column0 + dc), db, dc in {0, 1},
+ *   column0 = floor((x - half - start) / spacing), band0 = floor((z - half - base) / spacing)
+ *   (frontFaceLean's occupancy, src/pysurf/waveBreaking.py:559-634).
+ * sph_bed_sheet: the x of every fluid particle less than wet_height above the bed profile
+ *   (bed_x, bed_z; numpy.interp between its vertices), in no set order, into xs (capacity
+ *   entries; *count gets how many there are) (waterlineX, src/pysurf/waveBreaking.py:636-656). */
+int sph_surface_tops(SphSystem *sys, double x0, double width, int64_t count, double *tops);
+int sph_face_cells(SphSystem *sys, double low_x, double high_x, double low_z, double half, double start,
+                   double base, double spacing, int64_t columns, int64_t bands, uint8_t *marks);
+int sph_bed_sheet(SphSystem *sys, const double *bed_x, const double *bed_z, int64_t bed_count, double wet_height,
+                  double *xs, int64_t capacity, int64_t *count);
+
 /* The same loop in three calls, for callers that overlap their own work with the steps:
  * sph_begin_steps sets the clock and the limits on the device; sph_enqueue_steps queues `count`
  * steps on the handle's stream and returns at once (steps past the limits do nothing);

@@ -71,6 +71,9 @@ SIGNATURES = {
     'sph_cell_order_key': [_pd, _i64, _i, _d, _pi64, _pi64, _i],
     'sph_neighbor_list': [_h, _d, _pi64, _pi32, _i64, _pi64],
     'sph_split': [_h, _pu8, _d, _d, _pi64],
+    'sph_surface_tops': [_h, _d, _d, _i64, _pd],
+    'sph_face_cells': [_h, _d, _d, _d, _d, _d, _d, _d, _i64, _i64, _pu8],
+    'sph_bed_sheet': [_h, _pd, _pd, _i64, _d, _pd, _i64, _pi64],
     'sph_last_advance_ms': [_h, _pd],
     'sph_begin_steps': [_h, _d, _i64, _d, _d, _i64, _d, _d, _d, _i64],
     'sph_enqueue_steps': [_h, _i64],

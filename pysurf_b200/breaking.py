@@ -15,9 +15,11 @@ This module restates its 'cells' face measure, the one its first-order (lattice)
                     consecutive updates with the face leaning a spacing or more, with the crest past
                     `searchFromX` (waveBreaking.py:709-906, the 'cells' branch)
 
-`runToBreaking` steps a `PairSums` on the device to the breaking point, pulling the fluid's
-positions at each tracker update.  The arithmetic is float64 numpy on the pulled positions, as the
-reference's is, so a device run and a float64 run of the same case are read by the same code.
+`runToBreaking` steps a `PairSums` on the device to the breaking point.  At each tracker update the
+device takes the reductions an update needs (each column's highest particle, the face window's
+cells, the x of the bed's water sheet: sph_surface_tops, sph_face_cells, sph_bed_sheet) with the
+float64 arithmetic of the host's measures, and only those come back; `updateOnDevice` then reads
+them as `update` reads pulled positions, to the same values.
 """
 from __future__ import annotations
 
@@ -85,6 +87,11 @@ def faceLean(positions: np.ndarray, crestX: float, stillWaterLevel: float, spaci
             c, b = column0 + dc, band0 + db
             keep = (c >= 0) & (c < columns) & (b >= 0)
             marked[b[keep], c[keep]] = True
+    return leanOfCells(marked, start, spacing)
+
+
+def leanOfCells(marked: np.ndarray, start: float, spacing: float) -> float:
+    """The lean from the window's marked cells (bands bottom up, columns from `start`)."""
     faces = []
     for band in marked:
         first = np.flatnonzero(band[:2])
@@ -165,14 +172,40 @@ class BreakingTracker:
     def update(self, time: float, positions: np.ndarray) -> None:
         """Read the wave from the fluid's positions (N, 2) at `time`."""
         bed, s = self.bed, self.spacing
-        swl = bed.stillWaterLevel
         centers, elevation = surfaceProfile(positions, bed.startX, bed.endX, s)
+        crestX = float(centers[int(np.nanargmax(elevation))])
+        lean = faceLean(positions, crestX, bed.stillWaterLevel, s, self.faceReach)
+        self.record(time, centers, elevation, lean, waterlineX(positions, bed, 2.0 * s))
+
+    def updateOnDevice(self, time: float, sums) -> None:
+        """The same reading from the state a `PairSums` holds, its reductions taken on the device
+        (column tops, face cells, the bed's sheet): a few kilobytes come back instead of the positions."""
+        bed, s = self.bed, self.spacing
+        swl = bed.stillWaterLevel
+        count = max(1, int(math.ceil((bed.endX - bed.startX) / s)))
+        centers = bed.startX + (np.arange(count) + 0.5) * s
+        tops = sums.surfaceTops(bed.startX, s, count)
+        elevation = np.where(np.isfinite(tops), tops + 0.5 * s, np.nan)
+        crestX = float(centers[int(np.nanargmax(elevation))])
+        # faceLean's window, its cells marked on the device; the bands reach the highest particle
+        start, end, base, half = crestX - 0.5 * s, crestX + self.faceReach, swl + 0.5 * s, 0.5 * s
+        columns = max(1, int(math.ceil((end - start) / s)))
+        highest = float(np.max(tops[np.isfinite(tops)])) if np.isfinite(tops).any() else base
+        bands = max(1, int(math.floor((highest - half - base) / s)) + 2)
+        marked = sums.faceCells(start - half, end + half, base - half, half, start, base, s, columns, bands)
+        lean = leanOfCells(marked, start, s) if marked.any() else -np.inf
+        sheet = sums.bedSheet(bed.x, bed.z, 2.0 * s)
+        tip = float(np.partition(sheet, sheet.size - 3)[sheet.size - 3]) if sheet.size >= 3 else float('nan')
+        self.record(time, centers, elevation, lean, tip)
+
+    def record(self, time: float, centers: np.ndarray, elevation: np.ndarray, lean: float, tip: float) -> None:
+        """Record an update from its reading: the surface profile, the face lean, the waterline."""
+        bed, s = self.bed, self.spacing
+        swl = bed.stillWaterLevel
         top = int(np.nanargmax(elevation))
         crestX, crestHeight = float(centers[top]), float(elevation[top] - swl)
-        lean = faceLean(positions, crestX, swl, s, self.faceReach)
         steep = lean > (self.leanThreshold - 0.5) * s
         trough = troughAhead(centers, elevation, crestX, 2.0 * self.faceReach) - swl
-        tip = waterlineX(positions, bed, 2.0 * s)
         if np.isfinite(tip):
             runup = float(bed.elevation(tip) - swl)
             self.maxRunup = runup if not np.isfinite(self.maxRunup) else max(self.maxRunup, runup)
@@ -202,11 +235,12 @@ def trackerFor(case) -> BreakingTracker:
                            searchFromX=float(info['toeX']))
 
 
-def runToBreaking(case, sums, endTime: float, trackInterval: float = 0.01, maxSteps: int = 1 << 40):
+def runToBreaking(case, sums, endTime: float, trackInterval: float = 0.01, maxSteps: int = 1 << 40,
+                  onDevice: bool = True):
     """Step the case on the device from its start until the tracker's breaking point is final or
-    `endTime`, updating the tracker every `trackInterval` sqrt(d / g) of simulated time from the
-    pulled fluid positions (src/pysurf/BreakingWave.py:885-912).  `sums` holds the pushed state.
-    Returns (tracker, time, steps)."""
+    `endTime`, updating the tracker every `trackInterval` sqrt(d / g) of simulated time
+    (src/pysurf/BreakingWave.py:885-912): from the device's reductions (`onDevice`), else from the
+    pulled fluid positions.  `sums` holds the pushed state.  Returns (tracker, time, steps)."""
     depth = float(case.info['depth'])
     interval = trackInterval * math.sqrt(depth / 9.80665)
     tracker = trackerFor(case)
@@ -219,7 +253,10 @@ def runToBreaking(case, sums, endTime: float, trackInterval: float = 0.01, maxSt
         time, step, dt = sums.advance(time, step, target, maxSteps, case.smoothingLength, case.cflNumber,
                                       case.maxTimeStep, case.densityFilterInterval, dt)
         if time >= nextTrack:
-            positions = sums.pullPositions(positions)
-            tracker.update(time, positions[fluid])
+            if onDevice:
+                tracker.updateOnDevice(time, sums)
+            else:
+                positions = sums.pullPositions(positions)
+                tracker.update(time, positions[fluid])
             nextTrack += interval
     return tracker, time, step

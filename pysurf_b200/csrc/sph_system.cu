@@ -126,6 +126,8 @@ struct SphSystem {
     Control *hCtl = nullptr;    // pinned
     // the neighbour table: listCap entries a slot (0: the sweeps walk the cells), stride capacity
     int *nbr = nullptr, *ncount = nullptr, *dMaxCount = nullptr;
+    void *surface = nullptr;        // the breaking tracker's read scratch
+    size_t surfaceBytes = 0;
     size_t nbrEntries = 0;
     int listCap = 0;
     int tableMode = 1;          // 0 never build the table, 1 build it when it fits the budget
@@ -568,6 +570,7 @@ int sph_destroy(SphSystem *sys)
     cudaFree(sys->sortBuffers.cellCount);
     cudaFree(sys->sortBuffers.partials);
     cudaFree(sys->dMaxCount);
+    cudaFree(sys->surface);
     cudaFree(sys->ctl);
     cudaFree(sys->bedX);
     cudaFree(sys->bedZ);
@@ -1449,6 +1452,88 @@ int sph_neighbor_list(SphSystem *sys, double radius, int64_t *offsets, int32_t *
     cudaFree(dOffsets);
     cudaFree(dRows);
     if (err != cudaSuccess) return fail(SPH_ERR_CUDA, cudaGetErrorString(err));
+    return SPH_OK;
+}
+
+// ---- the breaking tracker's reads ---------------------------------------------------------------
+
+// Scratch of at least `bytes` for the tracker's reads (grown as needed, kept with the handle).
+static int surfaceScratch(SphSystem *sys, size_t bytes, void **out)
+{
+    if (bytes > sys->surfaceBytes) {
+        cudaFree(sys->surface);
+        sys->surface = nullptr;
+        sys->surfaceBytes = 0;
+        CUDA_TRY(cudaMalloc(&sys->surface, bytes));
+        sys->surfaceBytes = bytes;
+    }
+    *out = sys->surface;
+    return SPH_OK;
+}
+
+int sph_surface_tops(SphSystem *sys, double x0, double width, int64_t count, double *tops)
+{
+    CHECK_SYS(sys);
+    if (!tops || count <= 0 || count > (1ll << 28) || !(width > 0.0)) return fail(SPH_ERR_INVALID, "bad columns");
+    if (!sys->resident) return fail(SPH_ERR_STATE, "no device state: call sph_push first");
+    if (sys->dim != 2) return fail(SPH_ERR_UNSUPPORTED, "the surface reads are 2D");
+    void *scratch = nullptr;
+    TRY(surfaceScratch(sys, sizeof(double) * 2 * (size_t)count, &scratch));
+    unsigned long long *bits = (unsigned long long *)scratch;
+    double *values = (double *)scratch + count;
+    launchSurfaceTops(sys->n, sys->master[sys->cur], 1, x0, width, count, bits, values, sys->stream);
+    CUDA_TRY(cudaGetLastError());
+    TRY(sys->download(tops, values, sizeof(double) * count));
+    CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    return SPH_OK;
+}
+
+int sph_face_cells(SphSystem *sys, double low_x, double high_x, double low_z, double half, double start,
+                   double base, double spacing, int64_t columns, int64_t bands, uint8_t *marks)
+{
+    CHECK_SYS(sys);
+    if (!marks || columns <= 0 || bands <= 0 || columns * bands > (1ll << 30) || !(spacing > 0.0))
+        return fail(SPH_ERR_INVALID, "bad window");
+    if (!sys->resident) return fail(SPH_ERR_STATE, "no device state: call sph_push first");
+    if (sys->dim != 2) return fail(SPH_ERR_UNSUPPORTED, "the surface reads are 2D");
+    const size_t bytes = (size_t)columns * (size_t)bands;
+    void *scratch = nullptr;
+    TRY(surfaceScratch(sys, bytes, &scratch));
+    launchFaceCells(sys->n, sys->master[sys->cur], 1, low_x, high_x, low_z, half, start, base, spacing, columns,
+                    bands, (uint8_t *)scratch, sys->stream);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(marks, scratch, bytes, cudaMemcpyDeviceToHost, sys->stream));
+    CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    return SPH_OK;
+}
+
+int sph_bed_sheet(SphSystem *sys, const double *bed_x, const double *bed_z, int64_t bed_count, double wet_height,
+                  double *xs, int64_t capacity, int64_t *count)
+{
+    CHECK_SYS(sys);
+    if (!bed_x || !bed_z || !count || bed_count < 2 || bed_count > (1 << 24) || capacity < 0 || (capacity && !xs))
+        return fail(SPH_ERR_INVALID, "bad bed or output");
+    if (!sys->resident) return fail(SPH_ERR_STATE, "no device state: call sph_push first");
+    if (sys->dim != 2) return fail(SPH_ERR_UNSUPPORTED, "the surface reads are 2D");
+    const int m = (int)bed_count, n = sys->n;
+    void *scratch = nullptr;
+    TRY(surfaceScratch(sys, sizeof(double) * (2 * (size_t)m + 1 + (size_t)n), &scratch));
+    double *bx = (double *)scratch, *bz = bx + m;
+    int *dCount = (int *)(bz + m);
+    double *out = bz + m + 1;
+    CUDA_TRY(cudaMemcpyAsync(bx, bed_x, sizeof(double) * m, cudaMemcpyHostToDevice, sys->stream));
+    CUDA_TRY(cudaMemcpyAsync(bz, bed_z, sizeof(double) * m, cudaMemcpyHostToDevice, sys->stream));
+    launchBedSheet(n, sys->master[sys->cur], 1, bx, bz, m, wet_height, out, dCount, sys->stream);
+    CUDA_TRY(cudaGetLastError());
+    int found = 0;
+    CUDA_TRY(cudaMemcpyAsync(&found, dCount, sizeof(int), cudaMemcpyDeviceToHost, sys->stream));
+    CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    *count = found;
+    const int64_t copy = std::min<int64_t>(found, capacity);
+    if (copy > 0) {
+        TRY(sys->download(xs, out, sizeof(double) * copy));
+        CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    }
     return SPH_OK;
 }
 

@@ -457,6 +457,33 @@ class PairSums:
             if value is not array:
                 array[:] = value
 
+    # -- the breaking tracker's reads (2D), on the device -- #
+
+    def surfaceTops(self, x0: float, width: float, count: int) -> np.ndarray:
+        """The highest fluid particle's height in each of `count` columns from x0 (-inf where empty)."""
+        tops = np.empty(int(count))
+        check(self._lib.sph_surface_tops(self._handle, float(x0), float(width), int(count), dptr(tops)),
+              'surfaceTops')
+        return tops
+
+    def faceCells(self, lowX: float, highX: float, lowZ: float, half: float, start: float, base: float,
+                  spacing: float, columns: int, bands: int) -> np.ndarray:
+        """The face window's marked cells, (bands, columns) booleans (see sph_face_cells)."""
+        marks = np.empty((int(bands), int(columns)), dtype=np.uint8)
+        check(self._lib.sph_face_cells(self._handle, float(lowX), float(highX), float(lowZ), float(half),
+                                       float(start), float(base), float(spacing), int(columns), int(bands),
+                                       marks.ctypes.data_as(_lib._pu8)), 'faceCells')
+        return marks.astype(bool)
+
+    def bedSheet(self, bedX, bedZ, wetHeight: float) -> np.ndarray:
+        """The x of the fluid particles less than `wetHeight` above the bed profile, in no set order."""
+        bx, bz = f64(bedX), f64(bedZ)
+        xs = np.empty(max(self.count, 1))
+        found = _lib.C.c_int64(0)
+        check(self._lib.sph_bed_sheet(self._handle, dptr(bx), dptr(bz), len(bx), float(wetHeight), dptr(xs),
+                                      len(xs), _lib.C.byref(found)), 'bedSheet')
+        return xs[:found.value]
+
     def pullPositions(self, out: np.ndarray | None = None) -> np.ndarray:
         """The positions alone, in the caller's order (a tracker's read): into `out` when given."""
         n, dim = self.count, self.dimensions

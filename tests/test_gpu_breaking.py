@@ -50,3 +50,26 @@ def test_the_device_breaks_where_the_float64_step_breaks():
     assert abs(a.time - b.time) <= 0.01 * b.time
     assert abs(a.crestX - b.crestX) <= 0.01 * b.crestX
     assert abs(a.crestHeight - b.crestHeight) <= 0.05 * b.crestHeight
+
+
+def test_the_device_reads_the_wave_as_the_host_does():
+    # the device's reductions give the tracker what pulled positions give it, to the last bit
+    case = cases.solitaryBeach(16)
+    sums = cases.pairSumsFor(case)
+    state = case.state.copy()
+    sums.push(state)
+    sums.setBoundary(case.boundary, state)
+    fluid = np.asarray(case.state.isFluid, dtype=bool)
+    onDevice, onHost = breaking.trackerFor(case), breaking.trackerFor(case)
+    time, step, dt = 0.0, 0, 0.0
+    for target in np.linspace(0.2, 4.0, 12):
+        time, step, dt = sums.advance(time, step, float(target), 1 << 40, case.smoothingLength, case.cflNumber,
+                                      case.maxTimeStep, 0, dt)
+        onDevice.updateOnDevice(time, sums)
+        onHost.update(time, sums.pullPositions()[fluid])
+    for name in ('crestX', 'crestHeight', 'lean', 'waterline'):
+        assert np.array_equal(getattr(onDevice, name), getattr(onHost, name), equal_nan=True), name
+    assert onDevice.maxRunup == onHost.maxRunup or (np.isnan(onDevice.maxRunup) and np.isnan(onHost.maxRunup))
+    assert (onDevice.breakingPoint is None) == (onHost.breakingPoint is None)
+    if onHost.breakingPoint is not None:
+        assert onDevice.breakingPoint == onHost.breakingPoint
