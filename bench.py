@@ -60,6 +60,14 @@ def parseArgs():
     p.add_argument('--no-table', action='store_true', help='walk the cells in every sweep (no neighbour table)')
     p.add_argument('--to-breaking', action='store_true',
                    help='run the beach from its start to the breaking point and report the time it takes')
+    p.add_argument('--sweep', type=int, default=0,
+                   help='solve this many cases of the seeded 256-case beach sweep to their breaking points, '
+                        'case by case and then batched, and report both')
+    p.add_argument('--slots', type=int, default=16, help='concurrent cases in the batched sweep and the server')
+    p.add_argument('--serve', type=int, default=0,
+                   help='serve this many requests arriving as a Poisson stream (see serveBench)')
+    p.add_argument('--horizon-scale', type=float, default=0.1,
+                   help='the served requests horizons, U(2, 6) s of simulated time times this')
     p.add_argument('--no-e2e', action='store_true')
     p.add_argument('--no-cpu', action='store_true')
     return p.parse_args()
@@ -270,8 +278,41 @@ def toBreaking(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def sweepBench(args) -> None:
+    """BASELINE config 4 at the size asked: the first --sweep cases of the seeded sweep (slope
+    log-U(1/35, 1/8), H/d U(0.2, 0.6), 16-64 ppd) to their breaking points, first one after another,
+    then --slots at a time; every batched result must equal its case-by-case one."""
+    import numpy as np
+    from pysurf_b200 import batch
+    specs = batch.drawSweep(256, seed=0)[:args.sweep]
+    runs = {}
+    for name, slots in (('case_by_case', 1), ('batched', args.slots)):
+        start = time.perf_counter()
+        results = batch.BatchRunner(slots=slots).run(specs)
+        runs[name] = (time.perf_counter() - start, results)
+    (serial, alone), (batched, mixed) = runs['case_by_case'], runs['batched']
+    same = all(a.key() == m.key() and a.error is None and m.error is None for a, m in zip(alone, mixed))
+    updates = sum(r.fluidParticles * r.steps for r in mixed)
+    broke = sum(1 for r in mixed if r.breakingTime == r.breakingTime)
+    seconds = np.array([r.seconds for r in mixed])
+    line = {'metric': 'cases/h', 'value': 3600.0 * len(specs) / batched, 'unit': 'cases/h', 'n_gpus': 1,
+            'higher_is_better': True, 'data': 'synthetic',
+            'config': {'workload': f'the first {len(specs)} cases of the 256-case 2D beach sweep (seed 0), each to '
+                                   f'its breaking point', 'slots': args.slots,
+                       'fluid_particles': [r.fluidParticles for r in mixed]},
+            'case_by_case_cases_per_h': 3600.0 * len(specs) / serial, 'speedup': serial / batched,
+            'seconds_batched': batched, 'seconds_case_by_case': serial, 'broke': broke,
+            'results_identical_alone_and_batched': same, 'particle_updates_per_s': updates / batched,
+            'case_seconds_p50': float(np.percentile(seconds, 50)),
+            'case_seconds_p99': float(np.percentile(seconds, 99))}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     args = parseArgs()
+    if args.sweep:
+        sweepBench(args)
+        return
     if args.impl == 'reference':
         referenceArm(args)
         return
