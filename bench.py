@@ -308,8 +308,48 @@ def sweepBench(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def ridgeRequest(spec):
+    from pysurf_b200 import cases
+    return cases.ridgeWave3D(spec.ppd)
+
+
+def serveBench(args) -> None:
+    """BASELINE config 5 at a reduced size: --serve requests arriving as a Poisson stream at 20 a
+    second (seed 0), 80% 2D beaches drawn as the sweep draws them and 20% 3D ridges at 8-16 ppd (0.4M
+    to 2.4M particles), each run for U(2, 6) s of simulated time times --horizon-scale; admitted as
+    slots (--slots) and device memory free up, solved beside the requests in flight."""
+    import numpy as np
+    from pysurf_b200 import batch
+    rng = np.random.default_rng(0)
+    sweep = batch.drawSweep(args.serve, seed=0)
+    arrivals = batch.poissonArrivals(args.serve, 20.0, seed=0)
+    requests = []
+    for k in range(args.serve):
+        horizon = float(rng.uniform(2.0, 6.0)) * args.horizon_scale
+        if rng.uniform() < 0.2:
+            spec = batch.CaseSpec(k, 0.0, 0.5, int(rng.integers(8, 17)), endTime=horizon, toBreaking=False)
+            requests.append(batch.Request(float(arrivals[k]), spec, ridgeRequest))
+        else:
+            base = sweep[k]
+            spec = batch.CaseSpec(k, base.slope, base.height, base.ppd, endTime=horizon, toBreaking=False)
+            requests.append(batch.Request(float(arrivals[k]), spec))
+    out = batch.serve(requests, slots=args.slots)
+    results = out['results']
+    line = {'metric': 'p99 latency', 'value': out['latency_p99_s'], 'unit': 's', 'n_gpus': 1,
+            'higher_is_better': False, 'data': 'synthetic',
+            'config': {'workload': f'{args.serve} requests, Poisson 20/s, 80% 2D beach 16-64 ppd, 20% 3D ridge '
+                                   f'8-16 ppd, horizons U(2, 6) s x {args.horizon_scale}', 'slots': args.slots},
+            'latency_p50_s': out['latency_p50_s'], 'latency_p99_s': out['latency_p99_s'],
+            'seconds': out['seconds'], 'particle_updates_per_s': out['particle_updates_per_s'],
+            'failed': sum(1 for r in results if r.error), 'particles': [r.particles for r in results]}
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     args = parseArgs()
+    if args.serve:
+        serveBench(args)
+        return
     if args.sweep:
         sweepBench(args)
         return
