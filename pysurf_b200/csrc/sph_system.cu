@@ -744,6 +744,7 @@ static int loadState(SphSystem *sys, int64_t count, const double *positions, con
                      lengths ? sh : nullptr, sys->h, sys->master[0], sys->stream);
     CUDA_TRY(cudaGetLastError());
     sys->framed = false;
+    sys->cellsFresh = false;    // new positions: the cell list is sorted again before its next use
     return SPH_OK;
 }
 
@@ -1471,6 +1472,29 @@ static int surfaceScratch(SphSystem *sys, size_t bytes, void **out)
     return SPH_OK;
 }
 
+int sph_split_crest_zone(SphSystem *sys, double x0, double y0, double width, int64_t nx, int64_t ny,
+                         double threshold, double min_mass, double reference_density, double length_ratio,
+                         int64_t *split)
+{
+    CHECK_SYS(sys);
+    if (!split || nx <= 0 || ny <= 0 || nx * ny > (1ll << 28) || !(width > 0.0))
+        return fail(SPH_ERR_INVALID, "bad columns");
+    if (!sys->resident) return fail(SPH_ERR_STATE, "no device state: call sph_push first");
+    *split = 0;
+    const int n = sys->n;
+    if (n == 0) return SPH_OK;
+    void *scratch = nullptr;
+    TRY(surfaceScratch(sys, sizeof(unsigned long long) * (size_t)nx * (size_t)ny, &scratch));
+    launchCrestZone(n, sys->master[sys->cur], sys->dim, x0, y0, width, nx, ny, (unsigned long long *)scratch,
+                    threshold, min_mass, sys->dStageU8, sys->stream);
+    CUDA_TRY(cudaGetLastError());
+    // the zone in the caller's order, then the split as sph_split takes it
+    std::vector<uint8_t> mask(n);
+    CUDA_TRY(cudaMemcpyAsync(mask.data(), sys->dStageU8, n, cudaMemcpyDeviceToHost, sys->stream));
+    CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    return sph_split(sys, mask.data(), reference_density, length_ratio, split);
+}
+
 int sph_surface_tops(SphSystem *sys, double x0, double width, int64_t count, double *tops)
 {
     CHECK_SYS(sys);
@@ -1582,6 +1606,7 @@ int sph_split(SphSystem *sys, const uint8_t *mask, double reference_density, dou
     sys->hMin = hMin;
     sys->mixedH = mixed;
     sys->framed = false;
+    sys->cellsFresh = false;    // the daughters have no cell yet: the next use sorts again
     sys->graphDirty = true;
     sys->listDirty = true;
     *split = count;
