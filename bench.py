@@ -68,6 +68,8 @@ def parseArgs():
                    help='serve this many requests arriving as a Poisson stream (see serveBench)')
     p.add_argument('--horizon-scale', type=float, default=0.1,
                    help='the served requests horizons, U(2, 6) s of simulated time times this')
+    p.add_argument('--refine', action='store_true',
+                   help='split the crest zone (surface above 0.3 H) into daughters of h/2 before timing')
     p.add_argument('--no-e2e', action='store_true')
     p.add_argument('--no-cpu', action='store_true')
     return p.parse_args()
@@ -379,6 +381,13 @@ def main() -> None:
     sums.setBoundary(case.boundary, state)
     neighbours = meanNeighbours(case)
     h, cfl, maxdt = case.smoothingLength, case.cflNumber, case.maxTimeStep
+    refined = None
+    if args.refine:
+        refined = cases.refineCrestZone(sums, case)
+        h = 0.5 * case.smoothingLength     # the shortest length sets the time step
+        neighbours = float('nan')           # mixed lengths: the start's count no longer stands
+        args.no_e2e = args.no_cpu = True    # the host copy no longer matches the device's count
+    fluidCount = case.fluidCount + (refined or 0) * (2 ** case.dimensions - 1)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device='cuda')     # 256 MiB, twice the L2
 
     # warm-up steps (untimed), then exactly K timed steps
@@ -407,7 +416,7 @@ def main() -> None:
     stepMs = [a.elapsed_time(b) for a, b in zip(starts, stops)]
     totalMs = replicas.maxOverRanks(float(sum(stepMs)), ranks)
     replicas.barrier(ranks)
-    value = world * case.fluidCount * args.steps / (totalMs / 1e3)
+    value = world * fluidCount * args.steps / (totalMs / 1e3)
 
     names = sums.stageNames()
     stages = {name: float(np.mean([m[i] for m in stageMs])) for i, name in enumerate(names)}
@@ -415,15 +424,15 @@ def main() -> None:
     peaks = measuredPeaks()
     kernelMs = stages[dominant]
     unitBytes = ALGORITHMIC_BYTES[case.dimensions]
-    achieved = unitBytes * case.fluidCount / (kernelMs / 1e3) / 1e9
-    pairFlop = case.fluidCount * neighbours * FLOP_PER_PAIR
+    achieved = unitBytes * fluidCount / (kernelMs / 1e3) / 1e9
+    pairFlop = fluidCount * neighbours * FLOP_PER_PAIR
     simt = {'flop_per_pair': FLOP_PER_PAIR, 'neighbours_per_fluid_particle': neighbours,
             'achieved_tflops': pairFlop / (totalMs / args.steps / 1e3) / 1e12, 'peak_tflops': FP32_SIMT_TFLOPS,
             'peak_source': 'nominal FP32 SIMT: 148 SMs x 128 lanes x 2 flop x 1965 MHz'}
     simt['frac'] = simt['achieved_tflops'] / FP32_SIMT_TFLOPS
     roofline = {'bound': 'hbm', 'kernel': dominant, 'achieved': achieved, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
                 'frac': achieved / peaks['hbm_gbs'], 'traffic': profiledTraffic(case), 'peak_source': peaks['source'],
-                'kernel_ms': kernelMs, 'bytes_per_update': unitBytes, 'step_hbm_frac': unitBytes * case.fluidCount /
+                'kernel_ms': kernelMs, 'bytes_per_update': unitBytes, 'step_hbm_frac': unitBytes * fluidCount /
                 (totalMs / args.steps / 1e3) / 1e9 / peaks['hbm_gbs']}
 
     # end to end through the public API with host buffers: push, one step, pull, every step
@@ -458,7 +467,7 @@ def main() -> None:
         e2eMs = max(begin.elapsed_time(end), 0.0)
         wallMs = (time.perf_counter() - wall) * 1e3
         e2eMs = replicas.maxOverRanks(max(e2eMs, wallMs), ranks)
-        e2e = {'value': world * case.fluidCount * e2eSteps / (e2eMs / 1e3), 'unit': METRIC,
+        e2e = {'value': world * fluidCount * e2eSteps / (e2eMs / 1e3), 'unit': METRIC,
                'h2d_bytes_per_step': bytesIn, 'd2h_bytes_per_step': bytesOut, 'steps': e2eSteps,
                'ms_per_step': e2eMs / e2eSteps}
 
@@ -471,6 +480,7 @@ def main() -> None:
                 'warmup': args.warmup, 'ms_per_step': totalMs / args.steps, 'higher_is_better': True,
                 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32 sums, f64 state', 'data': 'synthetic',
                 'config': dict(config(case), parallelism=f'replicas{world}' if world > 1 else 'single',
+                               crest_zone_split=refined, fluid_particles_after_split=fluidCount,
                                **sweepConfig(sums, not args.no_table, args.threads or 4)),
                 'clocks': clocks, 'e2e': e2e, 'gpu_launches': launchesPerStep * args.steps,
                 'roofline': roofline, 'pair_flops': simt, 'stages_ms': stages, 'cpu_baseline': cpu,

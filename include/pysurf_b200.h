@@ -169,6 +169,15 @@ int sph_neighbor_list(SphSystem *sys, double radius, int64_t *offsets, int32_t *
  * and the rest appended in the caller's order.  *split returns how many split. */
 int sph_split(SphSystem *sys, const uint8_t *mask, double reference_density, double length_ratio, int64_t *split);
 
+/* Crest-zone refinement on the device: every fluid particle of mass at least min_mass (one not yet
+ * split) whose column -- columns `width` across from (x0, y0), nx by ny of them (ny 1 in 2D) --
+ * has its highest fluid particle above `threshold` (the surface's height), splits as sph_split
+ * splits it; *split gets how many did.  The zone of BreakingWave3D._refineCrest
+ * (src/pysurf/BreakingWave3D.py:530-576) read as the columns where the surface stands high. */
+int sph_split_crest_zone(SphSystem *sys, double x0, double y0, double width, int64_t nx, int64_t ny,
+                         double threshold, double min_mass, double reference_density, double length_ratio,
+                         int64_t *split);
+
 /* ---- The breaking tracker's reads of the fluid (2D) -----------------------------------------
  *
  * The reference's BreakingTracker (src/pysurf/waveBreaking.py:709-906) reads the fluid's pulled

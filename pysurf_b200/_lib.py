@@ -72,6 +72,7 @@ SIGNATURES = {
     'sph_neighbor_list': [_h, _d, _pi64, _pi32, _i64, _pi64],
     'sph_split': [_h, _pu8, _d, _d, _pi64],
     'sph_surface_tops': [_h, _d, _d, _i64, _pd],
+    'sph_split_crest_zone': [_h, _d, _d, _d, _i64, _i64, _d, _d, _d, _d, _pi64],
     'sph_face_cells': [_h, _d, _d, _d, _d, _d, _d, _d, _i64, _i64, _pu8],
     'sph_bed_sheet': [_h, _pd, _pd, _i64, _d, _pd, _i64, _pi64],
     'sph_last_advance_ms': [_h, _pd],

@@ -376,6 +376,22 @@ def ridgeWave3D(particlesPerDepth: int = 32, depth: float = 1.0, height: float =
                       'tank': [length, width], 'ppd': particlesPerDepth, 'layers': layers})
 
 
+def refineCrestZone(sums, case: Case, share: float = 0.3, lengthRatio: float = 0.5) -> int:
+    """The crest-zone split of BASELINE's 3D ridge workload: every fluid particle not yet split, in a
+    column (one spacing across) whose surface stands more than `share` H above still water, splits
+    into 2^dim daughters of h times `lengthRatio` (src/pysurf/sphRefinement.py:136-190), on the
+    device.  Returns how many split."""
+    info, s = case.info, case.spacing
+    depth = float(info['depth'])
+    height = float(info['H/d']) * depth
+    lower, upper = case.domainMin, case.domainMax
+    nx = int(math.ceil((upper[0] - lower[0]) / s))
+    ny = int(math.ceil((upper[1] - lower[1]) / s)) if case.dimensions == 3 else 1
+    fluidMass = float(np.max(case.state.masses[case.state.isFluid]))
+    return sums.splitCrestZone(lower[0], lower[1], s, nx, ny, depth + share * height, 0.999 * fluidMass,
+                               case.referenceDensity, lengthRatio)
+
+
 def pairSumsFor(case: Case, cellsPerSupport: int | None = None, device: int = 0):
     """A PairSums set up for a case: the switches WcsphSolver.__init__ sets (src/pysurf/sphSolver.py:1499-1518)
     and the physics WcsphSolver.advance sets (src/pysurf/sphSolver.py:1970-1972)."""

@@ -86,6 +86,9 @@ void launchFaceCells(int n, const MasterView &M, int vertical, double lowX, doub
                      cudaStream_t st);
 void launchBedSheet(int n, const MasterView &M, int vertical, const double *bx, const double *bz, int m,
                     double wetHeight, double *out, int *count, cudaStream_t st);
+void launchCrestZone(int n, const MasterView &M, int dim, double x0, double y0, double width, long long nx,
+                     long long ny, unsigned long long *tops, double threshold, double minMass, uint8_t *chosen,
+                     cudaStream_t st);
 void launchSplit(int n, int dim, const MasterView &M, const uint8_t *chosen, const int *rank, double rho0,
                  double lengthRatio, int total, cudaStream_t st);
 

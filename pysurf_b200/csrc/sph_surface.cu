@@ -1,4 +1,4 @@
-// sph_surface.cu -- the breaking tracker's reads of the fluid, on the device.
+// sph_surface.cu -- the breaking tracker's reads of the fluid, and the crest zone, on the device.
 //
 // A tracker update needs three small things from the fluid's positions, not the positions
 // themselves: each column's highest particle (the free surface, src/pysurf/waveBreaking.py:129-162),
@@ -92,7 +92,51 @@ __global__ void bedSheetKernel(int n, const double *x, const double *z, const ui
     if (__dsub_rn(z[s], bedElevation(xv, bx, bz, m)) < wetHeight) out[atomicAdd(count, 1)] = xv;
 }
 
+// The crest zone: tops[cy * nx + cx] = the highest fluid particle (vertical axis dim - 1) of the
+// column (cx, cy) of width `width` from (x0, y0) (cy = 0 in 2D).
+__global__ void columnTopsKernel(int n, MasterView M, int dim, double x0, double y0, double width, long long nx,
+                                 long long ny, unsigned long long *tops)
+{
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n || !M.fluid[s]) return;
+    const double cx = floor((M.x[0][s] - x0) / width);
+    const double cy = dim == 3 ? floor((M.x[1][s] - y0) / width) : 0.0;
+    if (!(cx >= 0.0 && cx < (double)nx && cy >= 0.0 && cy < (double)ny)) return;
+    atomicMax(&tops[(long long)cy * nx + (long long)cx], orderedBits(M.x[dim - 1][s]));
+}
+
+// chosen[caller index] = 1 for a fluid particle of at least minMass (not yet split) whose column's
+// top stands above `threshold`.
+__global__ void crestZoneKernel(int n, MasterView M, int dim, double x0, double y0, double width, long long nx,
+                                long long ny, const unsigned long long *tops, double threshold, double minMass,
+                                uint8_t *chosen)
+{
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    bool zone = false;
+    if (M.fluid[s] && M.m[s] >= minMass) {
+        const double cx = floor((M.x[0][s] - x0) / width);
+        const double cy = dim == 3 ? floor((M.x[1][s] - y0) / width) : 0.0;
+        if (cx >= 0.0 && cx < (double)nx && cy >= 0.0 && cy < (double)ny) {
+            const unsigned long long top = tops[(long long)cy * nx + (long long)cx];
+            zone = top != 0 && fromOrderedBits(top) > threshold;
+        }
+    }
+    chosen[M.orig[s]] = zone ? 1 : 0;
+}
+
 static inline int blocksFor(long long n, int block) { return (int)((n + block - 1) / block); }
+
+void launchCrestZone(int n, const MasterView &M, int dim, double x0, double y0, double width, long long nx,
+                     long long ny, unsigned long long *tops, double threshold, double minMass, uint8_t *chosen,
+                     cudaStream_t st)
+{
+    cudaMemsetAsync(tops, 0, sizeof(unsigned long long) * nx * ny, st);
+    if (n == 0) return;
+    columnTopsKernel<<<blocksFor(n, 256), 256, 0, st>>>(n, M, dim, x0, y0, width, nx, ny, tops);
+    crestZoneKernel<<<blocksFor(n, 256), 256, 0, st>>>(n, M, dim, x0, y0, width, nx, ny, tops, threshold, minMass,
+                                                       chosen);
+}
 
 void launchSurfaceTops(int n, const MasterView &M, int vertical, double x0, double width, long long count,
                        unsigned long long *scratch, double *out, cudaStream_t st)

@@ -582,6 +582,19 @@ class PairSums:
         self.count = int(total.value)
         return int(count.value)
 
+    def splitCrestZone(self, x0: float, y0: float, width: float, nx: int, ny: int, threshold: float,
+                       minMass: float, referenceDensity: float, lengthRatio: float = 0.5) -> int:
+        """Split, on the device, every unsplit fluid particle (mass at least `minMass`) whose column
+        (`width` across from (x0, y0), nx by ny) has its surface above `threshold`; returns how many."""
+        count = _lib.C.c_int64(0)
+        check(self._lib.sph_split_crest_zone(self._handle, float(x0), float(y0), float(width), int(nx), int(ny),
+                                             float(threshold), float(minMass), float(referenceDensity),
+                                             float(lengthRatio), _lib.C.byref(count)), 'splitCrestZone')
+        total = _lib.C.c_int64(0)
+        check(self._lib.sph_count(self._handle, _lib.C.byref(total)))
+        self.count = int(total.value)
+        return int(count.value)
+
     def pullState(self) -> dict:
         """The whole device state in the caller's order, masses, lengths and flags included."""
         n, dim = self.count, self.dimensions
