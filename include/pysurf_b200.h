@@ -78,6 +78,16 @@ int sph_set_wall_pressure(SphSystem *sys, int extrapolated);
 int sph_set_negative_pressure(SphSystem *sys, int enabled);
 int sph_set_continuity_correction(SphSystem *sys, int enabled);
 int sph_set_viscosity_limiter(SphSystem *sys, int enabled);
+/* PairSums.setClosure (src/pysurf/sphGpu.py:1752-1779): the delta-LES-SPH closure on or off, with
+ * c0, rho0 and the water's kinematic viscosity.  When on, every step takes each particle's alpha_i
+ * and delta_i from its velocity gradient (src/pysurf/sphSolver.py:1232-1274), adds the closure's
+ * viscous term to every fluid pair's accelerations and takes each fluid pair's diffusion
+ * coefficient as the harmonic mean of the two deltas. */
+int sph_set_closure(SphSystem *sys, int enabled, double sound_speed, double reference_density,
+                    double kinematic_viscosity);
+/* PairSums.closureCoefficients (src/pysurf/sphGpu.py:1841-1853): alpha_i and delta_i, caller order. */
+int sph_closure_coefficients(SphSystem *sys, const double *velocities, const double *densities, double *alphas,
+                             double *deltas);
 /* PairSums.setPhysics (src/pysurf/sphGpu.py:2173-2205); density_floor in kg/m^3, 0 for none. */
 int sph_set_physics(SphSystem *sys, double reference_density, double sound_speed, double alpha,
                     double boundary_viscosity_factor, const double *gravity, double xsph_epsilon,

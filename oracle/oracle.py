@@ -50,7 +50,8 @@ class StepParams(C.Structure):
                 ('wallExtrapolated', C.c_int), ('tension', C.c_int), ('corrected', C.c_int),
                 ('limited', C.c_int), ('cfl', C.c_double), ('maxTimeStep', C.c_double),
                 ('filterDensity', C.c_int), ('boundaryKind', C.c_int), ('lower', C.c_double * 3),
-                ('upper', C.c_double * 3), ('openTop', C.c_int), ('bed', BedParams), ('field', FieldParams)]
+                ('upper', C.c_double * 3), ('openTop', C.c_int), ('bed', BedParams), ('field', FieldParams),
+                ('closure', C.c_int), ('viscosity', C.c_double)]
 
 
 def lib():
@@ -68,9 +69,11 @@ def lib():
         L.orx_correction_matrices.argtypes = sysargs + [C.c_long, _dp, _dp]
         L.orx_density_gradients.argtypes = sysargs + [C.c_long, _dp, _dp, _dp]
         L.orx_accelerations.argtypes = sysargs + [C.c_long, _dp, _dp, _dp, _vp, C.c_double, C.c_double,
-                                                  C.c_double, _dp, C.c_int, _dp]
+                                                  C.c_double, _dp, C.c_int, C.c_int, C.c_double, C.c_double, _vp,
+                                                  _dp]
         L.orx_continuity.argtypes = sysargs + [C.c_long, _dp, _dp, _vp, _vp, C.c_int, C.c_double, C.c_double,
-                                               C.c_double, C.c_double, C.c_int, _dp]
+                                               C.c_double, C.c_double, C.c_int, C.c_int, _vp, _dp]
+        L.orx_closure_coefficients.argtypes = sysargs + [C.c_long, _dp, C.c_double, _dp, _dp]
         L.orx_xsph.argtypes = sysargs + [C.c_long, _dp, _dp, C.c_double, _dp]
         L.orx_shepard.argtypes = sysargs + [C.c_long, _dp, _dp]
         L.or_step.argtypes = [C.POINTER(StepParams), C.c_long, _dp, _dp, _dp, _dp, _dp, _u8, _dp, _dp]
@@ -157,16 +160,32 @@ class System:
         return out
 
     def pairAccelerations(self, velocities, densities, pressures, c0, alpha, boundaryFactor, gravity,
-                          gradients=None):
+                          gradients=None, limited=None, closure=None):
+        """limited: the limiter (by default on when `gradients` are given); closure: None, or
+        (alphas, viscosity, rho0) for the delta-LES-SPH term (src/pysurf/sphSolver.py:1283-1326)."""
         out = np.empty((self.n, self.dim))
         G = None if gradients is None else _f64(gradients)
+        limited = G is not None if limited is None else bool(limited)
+        alphas, waterTerm, rho0 = None, 0.0, 1000.0
+        if closure is not None:
+            alphas = _f64(closure[0])
+            waterTerm = 2.0 * (self.dim + 2) * float(closure[1]) / c0
+            rho0 = float(closure[2])
         lib().orx_accelerations(*self._args(), self.n, self._vec(velocities), _f64(densities), _f64(pressures),
                                 None if G is None else G.ctypes.data_as(C.c_void_p), c0, alpha, boundaryFactor,
-                                _f64(np.resize(gravity, 3)), int(G is not None), out)
+                                _f64(np.resize(gravity, 3)), int(limited), int(closure is not None), waterTerm, rho0,
+                                None if alphas is None else alphas.ctypes.data_as(C.c_void_p), out)
         return out
 
+    def closureCoefficients(self, gradients, c0):
+        """src/pysurf/sphSolver.py:1232-1274: each particle's alpha_i and delta_i."""
+        alphas, deltas = np.empty(self.n), np.empty(self.n)
+        lib().orx_closure_coefficients(*self._args(), self.n, _f64(gradients), c0, alphas, deltas)
+        return alphas, deltas
+
     def continuityRate(self, velocities, densities=None, mode='none', delta=0.1, c0=20.0, rho0=1000.0,
-                       gravity=9.81, corrections=None, gradients=None):
+                       gravity=9.81, corrections=None, gradients=None, deltas=None):
+        """deltas: each particle's closure delta_i, whose pair harmonic mean replaces `delta`."""
         modes = {'none': 0, 'molteni': 1, 'hydrostatic': 2, 'antuono': 3}
         rho = _f64(densities if densities is not None else np.full(self.n, rho0))
         L = None if corrections is None else _f64(corrections)
@@ -177,7 +196,8 @@ class System:
         lib().orx_continuity(*self._args(), self.n, self._vec(velocities), rho,
                              None if L is None else L.ctypes.data_as(C.c_void_p),
                              None if gr is None else gr.ctypes.data_as(C.c_void_p), modes[mode], delta, c0, rho0,
-                             gravity, int(L is not None), out)
+                             gravity, int(L is not None), int(deltas is not None),
+                             None if deltas is None else _f64(deltas).ctypes.data_as(C.c_void_p), out)
         return out
 
     def xsphVelocity(self, velocities, densities, epsilon):
@@ -241,7 +261,7 @@ class Stepper:
     def __init__(self, dim, kernelType, hMax, rho0, c0, alpha, gravity, boundaryFactor=0.0, xsphEpsilon=0.0,
                  densityFloor=0.0, diffusion='none', delta=0.1, wallExtrapolated=False, tension=False,
                  corrected=False, limited=False, cfl=0.25, maxTimeStep=1.0, period=0.0, filterInterval=0,
-                 boundary=None):
+                 boundary=None, closure=False, viscosity=1.0034e-6):
         sp = StepParams()
         sp.dim, sp.kind, sp.period, sp.hMax, sp.hMin = dim, 1 if kernelType == 'wendlandC2' else 0, period, hMax, hMax
         sp.rho0, sp.c0, sp.alpha, sp.boundaryFactor = rho0, c0, alpha, boundaryFactor
@@ -252,6 +272,7 @@ class Stepper:
         sp.wallExtrapolated, sp.tension, sp.corrected, sp.limited = (int(wallExtrapolated), int(tension),
                                                                     int(corrected), int(limited))
         sp.cfl, sp.maxTimeStep = cfl, maxTimeStep
+        sp.closure, sp.viscosity = int(closure), float(viscosity)
         self.params, self.filterInterval, self._keep = sp, filterInterval, None
         self.setBoundary(boundary)
         self.time, self.step = 0.0, 0

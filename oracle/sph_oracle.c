@@ -417,7 +417,39 @@ void or_density_gradients(const Sys *s, long n, const double *rho, const double 
 typedef struct {
     double c0, alpha, boundaryFactor, g[3];
     int limited;
+    int closure;                /* the delta-LES-SPH viscous term on fluid pairs */
+    double waterTerm, rho0;     /* 2 (dim + 2) nu / c0, and rho0 */
+    const double *alphas;       /* each particle's alpha_i (or_closure_coefficients) */
 } AccelParams;
+
+static double harmonic_mean(double a, double b)
+{
+    double both = a + b;
+    return both > 0.0 ? 2.0 * a * b / both : 0.0;
+}
+
+/* src/pysurf/sphSolver.py:1232-1274 (closureCoefficients): ||D|| = sqrt(2 D:D), D = (G + G^T) / 2,
+ * alpha_i = 2 (dim + 2) (C_S l)^2 ||D|| / (c0 h), delta_i = (C_delta l)^2 ||D|| / (c0 h), l = 2 h,
+ * C_S 0.12, C_delta 1.5, each at most 0.2; zero on the boundary. */
+void or_closure_coefficients(const Sys *s, long n, const double *G, double c0, double *alphas, double *deltas)
+{
+    int dim = s->dim, dd = dim * dim;
+    for (long i = 0; i < n; ++i) {
+        alphas[i] = deltas[i] = 0.0;
+        if (!s->fluid[i]) continue;
+        double sum = 0.0;
+        for (int a = 0; a < dim; ++a)
+            for (int b = 0; b < dim; ++b) {
+                double e = 0.5 * (G[i * dd + a * dim + b] + G[i * dd + b * dim + a]);
+                sum += e * e;
+            }
+        double norm = sqrt(2.0 * sum), h = s->h[i], width = 2.0 * h;
+        double al = 2.0 * (dim + 2) * (0.12 * width) * (0.12 * width) * norm / (c0 * h);
+        double de = (1.5 * width) * (1.5 * width) * norm / (c0 * h);
+        alphas[i] = al < 0.2 ? al : 0.2;
+        deltas[i] = de < 0.2 ? de : 0.2;
+    }
+}
 
 /* src/pysurf/sphSolver.py:1122-1149 (artificialViscosity), 1192-1230 (limitedVelocityDifference),
  * 1328-1356 (pairAccelerations), 1610-1643 (_computeRates); src/pysurf/sphGpu.py:303-414.
@@ -466,6 +498,13 @@ void or_accelerations(const Sys *s, long n, const double *v, const double *rho, 
                 visc = -ap->alpha * ap->c0 * mu / (0.5 * (rho[i] + rho[j]));
                 if (!s->fluid[j]) visc *= ap->boundaryFactor;
             }
+            if (ap->closure && s->fluid[j]) {
+                /* src/pysurf/sphSolver.py:1283-1326 (closureViscosity): every fluid pair, the plain v_ij . r_ij */
+                double plain = 0.0;
+                for (int c = 0; c < dim; ++c) plain += rel[c] * d[c];
+                double pairAlpha = ap->waterTerm / h + harmonic_mean(ap->alphas[i], ap->alphas[j]);
+                visc += -pairAlpha * ap->c0 * h * ap->rho0 * plain / (r * r * rho[i] * rho[j]);
+            }
             double coef = -(own + p[j] / (rho[j] * rho[j]) + visc) * s->m[j];
             double f = coef * kernel_slope(s->kind, dim, r, h) / r;
             for (int c = 0; c < dim; ++c) tot[c] += f * d[c];
@@ -478,6 +517,8 @@ typedef struct {
     int mode;              /* 0 none, 1 molteni, 2 hydrostatic, 3 antuono */
     double delta, c0, rho0, gravity;
     int corrected;
+    int closure;           /* the pair's delta is the harmonic mean of the two particles' (closure) */
+    const double *deltas;
 } ContinuityParams;
 
 /* src/pysurf/sphSolver.py:623-654 (continuityRate), 718-822 (hydrostaticDensityDifference,
@@ -520,7 +561,8 @@ void or_continuity(const Sys *s, long n, const double *v, const double *rho, con
                     diff += 0.5 * t;
                 }
                 double outward = -slope * r;
-                total += 2.0 * cp->delta * h * cp->c0 * diff * outward / (r * r + 0.01 * h * h) * s->m[j] / rho[j];
+                double delta = cp->closure ? harmonic_mean(cp->deltas[i], cp->deltas[j]) : cp->delta;
+                total += 2.0 * delta * h * cp->c0 * diff * outward / (r * r + 0.01 * h * h) * s->m[j] / rho[j];
             }
         }
         out[i] = total;
@@ -718,6 +760,8 @@ typedef struct {
     double lower[3], upper[3]; int openTop;     /* container */
     BedParams bed;
     FieldParams field;
+    int closure;                                 /* delta-LES-SPH closure, with the water's viscosity */
+    double viscosity;
 } StepParams;
 
 static double cfl_time_step(double h, double c0, double vmax, double amax, double cfl, double maxdt)
@@ -753,11 +797,19 @@ double or_step(const StepParams *sp, long n, double *x, double *v, double *rho, 
         memcpy(rho, rw, sizeof(double) * (size_t)n);
         free(pw); free(rw);
     }
-    if (sp->limited) {
+    double *alphas = NULL, *deltas = NULL;
+    if (sp->limited || sp->closure) {
         G = (double *)malloc(sizeof(double) * (size_t)n * dim * dim);
         or_velocity_gradients(&s, n, v, rho, G);
     }
-    AccelParams ap = {sp->c0, sp->alpha, sp->boundaryFactor, {sp->g[0], sp->g[1], sp->g[2]}, sp->limited};
+    if (sp->closure) {
+        /* the coefficients come from the step's starting velocities; the diffusion reuses them */
+        alphas = (double *)malloc(sizeof(double) * (size_t)n);
+        deltas = (double *)malloc(sizeof(double) * (size_t)n);
+        or_closure_coefficients(&s, n, G, sp->c0, alphas, deltas);
+    }
+    AccelParams ap = {sp->c0, sp->alpha, sp->boundaryFactor, {sp->g[0], sp->g[1], sp->g[2]}, sp->limited,
+                      sp->closure, 2.0 * (dim + 2) * sp->viscosity / sp->c0, sp->rho0, alphas};
     or_accelerations(&s, n, v, rho, p, G, &ap, a);
     double vmax = 0.0, amax = 0.0;
     for (long i = 0; i < n; ++i) {
@@ -779,7 +831,8 @@ double or_step(const StepParams *sp, long n, double *x, double *v, double *rho, 
         gr = (double *)malloc(sizeof(double) * (size_t)n * dim);
         or_density_gradients(&s, n, rho, L, gr);
     }
-    ContinuityParams cp = {sp->diffusion, sp->delta, sp->c0, sp->rho0, fabs(sp->g[dim - 1]), sp->corrected};
+    ContinuityParams cp = {sp->diffusion, sp->delta, sp->c0, sp->rho0, fabs(sp->g[dim - 1]), sp->corrected,
+                           sp->closure, deltas};
     or_continuity(&s, n, v, rho, L, gr, &cp, tmp);
     for (long i = 0; i < n; ++i) {
         rho[i] += tmp[i] * dt;
@@ -800,7 +853,7 @@ double or_step(const StepParams *sp, long n, double *x, double *v, double *rho, 
     if (sp->boundaryKind == 1) or_enforce_container(n, dim, x, v, fluid, sp->lower, sp->upper, sp->openTop);
     else if (sp->boundaryKind == 2) or_enforce_bed(n, dim, x, v, fluid, &sp->bed);
     else if (sp->boundaryKind == 3) or_enforce_heightfield(n, x, v, fluid, &sp->field);
-    free(off); free(nbr); free(tmp); free(G); free(L); free(gr); free(xs);
+    free(off); free(nbr); free(tmp); free(G); free(L); free(gr); free(xs); free(alphas); free(deltas);
     return dt;
 }
 
@@ -823,20 +876,26 @@ void orx_density_gradients(SYS_ARGS, long n, const double *rho, const double *L,
 { SYS_MAKE; or_density_gradients(&s, n, rho, L, out); }
 
 void orx_accelerations(SYS_ARGS, long n, const double *v, const double *rho, const double *p, const double *G,
-                       double c0, double alpha, double boundaryFactor, const double *g, int limited, double *a)
+                       double c0, double alpha, double boundaryFactor, const double *g, int limited, int closure,
+                       double waterTerm, double rho0, const double *alphas, double *a)
 {
     SYS_MAKE;
-    AccelParams ap = {c0, alpha, boundaryFactor, {g[0], g[1], dim == 3 ? g[2] : 0.0}, limited};
+    AccelParams ap = {c0, alpha, boundaryFactor, {g[0], g[1], dim == 3 ? g[2] : 0.0}, limited, closure, waterTerm,
+                      rho0, alphas};
     or_accelerations(&s, n, v, rho, p, G, &ap, a);
 }
 
 void orx_continuity(SYS_ARGS, long n, const double *v, const double *rho, const double *L, const double *gradRho,
-                    int mode, double delta, double c0, double rho0, double gravity, int corrected, double *out)
+                    int mode, double delta, double c0, double rho0, double gravity, int corrected, int closure,
+                    const double *deltas, double *out)
 {
     SYS_MAKE;
-    ContinuityParams cp = {mode, delta, c0, rho0, gravity, corrected};
+    ContinuityParams cp = {mode, delta, c0, rho0, gravity, corrected, closure, deltas};
     or_continuity(&s, n, v, rho, L, gradRho, &cp, out);
 }
+
+void orx_closure_coefficients(SYS_ARGS, long n, const double *G, double c0, double *alphas, double *deltas)
+{ SYS_MAKE; or_closure_coefficients(&s, n, G, c0, alphas, deltas); }
 
 void orx_xsph(SYS_ARGS, long n, const double *v, const double *rho, double eps, double *out)
 { SYS_MAKE; or_xsph(&s, n, v, rho, eps, out); }

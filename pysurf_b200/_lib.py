@@ -71,6 +71,8 @@ SIGNATURES = {
     'sph_cell_order_key': [_pd, _i64, _i, _d, _pi64, _pi64, _i],
     'sph_neighbor_list': [_h, _d, _pi64, _pi32, _i64, _pi64],
     'sph_split': [_h, _pu8, _d, _d, _pi64],
+    'sph_set_closure': [_h, _i, _d, _d, _d],
+    'sph_closure_coefficients': [_h, _pd, _pd, _pd, _pd],
     'sph_surface_tops': [_h, _d, _d, _i64, _pd],
     'sph_split_crest_zone': [_h, _d, _d, _d, _i64, _i64, _d, _d, _d, _d, _pi64],
     'sph_face_cells': [_h, _d, _d, _d, _d, _d, _d, _d, _i64, _i64, _pu8],

@@ -55,6 +55,8 @@ class Case:
     maxTimeStep: float = 1.0
     densityFilterInterval: int = 0
     period: float = 0.0
+    turbulenceClosure: str = 'none'   # 'deltaLes': the delta-LES-SPH closure
+    kinematicViscosity: float = 1.0034e-6     # src/pysurf/constants.py:35, the closure's water term
     info: dict = field(default_factory=dict)
 
     @property
@@ -406,6 +408,8 @@ def pairSumsFor(case: Case, cellsPerSupport: int | None = None, device: int = 0)
     sums.setNegativePressure(case.negativePressure)
     sums.setContinuityCorrection(case.continuityCorrection)
     sums.setViscosityLimiter(case.viscosityLimiter)
+    sums.setClosure(case.turbulenceClosure == 'deltaLes', case.soundSpeed, case.referenceDensity,
+                    case.kinematicViscosity)
     sums.setPhysics(case.referenceDensity, case.soundSpeed, case.alpha, case.boundaryViscosityFactor, case.gravity,
                     case.xsphEpsilon, case.densityFloor)
     return sums

@@ -79,6 +79,12 @@ struct Params {
     int wallExtrapolated;
     float xsphEpsilon;
     double gravity64[3];
+    // delta-LES-SPH closure (src/pysurf/sphSolver.py:1232-1326): the eddy coefficients from the
+    // velocity gradients, a viscous term on every fluid pair, the pair's diffusion coefficient
+    int closure;
+    float waterTerm;        // 2 (dim + 2) nu / c0: the water's own viscosity as an alpha times h
+    float closureRho0;
+    float closureC0;        // the closure's sound speed: its coefficients and its diffusion's 2 c0
     // neighbour table: up to listCap entries a particle (a multiple of 4), entry k of slot i at
     // 4 ((k / 4) listStride + i) + k % 4; listCap 0: no table, the sweeps walk the cells
     int listCap;
@@ -98,6 +104,7 @@ struct Frame {
     float *rate;            // d rho / dt
     float *scalar;          // scratch per particle (Shepard, wall pressure outputs)
     float4 *vec;            // scratch per particle (XSPH transport velocity)
+    float2 *eddy;           // closure: each particle's (alpha_i, delta_i)
     int *nbr;               // neighbour table (chunks of four), top bit: a pair across the periodic seam
     int *ncount;            // each slot's neighbour count (may exceed the table's capacity)
     // master (current buffers)

@@ -369,6 +369,7 @@ struct MomentumVisit {
     const Params &P; const Frame &F;
     Smoothing<K, D> S;
     float vi[3], rhoI, own, viscosityScale;   // viscosityScale: -alpha c0
+    float alphaI;                               // closure: this particle's eddy alpha
     float Gi[3][3];
     float total[3];
     __device__ bool accept(bool) const { return true; }
@@ -381,6 +382,7 @@ struct MomentumVisit {
         velocityIn<D>(Kj, vj);
         float rel[3] = {vi[0] - vj[0], vi[1] - vj[1], vi[2] - vj[2]};
         float approach = rel[0] * d[0] + rel[1] * d[1] + (D == 3 ? rel[2] * d[2] : 0.0f);
+        const float plain = approach;           // before the limiter reconstructs it
         float viscosity = 0.0f;
         if (approach < 0.0f && P.limited && fluidJ) {
             float Gj[3][3];
@@ -411,6 +413,14 @@ struct MomentumVisit {
             viscosity = __fdividef(viscosityScale * h * approach,
                                    (r * r + k.soft) * (0.5f * (rhoI + densityIn<D>(Kj))));
             if (!fluidJ) viscosity *= P.boundaryFactor;
+        }
+        if (P.closure && fluidJ) {
+            // delta-LES-SPH: -(K nu / (c0 h) + harmonic mean of the alphas) c0 h rho0 (v_ij . r_ij) /
+            // (r^2 rho_i rho_j) on every fluid pair, approaching or not (src/pysurf/sphGpu.py:388-396)
+            const float alphaJ = __ldg(&F.eddy[j].x), both = alphaI + alphaJ;
+            const float mean = both > 0.0f ? 2.0f * alphaI * alphaJ / both : 0.0f;
+            viscosity += -(P.waterTerm / h + mean) * P.c0 * h * P.closureRho0 * plain
+                       / (r * r * rhoI * densityIn<D>(Kj));
         }
         const float ratioJ = D == 2 ? Kj.w : __ldg(&F.aux[j].x);
         float coefficient = -(own + ratioJ + viscosity) * massIn<D>(B);
@@ -480,6 +490,7 @@ momentumKernel(Params P, Frame F, Control *ctl, int maxima)
             visit.rhoI = densityOf<D>(F, i);
             visit.own = pressureRatioOf<D>(F, i);
             visit.viscosityScale = -P.alpha * P.c0;
+            visit.alphaI = P.closure ? F.eddy[i].x : 0.0f;
             if (P.limited) loadMatrix<D>(F.G0, F.G1, F.G2, i, visit.Gi);
             visit.total[0] = visit.total[1] = visit.total[2] = 0.0f;
             forEachNeighbour<D, T>(P, F, i, G.t, hs, visit);
@@ -496,6 +507,34 @@ momentumKernel(Params P, Frame F, Control *ctl, int maxima)
         }
     }
     if (maxima) foldMaxima(ctl, speed, accel, (int)(gridDim.x * (blockDim.x >> 5)));
+}
+
+// The delta-LES-SPH closure's coefficients (src/pysurf/sphGpu.py:699-723): ||D|| = sqrt(2 D:D) of the
+// strain D = (G + G^T) / 2, alpha_i = 2 (dim + 2) (C_S l / h)^2 h ||D|| / c0 and
+// delta_i = (C_delta l / h)^2 h ||D|| / c0, l = 2 h, C_S 0.12, C_delta 1.5, each at most 0.2;
+// zero on the boundary.  G is the gradients sweep's, from this step's starting velocities.
+template <int D>
+__global__ void closureKernel(Params P, Frame F, const Control *ctl)
+{
+    if (ctl && !ctl->active) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    const float hs = signedLength<D>(F, i);
+    if (hs <= 0.0f) {
+        F.eddy[i] = make_float2(0.0f, 0.0f);
+        return;
+    }
+    float G[3][3];
+    loadMatrix<D>(F.G0, F.G1, F.G2, i, G);
+    float sum = 0.0f;
+    for (int a = 0; a < D; ++a)
+        for (int b = 0; b < D; ++b) {
+            const float e = 0.5f * (G[a][b] + G[b][a]);
+            sum += e * e;
+        }
+    const float scale = hs * sqrtf(2.0f * sum) / P.closureC0;
+    constexpr float smagorinsky = (0.12f * 2.0f) * (0.12f * 2.0f), diffusion = (1.5f * 2.0f) * (1.5f * 2.0f);
+    F.eddy[i] = make_float2(fminf(2.0f * (D + 2) * smagorinsky * scale, 0.2f), fminf(diffusion * scale, 0.2f));
 }
 
 // v += a dt on the fluid (src/pysurf/sphGpu.py:1084-1109); the frame takes the kicked velocity.
@@ -552,6 +591,7 @@ struct ContinuityVisit {
     Smoothing<K, D> S;
     bool boundaryI, diffuses, corrected;
     float vi[3], devI, Li[3][3], gi[3];
+    float deltaI;           // closure: this particle's eddy delta
     float total;
     __device__ bool accept(bool fluidJ) const { return !(boundaryI && !fluidJ); }
     __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int, const float4 &B,
@@ -587,10 +627,15 @@ struct ContinuityVisit {
                 for (int a = 0; a < D; ++a) t += (gi[a] + gjv[a]) * d[a];
                 difference += 0.5f * t;
             }
-            // 2 delta c0 h V_j (difference) (-(dW/dr) r) / (r^2 + 0.01 h^2), with (dW/dr) r = grad r^2
+            // 2 delta c0 h V_j (difference) (-(dW/dr) r) / (r^2 + 0.01 h^2), with (dW/dr) r = grad r^2;
+            // with the closure, 2 delta c0 is 2 c0 times the harmonic mean of the two deltas
+            float factor = P.diffusionFactor;
+            if (P.closure) {
+                const float deltaJ = __ldg(&F.eddy[j].y), both = deltaI + deltaJ;
+                factor = both > 0.0f ? 2.0f * P.closureC0 * (2.0f * deltaI * deltaJ / both) : 0.0f;
+            }
             const float r2 = r * r;
-            total += P.diffusionFactor * h * volumeIn<D>(B, X) * difference * (-grad)
-                   * __fdividef(r2, r2 + k.soft);
+            total += factor * h * volumeIn<D>(B, X) * difference * (-grad) * __fdividef(r2, r2 + k.soft);
         }
     }
 };
@@ -611,6 +656,7 @@ continuityKernel(Params P, Frame F, Control *ctl, Enforcement E, int mode)
     visit.corrected = P.corrected && !visit.boundaryI;
     velocityOf<D>(F, i, visit.vi);
     visit.devI = deviationOf<D>(F, i);
+    visit.deltaI = P.closure && visit.diffuses ? F.eddy[i].y : 0.0f;
     if (visit.corrected) loadMatrix<D>(F.L0, F.L1, F.L2, i, visit.Li);
     visit.gi[0] = visit.gi[1] = visit.gi[2] = 0.0f;
     if (visit.diffuses && P.diffusion == 3) {
@@ -734,6 +780,7 @@ static void launchT(const LaunchArgs &A, Stage stage)
     case Stage::Continuity: continuityKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.flag); break;
     case Stage::Xsph: xsphKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.densities, A.flag); break;
     case Stage::List: launchList<D>(A); break;
+    case Stage::Closure: closureKernel<D><<<pointwise, kBlock, 0, st>>>(P, F, A.ctl); break;
     }
 }
 

@@ -90,6 +90,9 @@ struct SphSystem {
     int diffusionMode = 0;
     double diffusionDelta = 0.1, diffusionC0 = 1.0, diffusionRho0 = 1000.0, diffusionG = 0.0;
     int wallExtrapolated = 0, tension = 0, corrected = 0, limited = 0;
+    int closure = 0;            // delta-LES-SPH closure, with its sound speed, rho0 and the water's viscosity
+    double closureC0 = 1.0, closureRho0 = 1000.0, closureNu = 0.0;
+    float2 *eddy = nullptr;
     bool physicsSet = false;
     Enforcement enforcement{};
     double *bedX = nullptr, *bedZ = nullptr, *table = nullptr;
@@ -161,8 +164,9 @@ struct SphSystem {
         }
         void *ptrs[] = {pa, pb, kin, G[0], G[1], G[2], L[0], L[1], L[2], gradRho, acc, vec, aux, pres, rate,
                         scalar, cell, sortBuffers.slotCell, sortBuffers.slotWithin, sortBuffers.perm,
-                        sortBuffers.bucket, dStage, dStageU8, dRank, nbr, ncount};
+                        sortBuffers.bucket, dStage, dStageU8, dRank, nbr, ncount, eddy};
         for (void *p : ptrs) cudaFree(p);
+        eddy = nullptr;
         nbr = ncount = nullptr;
         nbrEntries = 0;
         listCap = 0;
@@ -234,6 +238,7 @@ struct SphSystem {
         TRY(deviceAlloc(&gradRho, cap));
         TRY(deviceAlloc(&acc, cap));
         TRY(deviceAlloc(&vec, cap));
+        TRY(deviceAlloc(&eddy, cap));
         TRY(deviceAlloc(&rate, cap));
         TRY(deviceAlloc(&scalar, cap));
         TRY(deviceAlloc(&cell, cap));
@@ -249,6 +254,7 @@ struct SphSystem {
         CUDA_TRY(cudaMemsetAsync(kin, 0, sizeof(float4) * cap, stream));
         CUDA_TRY(cudaMemsetAsync(aux, 0, sizeof(float4) * cap, stream));
         CUDA_TRY(cudaMemsetAsync(pres, 0, sizeof(float) * cap, stream));
+        CUDA_TRY(cudaMemsetAsync(eddy, 0, sizeof(float2) * cap, stream));
         graphDirty = true;
         framed = false;
         return SPH_OK;
@@ -343,6 +349,10 @@ struct SphSystem {
         P.gravityOverSound = (float)(diffusionG / (diffusionC0 * diffusionC0));
         P.corrected = corrected;
         P.limited = limited;
+        P.closure = closure;
+        P.waterTerm = (float)(2.0 * (dim + 2) * closureNu / closureC0);
+        P.closureRho0 = (float)closureRho0;
+        P.closureC0 = (float)closureC0;
         P.wallExtrapolated = wallExtrapolated;
         P.xsphEpsilon = (float)xsphEpsilon;
         P.listCap = listCap;
@@ -357,7 +367,7 @@ struct SphSystem {
         F.cell = cell; F.cellStart = cellStart;
         F.G0 = G[0]; F.G1 = G[1]; F.G2 = G[2];
         F.L0 = L[0]; F.L1 = L[1]; F.L2 = L[2];
-        F.gradRho = gradRho; F.acc = acc; F.rate = rate; F.scalar = scalar; F.vec = vec;
+        F.gradRho = gradRho; F.acc = acc; F.rate = rate; F.scalar = scalar; F.vec = vec; F.eddy = eddy;
         F.nbr = nbr; F.ncount = ncount;
         const MasterView &M = master[cur];
         for (int a = 0; a < 3; ++a) { F.x[a] = M.x[a]; F.v[a] = M.v[a]; }
@@ -675,6 +685,22 @@ int sph_set_continuity_correction(SphSystem *sys, int enabled)
     return SPH_OK;
 }
 
+int sph_set_closure(SphSystem *sys, int enabled, double sound_speed, double reference_density,
+                    double kinematic_viscosity)
+{
+    CHECK_SYS(sys);
+    if (enabled && (!(sound_speed > 0.0) || !(reference_density > 0.0) || !(kinematic_viscosity >= 0.0)))
+        return fail(SPH_ERR_INVALID, "the closure needs a positive sound speed and density, a viscosity >= 0");
+    sys->closure = enabled ? 1 : 0;
+    if (enabled) {
+        sys->closureC0 = sound_speed;
+        sys->closureRho0 = reference_density;
+        sys->closureNu = kinematic_viscosity;
+    }
+    sys->graphDirty = true;
+    return SPH_OK;
+}
+
 int sph_set_viscosity_limiter(SphSystem *sys, int enabled)
 {
     CHECK_SYS(sys);
@@ -808,10 +834,11 @@ int sph_pair_accelerations(SphSystem *sys, const double *velocities, const doubl
     A.P.alpha = (float)alpha;
     A.P.boundaryFactor = (float)boundary_factor;
     for (int a = 0; a < 3; ++a) A.P.g[a] = a < sys->dim ? (float)gravity[a] : 0.0f;
-    if (sys->limited) {
+    if (sys->limited || sys->closure) {
         A.wantG = 1;
         launchStage(A, Stage::Gradients);
     }
+    if (sys->closure) launchStage(A, Stage::Closure);     // kept for the next continuityRate, as the reference does
     launchStage(A, Stage::Momentum);
     launchScatterFloat4(sys->n, sys->dim, A.F.orig, sys->acc, sys->stage(SphSystem::kOutSlot), sys->stream);
     return finish(sys, out, (size_t)sys->n * sys->dim);
@@ -899,6 +926,32 @@ int sph_velocity_gradients(SphSystem *sys, const double *velocities, const doubl
     launchStage(A, Stage::Gradients);
     launchScatterMatrix(sys->n, sys->dim, A.F.orig, A.F, 0, sys->stage(SphSystem::kOutSlot), sys->stream);
     return finish(sys, out, (size_t)sys->n * sys->dim * sys->dim);
+}
+
+int sph_closure_coefficients(SphSystem *sys, const double *velocities, const double *densities, double *alphas,
+                             double *deltas)
+{
+    CHECK_SYS(sys);
+    TRY(needFrame(sys));
+    if (!sys->closure) return fail(SPH_ERR_STATE, "the closure is off: call sph_set_closure first");
+    if (sys->n == 0) return SPH_OK;
+    if (!velocities || !densities || !alphas || !deltas) return fail(SPH_ERR_INVALID, "null argument");
+    TRY(loadFields(sys, velocities, densities, nullptr));
+    LaunchArgs A = sys->args(nullptr);
+    A.wantG = 1;
+    launchStage(A, Stage::Gradients);
+    launchStage(A, Stage::Closure);
+    // the two halves of (alpha, delta), scattered to the caller's order
+    std::vector<float2> packed(sys->n);
+    std::vector<int> orig(sys->n);
+    CUDA_TRY(cudaMemcpyAsync(packed.data(), sys->eddy, sizeof(float2) * sys->n, cudaMemcpyDeviceToHost, sys->stream));
+    CUDA_TRY(cudaMemcpyAsync(orig.data(), A.F.orig, sizeof(int) * sys->n, cudaMemcpyDeviceToHost, sys->stream));
+    CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    for (int s = 0; s < sys->n; ++s) {
+        alphas[orig[s]] = packed[s].x;
+        deltas[orig[s]] = packed[s].y;
+    }
+    return SPH_OK;
 }
 
 int sph_correction_matrices(SphSystem *sys, const double *densities, double *out)
@@ -1129,13 +1182,15 @@ static void enqueueRates(SphSystem *sys, bool filter, cudaEvent_t *events = null
     }
     mark(sys, events, 3);
     bool wantL = sys->corrected || sys->diffusionMode == 3;
-    if (sys->limited || wantL) {
-        A.wantG = sys->limited;
+    if (sys->limited || sys->closure || wantL) {
+        A.wantG = sys->limited || sys->closure;
         A.wantL = wantL;
         A.wantRho = sys->diffusionMode == 3;
         launchStage(A, Stage::Gradients);
         A.wantG = A.wantL = A.wantRho = 0;
     }
+    // the closure's coefficients, from this step's starting velocities (the diffusion reuses them)
+    if (sys->closure) launchStage(A, Stage::Closure);
     mark(sys, events, 4);
     launchStage(A, Stage::Momentum);
     mark(sys, events, 5);

@@ -11,8 +11,8 @@ What it carries: the cubic spline and the Wendland C2 kernels; the plain and the
 artificial viscosity; the continuity sum plain and corrected; the delta-SPH diffusive term in its
 'molteni', 'hydrostatic' and 'antuono' forms; the extrapolated wall pressure; negative pressure;
 the Shepard filter; XSPH; a periodic y axis; mixed smoothing lengths; container, bed and height
-field enforcement.  Particle shifting, the delta-LES-SPH closure and the energy budget are not
-carried yet: enabling one raises NotImplementedError, and every setter accepts them off.
+field enforcement; the delta-LES-SPH closure.  Particle shifting and the energy budget are not
+carried yet: enabling one raises NotImplementedError, and their setters accept them off.
 
 Beyond the reference's surface, ``advance`` runs a whole span of steps on the device with the
 time step taken there (no host round trip per step), ``split`` refines on the device, and
@@ -187,9 +187,11 @@ class PairSums:
 
     def setClosure(self, enabled: bool, soundSpeed: float = 1.0, referenceDensity: float = 1000.0,
                    kinematicViscosity: float = 0.0) -> None:
-        if enabled:
-            raise NotImplementedError('The delta-LES-SPH closure is not carried by the B200 backend yet.')
-        self.closureEnabled = False
+        """Whether the accelerations and the diffusive term carry the delta-LES-SPH closure
+        (src/pysurf/sphGpu.py:1752-1779; sphSolver.closureCoefficients, closureViscosity)."""
+        check(self._lib.sph_set_closure(self._handle, int(bool(enabled)), float(soundSpeed), float(referenceDensity),
+                                        float(kinematicViscosity)), 'setClosure')
+        self.closureEnabled = bool(enabled)
 
     def setEnergyBudget(self, enabled: bool) -> None:
         if enabled:
@@ -325,7 +327,13 @@ class PairSums:
         return out
 
     def closureCoefficients(self, velocities, densities):
-        raise ValueError('The closure is off; see setClosure.')
+        """Each particle's alpha_i and delta_i at the current positions (sphSolver.closureCoefficients)."""
+        if not self.closureEnabled:
+            raise ValueError('The closure is off; see setClosure.')
+        alphas, deltas = np.empty(self.count), np.empty(self.count)
+        check(self._lib.sph_closure_coefficients(self._handle, dptr(f64(velocities)), dptr(f64(densities)),
+                                                 dptr(alphas), dptr(deltas)), 'closureCoefficients')
+        return alphas, deltas
 
     def correctionMatrices(self, densities) -> np.ndarray:
         """L for every particle at the current positions, shape (N, dim, dim)."""

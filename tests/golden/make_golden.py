@@ -470,13 +470,64 @@ def makeBreaking():
     np.savez_compressed(os.path.join(HERE, 'breaking.npz'), **out)
 
 
+def makeClosure():
+    """The delta-LES-SPH closure (src/pysurf/sphSolver.py:1232-1326 and its use in _computeRates, 1615-1745):
+    coefficients, accelerations and continuity on the six clouds under a strained flow, and a
+    sloshing run with turbulenceClosure 'deltaLes'."""
+    from pysurf import constants
+    from pysurf.sphSolver import (artificialViscosity, closureCoefficients, closureViscosity, continuityRate,
+                                  densityDiffusionRate, harmonicMean, pairAccelerations, velocityGradients)
+    out = {}
+    nu = constants.freshwaterKinematicViscosity
+    for dimensions, periodic in [(2, False), (3, False), (3, True)]:
+        for kernelType in ('cubicSpline', 'wendlandC2'):
+            tag = f'{dimensions}d_{"p" if periodic else "o"}_{kernelType}'
+            case = cloud(dimensions, periodic, kernelType=kernelType)
+            i, j, fluid = case['i'], case['j'], case['isFluid']
+            n = len(fluid)
+            gravity = np.zeros(dimensions)
+            gravity[-1] = -9.81
+            factor = 0.3
+            strained = strainedFlow(case)
+            G = velocityGradients(case['masses'], case['densities'], strained, i, j, case['separation'],
+                                  case['gradients'], fluid)
+            alphas, deltas = closureCoefficients(G, fluid, case['h'], c0)
+            relative = strained[i] - strained[j]
+            viscosity = artificialViscosity(relative, case['separation'], case['distance'],
+                                            0.5 * (case['densities'][i] + case['densities'][j]), case['h'], c0, alpha)
+            boundaryPairs = ~(fluid[i] & fluid[j])
+            viscosity[boundaryPairs] *= factor
+            fp = ~boundaryPairs
+            fi, fj = i[fp], j[fp]
+            viscosity[fp] += closureViscosity(relative[fp], case['separation'][fp], case['distance'][fp],
+                                              case['densities'][fi], case['densities'][fj], case['h'], c0, rho0,
+                                              alphas[fi], alphas[fj], nu)
+            acc = pairAccelerations(case['masses'], case['densities'], case['pressures'], i, j, case['gradients'],
+                                    viscosity, n)
+            acc[fluid] += gravity
+            acc[~fluid] = 0.0
+            rate = continuityRate(case['masses'], strained, i, j, case['gradients'], n, fluid[i] | fluid[j])
+            rate = rate + densityDiffusionRate(case['masses'], case['densities'], i, j, case['separation'],
+                                               case['distance'], case['gradients'], n, case['h'], c0,
+                                               harmonicMean(deltas[i], deltas[j]), rho0, 9.81, fluid[i] & fluid[j])
+            for key, value in dict(alphas=alphas, deltas=deltas, accelerations=acc, continuity=rate).items():
+                out[f'{tag}/{key}'] = np.asarray(value)
+    out['viscosity'] = np.array(nu)
+    runs = {}
+    solver, particles, boundary = sloshing(turbulenceClosure='deltaLes', densityDiffusion='hydrostatic',
+                                           **deltaContinuity)
+    recordRun(runs, 'closure', solver, particles, 30, containerRecord(boundary))
+    out.update(runs)
+    np.savez_compressed(os.path.join(HERE, 'closure.npz'), **out)
+
+
 def main():
     root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('PYSURF_REFERENCE', '')
     if not root or not os.path.isdir(root):
         raise SystemExit('Give the reference checkout: make_golden.py /path/to/reference [fixture ...]')
     loadReference(root)
     makers = {'cellkeys': makeCellKeys, 'clouds': makeClouds, 'enforce': makeEnforcement, 'split': makeSplit,
-              'beach': makeBeach, 'runs': makeRuns, 'breaking': makeBreaking}
+              'beach': makeBeach, 'runs': makeRuns, 'breaking': makeBreaking, 'closure': makeClosure}
     for name in (sys.argv[2:] or list(makers)):
         makers[name]()
     for name in sorted(os.listdir(HERE)):

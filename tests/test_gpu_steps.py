@@ -6,11 +6,12 @@ Tolerances are those the reference holds its float32 device to against the numpy
 (tests/testSphGpu.py:503-517, 578-590): positions 1e-6 m, velocities and densities 1e-3, time 1e-4.
 """
 import math
+import os
 
 import numpy as np
 import pytest
 
-from conftest import golden, goldenTags
+from conftest import GOLDEN, golden, goldenTags
 from oracle import oracle
 from pysurf_b200 import cases
 from pysurf_b200.state import BedBoundary, ContainerBoundary, ParticleState, Profile
@@ -275,3 +276,18 @@ def test_threads_per_particle_on_the_benchmark_beach():
     assert t8 == pytest.approx(t1, rel=1e-9)
     assert np.abs(a.positions - b.positions).max() < 1e-9
     assert np.abs(a.velocities - b.velocities).max() < 1e-5
+
+
+def test_the_closure_run_follows_the_reference_host_steps():
+    # a sloshing tank under the delta-LES-SPH closure (turbulenceClosure 'deltaLes'), 30 device steps
+    # against the reference's float64 host steps and the oracle's
+    r = golden('closure.npz', 'closure')
+    case = caseFromRun(r)
+    case.turbulenceClosure = 'deltaLes'
+    case.kinematicViscosity = float(np.load(os.path.join(GOLDEN, 'closure.npz'))['viscosity'])
+    steps = int(r['steps'])
+    state, time, _ = deviceRun(case, steps)
+    assert time == pytest.approx(float(np.sum(r['dts'])), rel=1e-4)
+    assert np.abs(state.positions - r['finalPositions']).max() < 1e-6
+    assert np.abs(state.velocities - r['finalVelocities']).max() < 1e-3
+    assert np.abs(state.densities - r['finalDensities']).max() < 1e-3

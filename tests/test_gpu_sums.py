@@ -260,3 +260,23 @@ def test_every_sweep_form_gives_the_reference_sums(tag, threads, table):
     fluid = c['isFluid']
     close(s.xsphVelocity(c['velocities'], c['densities'], epsilon)[fluid], c['xsph'][fluid])
     assert np.allclose(s.shepardDensity(c['densities']), c['shepard'], rtol=2e-6, atol=0.0)
+
+
+@pytest.mark.parametrize('tag', CLOUDS)
+def test_closure_sums(tag):
+    # the delta-LES-SPH closure (src/pysurf/sphSolver.py:1232-1326) under the strained flow: the
+    # coefficients, the accelerations with its viscous term, the continuity with its diffusion
+    c, k = golden('clouds.npz', tag), golden('closure.npz', tag)
+    nu = float(np.load('tests/golden/closure.npz')['viscosity'])
+    dim = c['positions'].shape[1]
+    g = np.zeros(dim)
+    g[-1] = -9.81
+    s = pairSums(c)
+    s.setClosure(True, c0, rho0, nu)
+    s.setDiffusion('hydrostatic', 0.1, c0, rho0, 9.81)
+    alphas, deltas = s.closureCoefficients(c['strained'], c['densities'])
+    close(alphas, k['alphas'], 2e-4)
+    close(deltas, k['deltas'], 2e-4)
+    close(s.pairAccelerations(c['strained'], c['densities'], c['pressures'], c0, alpha, 0.3, g), k['accelerations'])
+    # the continuity takes the deltas of the last accelerations, as the reference's device does
+    close(s.continuityRate(c['strained'], c['densities']), k['continuity'])

@@ -143,3 +143,46 @@ def test_device_step_follows_the_reference_host_steps(tag):
     fluid = r['isFluid']
     assert np.allclose(state['accelerations'][fluid], r['finalAccelerations'][fluid], rtol=0.0,
                        atol=1e-8 * np.abs(r['finalAccelerations']).max())
+
+
+def closureGolden(tag):
+    return golden('closure.npz', tag)
+
+
+@pytest.mark.parametrize('tag', CLOUDS)
+def test_closure_sums_match_the_reference(tag):
+    # src/pysurf/sphSolver.py:1232-1326: coefficients from the strained flow's gradients, the
+    # delta-LES-SPH viscous term on every fluid pair, the diffusion at the pairs' harmonic-mean delta
+    c, k = golden('clouds.npz', tag), closureGolden(tag)
+    nu = float(np.load('tests/golden/closure.npz')['viscosity'])
+    s = system(c)
+    dim = c['positions'].shape[1]
+    g = np.zeros(dim)
+    g[-1] = -9.81
+    rho0, c0, alpha = 1000.0, 20.0, 0.1
+    G = s.velocityGradients(c['strained'], c['densities'])
+    alphas, deltas = s.closureCoefficients(G, c0)
+    assert close(alphas, k['alphas']) and close(deltas, k['deltas'])
+    assert close(s.pairAccelerations(c['strained'], c['densities'], c['pressures'], c0, alpha, 0.3, g, G, limited=False,
+                                     closure=(alphas, nu, rho0)), k['accelerations'])
+    assert close(s.continuityRate(c['strained'], c['densities'], 'hydrostatic', 0.1, c0, rho0, 9.81, deltas=deltas),
+                 k['continuity'])
+
+
+def test_closure_step_follows_the_reference_host_steps():
+    r = closureGolden('closure')
+    base = stepperFor(r)
+    sp = base.params
+    stepper = oracle.Stepper(int(sp.dim), 'wendlandC2' if sp.kind == 1 else 'cubicSpline', sp.hMax, sp.rho0, sp.c0,
+                             sp.alpha, r['gravity'], sp.boundaryFactor, sp.xsphEpsilon, sp.densityFloor,
+                             ['none', 'molteni', 'hydrostatic', 'antuono'][sp.diffusion], sp.delta,
+                             bool(sp.wallExtrapolated), bool(sp.tension), bool(sp.corrected), bool(sp.limited),
+                             sp.cfl, sp.maxTimeStep, sp.period, base.filterInterval,
+                             ('container', r['boundary_lower'], r['boundary_upper'], bool(r['boundary_openTop'])),
+                             closure=True, viscosity=float(np.load('tests/golden/closure.npz')['viscosity']))
+    state = {k: r[k].copy() for k in ('positions', 'velocities', 'densities', 'masses', 'isFluid')}
+    dts = [stepper(state) for _ in range(int(r['steps']))]
+    assert np.allclose(dts, r['dts'], rtol=1e-10, atol=0.0)
+    assert np.allclose(state['positions'], r['finalPositions'], rtol=0.0, atol=1e-11)
+    assert np.allclose(state['velocities'], r['finalVelocities'], rtol=0.0, atol=1e-8)
+    assert np.allclose(state['densities'], r['finalDensities'], rtol=1e-11, atol=0.0)
