@@ -51,7 +51,9 @@ class StepParams(C.Structure):
                 ('limited', C.c_int), ('cfl', C.c_double), ('maxTimeStep', C.c_double),
                 ('filterDensity', C.c_int), ('boundaryKind', C.c_int), ('lower', C.c_double * 3),
                 ('upper', C.c_double * 3), ('openTop', C.c_int), ('bed', BedParams), ('field', FieldParams),
-                ('closure', C.c_int), ('viscosity', C.c_double)]
+                ('closure', C.c_int), ('viscosity', C.c_double), ('shifting', C.c_int), ('shiftLocal', C.c_int),
+                ('shiftMach', C.c_double), ('spacingKernel', C.c_double), ('shiftThreshold', C.c_double),
+                ('lopsidedness', C.c_double)]
 
 
 def lib():
@@ -74,6 +76,11 @@ def lib():
         L.orx_continuity.argtypes = sysargs + [C.c_long, _dp, _dp, _vp, _vp, C.c_int, C.c_double, C.c_double,
                                                C.c_double, C.c_double, C.c_int, C.c_int, _vp, _dp]
         L.orx_closure_coefficients.argtypes = sysargs + [C.c_long, _dp, C.c_double, _dp, _dp]
+        L.orx_kernel_value.argtypes = [C.c_int, C.c_int, C.c_double, C.c_double]
+        L.orx_kernel_value.restype = C.c_double
+        L.orx_shifting_fields.argtypes = sysargs + [C.c_long, _dp, C.c_double, _dp, _dp, _dp, _dp]
+        L.orx_shift.argtypes = sysargs + [C.c_long, _dp, _dp, _dp, _dp, _dp, _dp, _dp, C.c_double, C.c_double, _dp,
+                                          _dp, _dp]
         L.orx_xsph.argtypes = sysargs + [C.c_long, _dp, _dp, C.c_double, _dp]
         L.orx_shepard.argtypes = sysargs + [C.c_long, _dp, _dp]
         L.or_step.argtypes = [C.POINTER(StepParams), C.c_long, _dp, _dp, _dp, _dp, _dp, _u8, _dp, _dp]
@@ -177,6 +184,22 @@ class System:
                                 None if alphas is None else alphas.ctypes.data_as(C.c_void_p), out)
         return out
 
+    def shiftingFields(self, densities, spacingKernel):
+        """src/pysurf/sphSolver.py:824-887: grad C, grad C0, div r and grad rho (fluid rows)."""
+        grad, plain, rg = (np.empty((self.n, self.dim)) for _ in range(3))
+        div = np.empty(self.n)
+        lib().orx_shifting_fields(*self._args(), self.n, _f64(densities), float(spacingKernel), grad, plain, div, rg)
+        return grad, plain, div, rg
+
+    def shift(self, densities, velocities, fields, size, threshold, lopsidedness):
+        """src/pysurf/sphSolver.py:889-1010: the shifts, density and velocity changes."""
+        grad, plain, div, rg = (_f64(f) for f in fields)
+        shift, dv = np.empty((self.n, self.dim)), np.empty((self.n, self.dim))
+        drho = np.empty(self.n)
+        lib().orx_shift(*self._args(), self.n, _f64(densities), self._vec(velocities), grad, plain, div, rg,
+                        _f64(np.broadcast_to(size, (self.n,))), float(threshold), float(lopsidedness), shift, drho, dv)
+        return shift, drho, dv
+
     def closureCoefficients(self, gradients, c0):
         """src/pysurf/sphSolver.py:1232-1274: each particle's alpha_i and delta_i."""
         alphas, deltas = np.empty(self.n), np.empty(self.n)
@@ -261,7 +284,8 @@ class Stepper:
     def __init__(self, dim, kernelType, hMax, rho0, c0, alpha, gravity, boundaryFactor=0.0, xsphEpsilon=0.0,
                  densityFloor=0.0, diffusion='none', delta=0.1, wallExtrapolated=False, tension=False,
                  corrected=False, limited=False, cfl=0.25, maxTimeStep=1.0, period=0.0, filterInterval=0,
-                 boundary=None, closure=False, viscosity=1.0034e-6):
+                 boundary=None, closure=False, viscosity=1.0034e-6, shifting=False, shiftingMach=0.1, spacing=None,
+                 shiftingLocal=False):
         sp = StepParams()
         sp.dim, sp.kind, sp.period, sp.hMax, sp.hMin = dim, 1 if kernelType == 'wendlandC2' else 0, period, hMax, hMax
         sp.rho0, sp.c0, sp.alpha, sp.boundaryFactor = rho0, c0, alpha, boundaryFactor
@@ -273,6 +297,12 @@ class Stepper:
                                                                     int(corrected), int(limited))
         sp.cfl, sp.maxTimeStep = cfl, maxTimeStep
         sp.closure, sp.viscosity = int(closure), float(viscosity)
+        if shifting:
+            # src/pysurf/sphSolver.py:258-274: the free surface's thresholds, W(dx) for the anti-clumping
+            sp.shifting, sp.shiftLocal, sp.shiftMach = 1, int(shiftingLocal), float(shiftingMach)
+            sp.spacingKernel = lib().orx_kernel_value(sp.kind, dim, float(spacing), hMax)
+            sp.shiftThreshold = {2: 1.5, 3: 2.4}[dim]
+            sp.lopsidedness = 0.4 if kernelType == 'wendlandC2' else 0.3
         self.params, self.filterInterval, self._keep = sp, filterInterval, None
         self.setBoundary(boundary)
         self.time, self.step = 0.0, 0

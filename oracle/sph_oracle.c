@@ -569,6 +569,111 @@ void or_continuity(const Sys *s, long n, const double *v, const double *rho, con
     }
 }
 
+/* Particle shifting, src/pysurf/sphSolver.py:824-887 (shiftingFields): over every neighbour of a
+ * fluid particle, grad C = sum V_j [1 + 0.2 (W_ij / W(dx))^4] grad W_ij, grad C0 = sum V_j grad W_ij,
+ * div r = -sum V_j r_ij . grad W_ij, grad rho = sum (rho_j - rho_i) V_j grad W_ij.  Boundary rows
+ * get zeros and a divergence of 1e6 (never a free surface). */
+void or_shifting_fields(const Sys *s, long n, const double *rho, double spacingKernel, double *grad, double *plain,
+                        double *div, double *rhoGrad)
+{
+    int dim = s->dim;
+    #pragma omp parallel for schedule(dynamic, 128)
+    for (long i = 0; i < n; ++i) {
+        double g[MAXD] = {0}, c[MAXD] = {0}, rg[MAXD] = {0}, total = 0.0;
+        if (s->fluid[i]) {
+            for (int64_t k = s->off[i]; k < s->off[i + 1]; ++k) {
+                long j = s->nbr[k];
+                double d[MAXD], r, h;
+                if (!pair_geom(s, i, j, d, &r, &h, 1)) continue;
+                double volume = s->m[j] / rho[j];
+                double slope = kernel_slope(s->kind, dim, r, h);
+                double ratio = kernel_value(s->kind, dim, r, h) / spacingKernel, square = ratio * ratio;
+                for (int a = 0; a < dim; ++a) {
+                    double weighted = volume * slope / r * d[a];
+                    c[a] += weighted;
+                    g[a] += (1.0 + 0.2 * square * square) * weighted;
+                    rg[a] += (rho[j] - rho[i]) * weighted;
+                }
+                total -= volume * slope * r;
+            }
+        } else {
+            total = 1.0e6;
+        }
+        for (int a = 0; a < dim; ++a) { grad[i * dim + a] = g[a]; plain[i * dim + a] = c[a]; rhoGrad[i * dim + a] = rg[a]; }
+        div[i] = total;
+    }
+}
+
+/* src/pysurf/sphSolver.py:889-979 (freeSurface, shiftingDisplacement) and 981-1010
+ * (shiftedVelocityChange).  A fluid particle is on the free surface when div r < threshold or
+ * h |grad C0| > lopsidedness; it and the boundary do not shift.  Next to a surface particle (one
+ * within 2h) the shift -size_i grad C loses its part along n, the kernel-weighted mean of the
+ * surface neighbours' outward normals -grad C0 / |grad C0|, or is zero where h |grad C| > 0.03;
+ * elsewhere it is whole.  The density change is shift . grad rho; the velocity change
+ * sum_j V_j (v_j - v_i) (grad W_ij . shift) over fluid neighbours. */
+void or_shift(const Sys *s, long n, const double *rho, const double *v, const double *grad, const double *plain,
+              const double *div, const double *rhoGrad, const double *size, double threshold, double lopsidedness,
+              double *shift, double *drho, double *dv)
+{
+    int dim = s->dim;
+    uint8_t *surface = (uint8_t *)malloc((size_t)n);
+    for (long i = 0; i < n; ++i) {
+        double length = 0.0;
+        for (int a = 0; a < dim; ++a) length += plain[i * dim + a] * plain[i * dim + a];
+        length = sqrt(length);
+        surface[i] = s->fluid[i] && (div[i] < threshold || s->h[i] * length > lopsidedness);
+    }
+    #pragma omp parallel for schedule(dynamic, 128)
+    for (long i = 0; i < n; ++i) {
+        double sh[MAXD] = {0}, nrm[MAXD] = {0};
+        int vicinity = 0;
+        for (int64_t k = s->off[i]; k < s->off[i + 1]; ++k) {
+            long j = s->nbr[k];
+            if (!surface[j]) continue;
+            double d[MAXD], r, h;
+            if (!pair_geom(s, i, j, d, &r, &h, 0)) continue;
+            vicinity = 1;
+            double length = 0.0;
+            for (int a = 0; a < dim; ++a) length += plain[j * dim + a] * plain[j * dim + a];
+            length = sqrt(length);
+            double w = kernel_value(s->kind, dim, r, h);
+            for (int a = 0; a < dim; ++a) nrm[a] += w * (-plain[j * dim + a] / length);
+        }
+        double gl = 0.0;
+        for (int a = 0; a < dim; ++a) { sh[a] = -size[i] * grad[i * dim + a]; gl += grad[i * dim + a] * grad[i * dim + a]; }
+        gl = sqrt(gl);
+        if (vicinity) {
+            double weight = 0.0;
+            for (int a = 0; a < dim; ++a) weight += nrm[a] * nrm[a];
+            weight = sqrt(weight);
+            if (weight > 0.0) {
+                double dot = 0.0;
+                for (int a = 0; a < dim; ++a) { nrm[a] /= weight; dot += sh[a] * nrm[a]; }
+                for (int a = 0; a < dim; ++a) sh[a] -= dot * nrm[a];
+            }
+        }
+        if (surface[i] || !s->fluid[i] || (vicinity && s->h[i] * gl > 0.03))
+            for (int a = 0; a < dim; ++a) sh[a] = 0.0;
+        double change = 0.0, vc[MAXD] = {0};
+        for (int a = 0; a < dim; ++a) change += sh[a] * rhoGrad[i * dim + a];
+        if (s->fluid[i]) {
+            for (int64_t k = s->off[i]; k < s->off[i + 1]; ++k) {
+                long j = s->nbr[k];
+                if (!s->fluid[j]) continue;
+                double d[MAXD], r, h;
+                if (!pair_geom(s, i, j, d, &r, &h, 1)) continue;
+                double dot = 0.0;
+                for (int a = 0; a < dim; ++a) dot += d[a] * sh[a];
+                double f = s->m[j] / rho[j] * kernel_slope(s->kind, dim, r, h) / r * dot;
+                for (int a = 0; a < dim; ++a) vc[a] += f * (v[j * dim + a] - v[i * dim + a]);
+            }
+        }
+        for (int a = 0; a < dim; ++a) { shift[i * dim + a] = sh[a]; dv[i * dim + a] = vc[a]; }
+        drho[i] = change;
+    }
+    free(surface);
+}
+
 /* src/pysurf/sphSolver.py:1358-1377 (xsphVelocity over fluid pairs); src/pysurf/sphGpu.py:725-766. */
 void or_xsph(const Sys *s, long n, const double *v, const double *rho, double eps, double *out)
 {
@@ -762,6 +867,8 @@ typedef struct {
     FieldParams field;
     int closure;                                 /* delta-LES-SPH closure, with the water's viscosity */
     double viscosity;
+    int shifting, shiftLocal;                    /* particle shifting: size c0 dt / h Ma (2h)^2, or 2 h |v| dt */
+    double shiftMach, spacingKernel, shiftThreshold, lopsidedness;
 } StepParams;
 
 static double cfl_time_step(double h, double c0, double vmax, double amax, double cfl, double maxdt)
@@ -845,15 +952,50 @@ double or_step(const StepParams *sp, long n, double *x, double *v, double *rho, 
         or_xsph(&s, n, v, rho, sp->xsphEpsilon, xs);
         transport = xs;
     }
+    double *start = NULL, *shift = NULL, *drho = NULL, *dvel = NULL;
+    if (sp->shifting) {
+        /* the shift takes the step's starting geometry (the pairs of its grid), the updated densities
+         * and the kicked velocities (src/pysurf/sphSolver.py:1760-1785) */
+        start = (double *)malloc(sizeof(double) * (size_t)n * dim);
+        memcpy(start, x, sizeof(double) * (size_t)n * dim);
+    }
     for (long i = 0; i < n; ++i) {
         if (!fluid[i]) continue;
         for (int c = 0; c < dim; ++c) x[i * dim + c] += transport[i * dim + c] * dt;
-        if (sp->period > 0.0) x[i * dim + 1] -= sp->period * floor(x[i * dim + 1] / sp->period);
     }
+    if (sp->shifting) {
+        Sys s0 = {dim, sp->kind, sp->period, start, h, fluid, m, off, nbr};
+        double *grad = (double *)malloc(sizeof(double) * (size_t)n * dim * 3), *plain = grad + (size_t)n * dim;
+        double *rg = plain + (size_t)n * dim, *div = (double *)malloc(sizeof(double) * (size_t)n * 2);
+        double *size = div + n;
+        shift = (double *)malloc(sizeof(double) * (size_t)n * dim * 2);
+        dvel = shift + (size_t)n * dim;
+        drho = (double *)malloc(sizeof(double) * (size_t)n);
+        or_shifting_fields(&s0, n, rho, sp->spacingKernel, grad, plain, div, rg);
+        for (long i = 0; i < n; ++i) {
+            double speed = 0.0;
+            for (int c = 0; c < dim; ++c) speed += v[i * dim + c] * v[i * dim + c];
+            size[i] = sp->shiftLocal ? 2.0 * h[i] * sqrt(speed) * dt
+                                     : (sp->c0 * dt / h[i]) * sp->shiftMach * (2.0 * h[i]) * (2.0 * h[i]);
+        }
+        or_shift(&s0, n, rho, v, grad, plain, div, rg, size, sp->shiftThreshold, sp->lopsidedness, shift, drho, dvel);
+        for (long i = 0; i < n; ++i) {
+            if (!fluid[i]) continue;
+            for (int c = 0; c < dim; ++c) {
+                x[i * dim + c] += shift[i * dim + c];
+                v[i * dim + c] += dvel[i * dim + c];
+            }
+            rho[i] += drho[i];
+        }
+        free(grad); free(div);
+    }
+    for (long i = 0; i < n; ++i)
+        if (fluid[i] && sp->period > 0.0) x[i * dim + 1] -= sp->period * floor(x[i * dim + 1] / sp->period);
     if (sp->boundaryKind == 1) or_enforce_container(n, dim, x, v, fluid, sp->lower, sp->upper, sp->openTop);
     else if (sp->boundaryKind == 2) or_enforce_bed(n, dim, x, v, fluid, &sp->bed);
     else if (sp->boundaryKind == 3) or_enforce_heightfield(n, x, v, fluid, &sp->field);
     free(off); free(nbr); free(tmp); free(G); free(L); free(gr); free(xs); free(alphas); free(deltas);
+    free(start); free(shift); free(drho);
     return dt;
 }
 
@@ -896,6 +1038,17 @@ void orx_continuity(SYS_ARGS, long n, const double *v, const double *rho, const 
 
 void orx_closure_coefficients(SYS_ARGS, long n, const double *G, double c0, double *alphas, double *deltas)
 { SYS_MAKE; or_closure_coefficients(&s, n, G, c0, alphas, deltas); }
+
+double orx_kernel_value(int kind, int dim, double r, double h) { return kernel_value(kind, dim, r, h); }
+
+void orx_shifting_fields(SYS_ARGS, long n, const double *rho, double spacingKernel, double *grad, double *plain,
+                         double *div, double *rhoGrad)
+{ SYS_MAKE; or_shifting_fields(&s, n, rho, spacingKernel, grad, plain, div, rhoGrad); }
+
+void orx_shift(SYS_ARGS, long n, const double *rho, const double *v, const double *grad, const double *plain,
+               const double *div, const double *rhoGrad, const double *size, double threshold, double lopsidedness,
+               double *shift, double *drho, double *dv)
+{ SYS_MAKE; or_shift(&s, n, rho, v, grad, plain, div, rhoGrad, size, threshold, lopsidedness, shift, drho, dv); }
 
 void orx_xsph(SYS_ARGS, long n, const double *v, const double *rho, double eps, double *out)
 { SYS_MAKE; or_xsph(&s, n, v, rho, eps, out); }

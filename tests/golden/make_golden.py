@@ -521,13 +521,84 @@ def makeClosure():
     np.savez_compressed(os.path.join(HERE, 'closure.npz'), **out)
 
 
+def latticeCloud(dimensions, kernelType, seed=11):
+    """Water on a jittered square lattice over three layers of wall particles, its top a free
+    surface: a shift acts inside it and the free-surface rules at its top."""
+    from pysurf.sphKernels import createKernel
+    from pysurf.sphNeighbors import neighborPairs
+    from pysurf.sphSolver import taitEquationOfState
+    rng = np.random.default_rng(seed)
+    spacing = 0.02
+    shape = (24, 18) if dimensions == 2 else (10, 8, 9)
+    axes = [np.arange(k) * spacing for k in shape]
+    grids = np.meshgrid(*axes, indexing='ij')
+    lattice = np.column_stack([g.ravel() for g in grids]) + 5.0
+    positions = lattice + rng.uniform(-0.15 * spacing, 0.15 * spacing, lattice.shape)
+    isFluid = lattice[:, -1] >= 5.0 + 3 * spacing - 1e-9
+    positions[~isFluid] = lattice[~isFluid]
+    count = len(positions)
+    h = (2.0 if kernelType == 'wendlandC2' else 1.3) * spacing
+    velocities = rng.normal(0.0, 0.1, size=(count, dimensions))
+    velocities[~isFluid] = 0.0
+    densities = rho0 * (1.0 + rng.uniform(-0.005, 0.005, size=count))
+    masses = np.full(count, rho0 * spacing ** dimensions)
+    i, j = neighborPairs(positions, 2.0 * h, None)
+    separation = positions[i] - positions[j]
+    distance = np.linalg.norm(separation, axis=1)
+    kernel = createKernel(kernelType, dimensions)
+    return dict(positions=positions, velocities=velocities, densities=densities, masses=masses, isFluid=isFluid,
+                pressures=taitEquationOfState(densities, rho0, c0), h=h, spacing=spacing, i=i, j=j,
+                separation=separation, distance=distance, values=kernel.evaluateBatch(distance, h),
+                gradients=kernel.gradientBatch(separation, distance, h), kernel=kernel)
+
+
+def makeShifting():
+    """Particle shifting (src/pysurf/sphSolver.py:824-1010, and its step in _integrate, 1760-1785): the
+    fields, the displacement, the density and velocity changes on the six clouds, and a sloshing run
+    with particleShifting on."""
+    from pysurf.sphSolver import shiftedVelocityChange, shiftingDisplacement, shiftingFields
+    out = {}
+    for dimensions in (2, 3):
+        for kernelType in ('cubicSpline', 'wendlandC2'):
+            tag = f'{dimensions}d_{kernelType}'
+            case = latticeCloud(dimensions, kernelType)
+            for key in ('positions', 'velocities', 'densities', 'masses', 'isFluid', 'pressures', 'h'):
+                out[f'{tag}/{key}'] = np.asarray(case[key])
+            out[f'{tag}/kernel'] = np.array(1 if kernelType == 'wendlandC2' else 0)
+            i, j, fluid = case['i'], case['j'], case['isFluid']
+            n = len(fluid)
+            spacing = case['spacing']
+            spacingKernel = float(case['kernel'].evaluate(spacing, case['h']))
+            fields = shiftingFields(case['masses'], case['densities'], i, j, case['separation'], case['values'],
+                                    case['gradients'], n, spacingKernel)
+            size = 0.2 * 0.1 * (2.0 * case['h']) ** 2
+            shift, densityChange = shiftingDisplacement(*fields, i, j, case['values'], fluid, size, case['h'],
+                                                        kernelType)
+            velocityChange = shiftedVelocityChange(case['masses'], case['densities'], case['velocities'], i, j,
+                                                   case['gradients'], shift, fluid[i] & fluid[j])
+            names = ('gradient', 'plain', 'divergence', 'densityGradient')
+            for key, value in list(zip(names, fields)) + [('shift', shift), ('densityChange', densityChange),
+                                                          ('velocityChange', velocityChange)]:
+                out[f'{tag}/{key}'] = np.asarray(value)
+            out[f'{tag}/spacingKernel'] = np.array(spacingKernel)
+            out[f'{tag}/size'] = np.array(size)
+    runs = {}
+    solver, particles, boundary = sloshing(particleShifting=True, densityDiffusion='hydrostatic', **deltaContinuity)
+    runs['shifting/mach'] = np.array(solver.config.shiftingMach)
+    runs['shifting/spacing'] = np.array(solver.config.particleSpacing)
+    recordRun(runs, 'shifting', solver, particles, 30, containerRecord(boundary))
+    out.update(runs)
+    np.savez_compressed(os.path.join(HERE, 'shifting.npz'), **out)
+
+
 def main():
     root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('PYSURF_REFERENCE', '')
     if not root or not os.path.isdir(root):
         raise SystemExit('Give the reference checkout: make_golden.py /path/to/reference [fixture ...]')
     loadReference(root)
     makers = {'cellkeys': makeCellKeys, 'clouds': makeClouds, 'enforce': makeEnforcement, 'split': makeSplit,
-              'beach': makeBeach, 'runs': makeRuns, 'breaking': makeBreaking, 'closure': makeClosure}
+              'beach': makeBeach, 'runs': makeRuns, 'breaking': makeBreaking, 'closure': makeClosure,
+              'shifting': makeShifting}
     for name in (sys.argv[2:] or list(makers)):
         makers[name]()
     for name in sorted(os.listdir(HERE)):

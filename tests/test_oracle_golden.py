@@ -186,3 +186,42 @@ def test_closure_step_follows_the_reference_host_steps():
     assert np.allclose(state['positions'], r['finalPositions'], rtol=0.0, atol=1e-11)
     assert np.allclose(state['velocities'], r['finalVelocities'], rtol=0.0, atol=1e-8)
     assert np.allclose(state['densities'], r['finalDensities'], rtol=1e-11, atol=0.0)
+
+
+SHIFT_CLOUDS = ['2d_cubicSpline', '2d_wendlandC2', '3d_cubicSpline', '3d_wendlandC2']
+
+
+@pytest.mark.parametrize('tag', SHIFT_CLOUDS)
+def test_shifting_matches_the_reference(tag):
+    # src/pysurf/sphSolver.py:824-1010 on water over a wall layer: fields, shift, density and velocity changes
+    k = golden('shifting.npz', tag)
+    kernelType = 'wendlandC2' if int(k['kernel']) == 1 else 'cubicSpline'
+    s = oracle.System(k['positions'], k['masses'], k['isFluid'], float(k['h']), kernelType, 0.0)
+    fluid = k['isFluid']
+    fields = s.shiftingFields(k['densities'], float(k['spacingKernel']))
+    for got, name in zip(fields, ('gradient', 'plain', 'divergence', 'densityGradient')):
+        assert close(got[fluid], k[name][fluid]), name
+    dim = k['positions'].shape[1]
+    shift, drho, dv = s.shift(k['densities'], k['velocities'], fields, float(k['size']), {2: 1.5, 3: 2.4}[dim],
+                              0.4 if kernelType == 'wendlandC2' else 0.3)
+    assert np.array_equal(np.abs(shift).sum(1) > 0, np.abs(k['shift']).sum(1) > 0)
+    assert close(shift, k['shift']) and close(drho, k['densityChange']) and close(dv, k['velocityChange'])
+
+
+def test_shifting_step_follows_the_reference_host_steps():
+    r = golden('shifting.npz', 'shifting')
+    base = stepperFor(r)
+    sp = base.params
+    stepper = oracle.Stepper(int(sp.dim), 'wendlandC2' if sp.kind == 1 else 'cubicSpline', sp.hMax, sp.rho0, sp.c0,
+                             sp.alpha, r['gravity'], sp.boundaryFactor, sp.xsphEpsilon, sp.densityFloor,
+                             ['none', 'molteni', 'hydrostatic', 'antuono'][sp.diffusion], sp.delta,
+                             bool(sp.wallExtrapolated), bool(sp.tension), bool(sp.corrected), bool(sp.limited),
+                             sp.cfl, sp.maxTimeStep, sp.period, base.filterInterval,
+                             ('container', r['boundary_lower'], r['boundary_upper'], bool(r['boundary_openTop'])),
+                             shifting=True, shiftingMach=float(r['mach']), spacing=float(r['spacing']))
+    state = {k: r[k].copy() for k in ('positions', 'velocities', 'densities', 'masses', 'isFluid')}
+    dts = [stepper(state) for _ in range(int(r['steps']))]
+    assert np.allclose(dts, r['dts'], rtol=1e-10, atol=0.0)
+    assert np.allclose(state['positions'], r['finalPositions'], rtol=0.0, atol=1e-11)
+    assert np.allclose(state['velocities'], r['finalVelocities'], rtol=0.0, atol=1e-8)
+    assert np.allclose(state['densities'], r['finalDensities'], rtol=1e-11, atol=0.0)
