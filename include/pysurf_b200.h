@@ -85,6 +85,17 @@ int sph_set_viscosity_limiter(SphSystem *sys, int enabled);
  * coefficient as the harmonic mean of the two deltas. */
 int sph_set_closure(SphSystem *sys, int enabled, double sound_speed, double reference_density,
                     double kinematic_viscosity);
+/* PairSums.setShifting (src/pysurf/sphGpu.py:1927-1957): particle shifting on or off, with the
+ * Mach number of its size CFL Ma (2h)^2, the particle spacing (for the anti-clumping weight's
+ * W(dx)), c0, and whether each particle's size is 2 h |v_i| dt instead (local).  It needs one
+ * smoothing length for every particle.  When on, each device step shifts the fluid after the
+ * density update, from the step's starting geometry (src/pysurf/sphSolver.py:1760-1785). */
+int sph_set_shifting(SphSystem *sys, int enabled, double mach, double spacing, double sound_speed, int local);
+/* PairSums.shiftingDisplacement (src/pysurf/sphGpu.py:1980-1995): this step's shift (n, dim), density
+ * change (n) and velocity change (n, dim) of every particle, caller order, zero on the boundary and
+ * the free surface. */
+int sph_shifting_displacement(SphSystem *sys, const double *densities, double time_step, const double *velocities,
+                              double *shifts, double *density_changes, double *velocity_changes);
 /* PairSums.closureCoefficients (src/pysurf/sphGpu.py:1841-1853): alpha_i and delta_i, caller order. */
 int sph_closure_coefficients(SphSystem *sys, const double *velocities, const double *densities, double *alphas,
                              double *deltas);

@@ -85,6 +85,12 @@ struct Params {
     float waterTerm;        // 2 (dim + 2) nu / c0: the water's own viscosity as an alpha times h
     float closureRho0;
     float closureC0;        // the closure's sound speed: its coefficients and its diffusion's 2 c0
+    // particle shifting (src/pysurf/sphSolver.py:824-1010): W(dx) for the anti-clumping weight, the
+    // free surface's divergence and lopsidedness thresholds, the size CFL Ma (2h)^2 or 2 h |v| dt
+    int shifting, shiftLocal;
+    float spacingKernel, shiftThreshold, lopsidedness;
+    double shiftScale;      // c0 Ma 4 h: the size CFL Ma (2h)^2 = shiftScale dt
+    double shiftDt;         // the host-step call's dt (the device steps take ctl->dt)
     // neighbour table: up to listCap entries a particle (a multiple of 4), entry k of slot i at
     // 4 ((k / 4) listStride + i) + k % 4; listCap 0: no table, the sweeps walk the cells
     int listCap;
@@ -105,6 +111,9 @@ struct Frame {
     float *scalar;          // scratch per particle (Shepard, wall pressure outputs)
     float4 *vec;            // scratch per particle (XSPH transport velocity)
     float2 *eddy;           // closure: each particle's (alpha_i, delta_i)
+    // shifting: grad C (w unused), grad C0 (w: div r, -1 where the support is lopsided, 1e6 on the
+    // boundary), grad rho; the shift (w: the density change) and the velocity change
+    float4 *shiftGrad, *shiftPlain, *shiftRhoGrad, *shift, *shiftDv;
     int *nbr;               // neighbour table (chunks of four), top bit: a pair across the periodic seam
     int *ncount;            // each slot's neighbour count (may exceed the table's capacity)
     // master (current buffers)

@@ -32,7 +32,7 @@ struct Enforcement {
     double originX, originY, stepX, stepY, lowY, highY, lowX, highX;
 };
 
-enum class Stage { ShepardSum, ShepardApply, Wall, Gradients, Momentum, Kick, Continuity, Xsph, List, Closure };
+enum class Stage { ShepardSum, ShepardApply, Wall, Gradients, Momentum, Kick, Continuity, Xsph, List, Closure, ShiftFields, Shift, ShiftDrift, FrameDensity };
 
 struct LaunchArgs {
     Params P;

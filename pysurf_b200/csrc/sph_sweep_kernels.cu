@@ -735,6 +735,228 @@ xsphKernel(Params P, Frame F, Control *ctl, Enforcement E, const float *densitie
 }
 
 // ------------------------------------------------------------------------------------------
+// Particle shifting (src/pysurf/sphGpu.py:856-1008; src/pysurf/sphSolver.py:824-1010), after the
+// density update, from the step's starting geometry (the frame's points), the updated densities and
+// the kicked velocities
+// ------------------------------------------------------------------------------------------
+
+// The frame takes the updated float64 densities: rho, rho - rho0, V = m / rho (p and p / rho^2
+// are not read again this step).
+template <int D>
+__global__ void frameDensityKernel(Params P, Frame F, const Control *ctl)
+{
+    if (ctl && !ctl->active) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    storeDensity<D>(F, i, massOf<D>(F, i), F.rho[i], P.devReference, F.pres[i]);
+}
+
+// Over every neighbour of a fluid slot: grad C with the anti-clumping weight 1 + 0.2 (W / W(dx))^4,
+// grad C0, div r = -sum V_j r_ij . grad W_ij, grad rho from the deviations.
+template <int D, int K>
+struct ShiftFieldsVisit {
+    static constexpr bool kSkipCoincident = true;
+    static constexpr bool kKinetic = false;
+    const Params &P; const Frame &F;
+    Smoothing<K, D> S;
+    float devI, gradient[3], plain[3], densityGradient[3], total;
+    __device__ bool accept(bool) const { return true; }
+    __device__ void operator()(int j, const float *d, float r, float h, bool, int, const float4 &B, const float4 &)
+    {
+        const KernelAt k = S.at(h);
+        const float q = r * k.invH;
+        const float4 X = auxRow<D>(F, j);
+        const float volume = volumeIn<D>(B, X);
+        const float grad = kernelGradient<K>(q, k);         // (dW/dr) / r
+        const float ratio = kernelValue<K>(q, k) / P.spacingKernel, square = ratio * ratio;
+        const float weight = 1.0f + 0.2f * square * square;
+        const float difference = deviationIn<D>(B, X) - devI;
+        for (int a = 0; a < D; ++a) {
+            const float weighted = volume * grad * d[a];
+            plain[a] += weighted;
+            gradient[a] += weight * weighted;
+            densityGradient[a] += difference * weighted;
+        }
+        total -= volume * grad * r * r;
+    }
+};
+
+template <int D, int K, int T>
+__global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>()) shiftFieldsKernel(Params P, Frame F, const Control *ctl)
+{
+    if (ctl && !ctl->active) return;
+    const Group<T> G = groupOf<T>();
+    const int i = G.i;
+    if (i >= P.n) return;
+    const float hs = signedLength<D>(F, i);
+    if (hs <= 0.0f) {
+        if (G.t != 0) return;
+        const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        F.shiftGrad[i] = zero;
+        F.shiftPlain[i] = make_float4(0.0f, 0.0f, 0.0f, 1.0e6f);
+        F.shiftRhoGrad[i] = zero;
+        return;
+    }
+    ShiftFieldsVisit<D, K> visit{P, F, Smoothing<K, D>(P)};
+    visit.devI = deviationOf<D>(F, i);
+    for (int a = 0; a < 3; ++a) visit.gradient[a] = visit.plain[a] = visit.densityGradient[a] = 0.0f;
+    visit.total = 0.0f;
+    forEachNeighbour<D, T>(P, F, i, G.t, hs, visit);
+    float c[3] = {0.0f, 0.0f, 0.0f}, g[3] = {0.0f, 0.0f, 0.0f}, rg[3] = {0.0f, 0.0f, 0.0f};
+    for (int a = 0; a < D; ++a) {
+        c[a] = groupSum<T>(visit.plain[a], G.mask);
+        g[a] = groupSum<T>(visit.gradient[a], G.mask);
+        rg[a] = groupSum<T>(visit.densityGradient[a], G.mask);
+    }
+    float total = groupSum<T>(visit.total, G.mask);
+    if (G.t != 0) return;
+    // a lopsided support marks the free surface (src/pysurf/sphSolver.py:889-902)
+    if (hs * sqrtf(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]) > P.lopsidedness) total = -1.0f;
+    F.shiftGrad[i] = make_float4(g[0], g[1], g[2], 0.0f);
+    F.shiftPlain[i] = make_float4(c[0], c[1], c[2], total);
+    F.shiftRhoGrad[i] = make_float4(rg[0], rg[1], rg[2], 0.0f);
+}
+
+// The surface neighbours of a slot: whether there is one within the support, and the
+// kernel-weighted sum of their outward normals -grad C0 / |grad C0|.
+template <int D, int K>
+struct SurfaceVisit {
+    static constexpr bool kSkipCoincident = false;
+    static constexpr bool kKinetic = false;
+    const Params &P; const Frame &F;
+    Smoothing<K, D> S;
+    float normal[3];
+    int vicinity;
+    __device__ bool accept(bool fluidJ) const { return fluidJ; }
+    __device__ void operator()(int j, const float *, float r, float h, bool, int, const float4 &, const float4 &)
+    {
+        const float4 plainJ = __ldg(&F.shiftPlain[j]);
+        if (!(plainJ.w < P.shiftThreshold)) return;
+        vicinity = 1;
+        const float length = sqrtf(plainJ.x * plainJ.x + plainJ.y * plainJ.y + plainJ.z * plainJ.z);
+        if (length > 0.0f) {
+            const KernelAt k = S.at(h);
+            const float w = kernelValue<K>(r * k.invH, k) / length;
+            normal[0] -= w * plainJ.x;
+            normal[1] -= w * plainJ.y;
+            normal[2] -= w * plainJ.z;
+        }
+    }
+};
+
+// The velocity at the shifted position: sum_j V_j (v_j - v_i) (grad W_ij . shift) over fluid pairs.
+template <int D, int K>
+struct ShiftedVelocityVisit {
+    static constexpr bool kSkipCoincident = true;
+    static constexpr bool kKinetic = true;
+    const Params &P; const Frame &F;
+    Smoothing<K, D> S;
+    float vi[3], shift[3], change[3];
+    __device__ bool accept(bool fluidJ) const { return fluidJ; }
+    __device__ void operator()(int j, const float *d, float r, float h, bool, int, const float4 &B, const float4 &Kj)
+    {
+        const KernelAt k = S.at(h);
+        const float4 X = auxRow<D>(F, j);
+        float dot = 0.0f;
+        for (int a = 0; a < D; ++a) dot += d[a] * shift[a];
+        const float f = volumeIn<D>(B, X) * kernelGradient<K>(r * k.invH, k) * dot;
+        float vj[3];
+        velocityIn<D>(Kj, vj);
+        for (int a = 0; a < D; ++a) change[a] += f * (vj[a] - vi[a]);
+    }
+};
+
+// The shift of a fluid slot off the free surface: -size grad C, along the surface next to a
+// surface particle (none where h |grad C| > 0.03 there), with the density change shift . grad rho
+// and the velocity change at the new position.  size: CFL Ma (2h)^2 with CFL = c0 dt / h, or
+// 2 h |v_i| dt (local).
+template <int D, int K, int T>
+__global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>()) shiftKernel(Params P, Frame F, const Control *ctl)
+{
+    if (ctl && !ctl->active) return;
+    const Group<T> G = groupOf<T>();
+    const int i = G.i;
+    if (i >= P.n) return;
+    const float4 zero = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    const float hs = signedLength<D>(F, i);
+    if (hs <= 0.0f || !(F.shiftPlain[i].w >= P.shiftThreshold)) {
+        if (G.t == 0) { F.shift[i] = zero; F.shiftDv[i] = zero; }
+        return;
+    }
+    SurfaceVisit<D, K> surface{P, F, Smoothing<K, D>(P)};
+    surface.normal[0] = surface.normal[1] = surface.normal[2] = 0.0f;
+    surface.vicinity = 0;
+    forEachNeighbour<D, T>(P, F, i, G.t, hs, surface);
+    float normal[3];
+    for (int a = 0; a < 3; ++a) normal[a] = groupSum<T>(surface.normal[a], G.mask);
+    const bool vicinity = groupSum<T>((float)surface.vicinity, G.mask) > 0.0f;
+    float vi[3];
+    velocityOf<D>(F, i, vi);
+    const double dt = ctl ? ctl->dt : P.shiftDt;
+    const float size =
+        P.shiftLocal ? (float)(2.0 * (double)hs * (double)sqrtf(vi[0] * vi[0] + vi[1] * vi[1] + vi[2] * vi[2]) * dt)
+                     : (float)(P.shiftScale * dt);
+    const float4 g = F.shiftGrad[i];
+    float shift[3] = {-size * g.x, -size * g.y, -size * g.z};
+    if (vicinity) {
+        if (hs * sqrtf(g.x * g.x + g.y * g.y + g.z * g.z) > 0.03f) {
+            shift[0] = shift[1] = shift[2] = 0.0f;
+        } else {
+            const float weight = sqrtf(normal[0] * normal[0] + normal[1] * normal[1] + normal[2] * normal[2]);
+            if (weight > 0.0f) {
+                float dot = 0.0f;
+                for (int a = 0; a < 3; ++a) { normal[a] /= weight; dot += shift[a] * normal[a]; }
+                for (int a = 0; a < 3; ++a) shift[a] -= dot * normal[a];
+            }
+        }
+    }
+    if (D == 2) shift[2] = 0.0f;
+    const float4 rg = F.shiftRhoGrad[i];
+    const float densityChange = shift[0] * rg.x + shift[1] * rg.y + shift[2] * rg.z;
+    float change[3] = {0.0f, 0.0f, 0.0f};
+    if (shift[0] != 0.0f || shift[1] != 0.0f || shift[2] != 0.0f) {
+        ShiftedVelocityVisit<D, K> velocity{P, F, Smoothing<K, D>(P)};
+        for (int a = 0; a < 3; ++a) { velocity.vi[a] = vi[a]; velocity.shift[a] = shift[a]; velocity.change[a] = 0.0f; }
+        forEachNeighbour<D, T>(P, F, i, G.t, hs, velocity);
+        for (int a = 0; a < D; ++a) change[a] = groupSum<T>(velocity.change[a], G.mask);
+    }
+    if (G.t != 0) return;
+    F.shift[i] = make_float4(shift[0], shift[1], shift[2], densityChange);
+    F.shiftDv[i] = make_float4(change[0], change[1], change[2], 0.0f);
+}
+
+// The drift of a shifting step (src/pysurf/sphGpu.py:1142-1186): x += u dt + shift, rho and v take
+// their changes, then the periodic wrap and the enforcement.  transport: XSPH's F.vec, else v.
+template <int D>
+__global__ void shiftDriftKernel(Params P, Frame F, Control *ctl, Enforcement E, int useTransport)
+{
+    if (!ctl->active) return;
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n || !F.fluid[i]) return;
+    const double dt = ctl->dt;
+    const float4 s = F.shift[i], dv = F.shiftDv[i];
+    const float4 u = F.vec[i];
+    const float sh[3] = {s.x, s.y, s.z}, dvel[3] = {dv.x, dv.y, dv.z}, ut[3] = {u.x, u.y, u.z};
+    double x[3] = {0.0, 0.0, 0.0}, v[3] = {0.0, 0.0, 0.0};
+    for (int a = 0; a < D; ++a) {
+        const double velocity = useTransport ? (double)ut[a] : F.v[a][i];
+        x[a] = F.x[a][i] + velocity * dt;
+        x[a] = x[a] + (double)sh[a];
+        v[a] = F.v[a][i] + (double)dvel[a];
+    }
+    F.rho[i] = F.rho[i] + (double)s.w;
+    if (P.period > 0.0) x[1] = x[1] - P.period * floor(x[1] / P.period);
+    enforceOne(E, D, x, v);
+    bool finite = isfinite(F.rho[i]);
+    for (int a = 0; a < D; ++a) {
+        F.x[a][i] = x[a];
+        F.v[a][i] = v[a];
+        finite = finite && isfinite(x[a]) && isfinite(v[a]);
+    }
+    if (!finite) atomicOr(&ctl->error, kErrNonFinite);
+}
+
+// ------------------------------------------------------------------------------------------
 // Launchers
 // ------------------------------------------------------------------------------------------
 
@@ -781,6 +1003,10 @@ static void launchT(const LaunchArgs &A, Stage stage)
     case Stage::Xsph: xsphKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.densities, A.flag); break;
     case Stage::List: launchList<D>(A); break;
     case Stage::Closure: closureKernel<D><<<pointwise, kBlock, 0, st>>>(P, F, A.ctl); break;
+    case Stage::ShiftFields: shiftFieldsKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl); break;
+    case Stage::Shift: shiftKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl); break;
+    case Stage::ShiftDrift: shiftDriftKernel<D><<<pointwise, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.flag); break;
+    case Stage::FrameDensity: frameDensityKernel<D><<<pointwise, kBlock, 0, st>>>(P, F, A.ctl); break;
     }
 }
 

@@ -57,6 +57,19 @@ double sigmaUnit(int kind, int dim)
     return dim == 2 ? 10.0 / (7.0 * pi) : 1.0 / pi;
 }
 
+// W(r) at h in float64 (src/pysurf/sphKernels.py:108-648), for the shift's W(dx).
+double kernelValueHost(int kind, int dim, double r, double h)
+{
+    const double q = r / h, sigma = sigmaUnit(kind, dim) / (dim == 2 ? h * h : h * h * h);
+    if (q >= 2.0) return 0.0;
+    if (kind == 1) {
+        const double rest = 1.0 - 0.5 * q;
+        return sigma * rest * rest * rest * rest * (2.0 * q + 1.0);
+    }
+    if (q < 1.0) return sigma * (1.0 - 1.5 * q * q + 0.75 * q * q * q);
+    return sigma * 0.25 * (2.0 - q) * (2.0 - q) * (2.0 - q);
+}
+
 template <class T>
 int deviceAlloc(T **ptr, size_t count)
 {
@@ -90,6 +103,10 @@ struct SphSystem {
     int diffusionMode = 0;
     double diffusionDelta = 0.1, diffusionC0 = 1.0, diffusionRho0 = 1000.0, diffusionG = 0.0;
     int wallExtrapolated = 0, tension = 0, corrected = 0, limited = 0;
+    int shifting = 0, shiftLocal = 0;   // particle shifting, its W(dx) and its size's c0 Ma 4 h
+    double spacingKernel = 1.0, shiftScale = 0.0;
+    float4 *shiftGrad = nullptr, *shiftPlain = nullptr, *shiftRhoGrad = nullptr, *shiftOut = nullptr,
+           *shiftDv = nullptr;
     int closure = 0;            // delta-LES-SPH closure, with its sound speed, rho0 and the water's viscosity
     double closureC0 = 1.0, closureRho0 = 1000.0, closureNu = 0.0;
     float2 *eddy = nullptr;
@@ -164,9 +181,11 @@ struct SphSystem {
         }
         void *ptrs[] = {pa, pb, kin, G[0], G[1], G[2], L[0], L[1], L[2], gradRho, acc, vec, aux, pres, rate,
                         scalar, cell, sortBuffers.slotCell, sortBuffers.slotWithin, sortBuffers.perm,
-                        sortBuffers.bucket, dStage, dStageU8, dRank, nbr, ncount, eddy};
+                        sortBuffers.bucket, dStage, dStageU8, dRank, nbr, ncount, eddy, shiftGrad, shiftPlain,
+                        shiftRhoGrad, shiftOut, shiftDv};
         for (void *p : ptrs) cudaFree(p);
         eddy = nullptr;
+        shiftGrad = shiftPlain = shiftRhoGrad = shiftOut = shiftDv = nullptr;
         nbr = ncount = nullptr;
         nbrEntries = 0;
         listCap = 0;
@@ -239,6 +258,10 @@ struct SphSystem {
         TRY(deviceAlloc(&acc, cap));
         TRY(deviceAlloc(&vec, cap));
         TRY(deviceAlloc(&eddy, cap));
+        for (float4 **p : {&shiftGrad, &shiftPlain, &shiftRhoGrad, &shiftOut, &shiftDv}) {
+            TRY(deviceAlloc(p, cap));
+            CUDA_TRY(cudaMemsetAsync(*p, 0, sizeof(float4) * cap, stream));
+        }
         TRY(deviceAlloc(&rate, cap));
         TRY(deviceAlloc(&scalar, cap));
         TRY(deviceAlloc(&cell, cap));
@@ -353,6 +376,13 @@ struct SphSystem {
         P.waterTerm = (float)(2.0 * (dim + 2) * closureNu / closureC0);
         P.closureRho0 = (float)closureRho0;
         P.closureC0 = (float)closureC0;
+        P.shifting = shifting;
+        P.shiftLocal = shiftLocal;
+        P.spacingKernel = (float)spacingKernel;
+        P.shiftThreshold = dim == 2 ? 1.5f : 2.4f;          // src/pysurf/sphSolver.py:265
+        P.lopsidedness = kind == 1 ? 0.4f : 0.3f;           // src/pysurf/sphSolver.py:266
+        P.shiftScale = shiftScale;
+        P.shiftDt = 0.0;
         P.wallExtrapolated = wallExtrapolated;
         P.xsphEpsilon = (float)xsphEpsilon;
         P.listCap = listCap;
@@ -368,6 +398,8 @@ struct SphSystem {
         F.G0 = G[0]; F.G1 = G[1]; F.G2 = G[2];
         F.L0 = L[0]; F.L1 = L[1]; F.L2 = L[2];
         F.gradRho = gradRho; F.acc = acc; F.rate = rate; F.scalar = scalar; F.vec = vec; F.eddy = eddy;
+        F.shiftGrad = shiftGrad; F.shiftPlain = shiftPlain; F.shiftRhoGrad = shiftRhoGrad; F.shift = shiftOut;
+        F.shiftDv = shiftDv;
         F.nbr = nbr; F.ncount = ncount;
         const MasterView &M = master[cur];
         for (int a = 0; a < 3; ++a) { F.x[a] = M.x[a]; F.v[a] = M.v[a]; }
@@ -701,6 +733,23 @@ int sph_set_closure(SphSystem *sys, int enabled, double sound_speed, double refe
     return SPH_OK;
 }
 
+int sph_set_shifting(SphSystem *sys, int enabled, double mach, double spacing, double sound_speed, int local)
+{
+    CHECK_SYS(sys);
+    if (enabled && (!(spacing > 0.0) || !(sound_speed > 0.0) || !(mach >= 0.0)))
+        return fail(SPH_ERR_INVALID, "shifting needs a positive spacing and sound speed, a Mach number >= 0");
+    if (enabled && sys->mixedH)
+        return fail(SPH_ERR_INVALID, "particle shifting needs one smoothing length for every particle");
+    sys->shifting = enabled ? 1 : 0;
+    if (enabled) {
+        sys->shiftLocal = local ? 1 : 0;
+        sys->spacingKernel = kernelValueHost(sys->kind, sys->dim, spacing, sys->h);
+        sys->shiftScale = sound_speed * mach * 4.0 * sys->h;
+    }
+    sys->graphDirty = true;
+    return SPH_OK;
+}
+
 int sph_set_viscosity_limiter(SphSystem *sys, int enabled)
 {
     CHECK_SYS(sys);
@@ -751,6 +800,8 @@ static int loadState(SphSystem *sys, int64_t count, const double *positions, con
                                              std::to_string(sys->h) + " m the cell list is built for");
         if (!(hMin > 0.0)) return fail(SPH_ERR_INVALID, "smoothing lengths must be positive");
     }
+    if (mixed && sys->shifting)
+        return fail(SPH_ERR_INVALID, "particle shifting needs one smoothing length for every particle");
     TRY(sys->reserve(n, false));
     if (sys->n != n) sys->graphDirty = true;
     sys->n = n;
@@ -951,6 +1002,39 @@ int sph_closure_coefficients(SphSystem *sys, const double *velocities, const dou
         alphas[orig[s]] = packed[s].x;
         deltas[orig[s]] = packed[s].y;
     }
+    return SPH_OK;
+}
+
+int sph_shifting_displacement(SphSystem *sys, const double *densities, double time_step, const double *velocities,
+                              double *shifts, double *density_changes, double *velocity_changes)
+{
+    CHECK_SYS(sys);
+    TRY(needFrame(sys));
+    if (!sys->shifting) return fail(SPH_ERR_STATE, "shifting is off: call sph_set_shifting first");
+    if (sys->mixedH) return fail(SPH_ERR_INVALID, "particle shifting needs one smoothing length for every particle");
+    if (sys->n == 0) return SPH_OK;
+    if (!densities || !velocities || !shifts || !density_changes || !velocity_changes)
+        return fail(SPH_ERR_INVALID, "null argument");
+    TRY(loadFields(sys, velocities, densities, nullptr));
+    LaunchArgs A = sys->args(nullptr);
+    A.P.shiftDt = time_step;
+    launchStage(A, Stage::ShiftFields);
+    launchStage(A, Stage::Shift);
+    const int n = sys->n, dim = sys->dim;
+    double *out = sys->stage(SphSystem::kOutSlot);
+    launchScatterFloat4(n, dim, A.F.orig, sys->shiftOut, out, sys->stream);
+    TRY(sys->download(shifts, out, sizeof(double) * n * dim));
+    CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    launchScatterFloat4(n, dim, A.F.orig, sys->shiftDv, out, sys->stream);
+    TRY(sys->download(velocity_changes, out, sizeof(double) * n * dim));
+    CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    // the density changes ride in the shifts' fourth lane
+    std::vector<float4> packed(n);
+    std::vector<int> orig(n);
+    CUDA_TRY(cudaMemcpyAsync(packed.data(), sys->shiftOut, sizeof(float4) * n, cudaMemcpyDeviceToHost, sys->stream));
+    CUDA_TRY(cudaMemcpyAsync(orig.data(), A.F.orig, sizeof(int) * n, cudaMemcpyDeviceToHost, sys->stream));
+    CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    for (int s = 0; s < n; ++s) density_changes[orig[s]] = packed[s].w;
     return SPH_OK;
 }
 
@@ -1202,7 +1286,25 @@ static void enqueueIntegrate(SphSystem *sys, cudaEvent_t *events = nullptr)
     LaunchArgs A = sys->args(sys->ctl);
     launchStage(A, Stage::Kick);
     mark(sys, events, 6);
-    if (sys->xsphEpsilon > 0.0) {
+    if (sys->shifting) {
+        // the density update, then the shift from the step's starting geometry, the updated
+        // densities and the kicked velocities, then one drift (src/pysurf/sphSolver.py:1760-1785)
+        A.flag = 1;
+        launchStage(A, Stage::Continuity);
+        int useTransport = 0;
+        if (sys->xsphEpsilon > 0.0) {
+            launchRefreshDensity(sys->n, A.F.rho, sys->scalar, sys->stream);
+            A.densities = sys->scalar;
+            A.flag = 0;
+            launchStage(A, Stage::Xsph);
+            useTransport = 1;
+        }
+        launchStage(A, Stage::FrameDensity);
+        launchStage(A, Stage::ShiftFields);
+        launchStage(A, Stage::Shift);
+        A.flag = useTransport;
+        launchStage(A, Stage::ShiftDrift);
+    } else if (sys->xsphEpsilon > 0.0) {
         A.flag = 1;
         launchStage(A, Stage::Continuity);
         launchRefreshDensity(sys->n, A.F.rho, sys->scalar, sys->stream);
@@ -1622,6 +1724,8 @@ int sph_split(SphSystem *sys, const uint8_t *mask, double reference_density, dou
     if (!mask || !split) return fail(SPH_ERR_INVALID, "null argument");
     if (!sys->resident) return fail(SPH_ERR_STATE, "no device state: call sph_push first");
     if (!(length_ratio > 0.0) || length_ratio > 1.0) return fail(SPH_ERR_INVALID, "the length ratio must be in (0, 1]");
+    if (sys->shifting && length_ratio != 1.0)
+        return fail(SPH_ERR_INVALID, "particle shifting needs one smoothing length for every particle");
     int n = sys->n, dim = sys->dim;
     *split = 0;
     if (n == 0) return SPH_OK;

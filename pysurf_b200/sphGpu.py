@@ -11,8 +11,8 @@ What it carries: the cubic spline and the Wendland C2 kernels; the plain and the
 artificial viscosity; the continuity sum plain and corrected; the delta-SPH diffusive term in its
 'molteni', 'hydrostatic' and 'antuono' forms; the extrapolated wall pressure; negative pressure;
 the Shepard filter; XSPH; a periodic y axis; mixed smoothing lengths; container, bed and height
-field enforcement; the delta-LES-SPH closure.  Particle shifting and the energy budget are not
-carried yet: enabling one raises NotImplementedError, and their setters accept them off.
+field enforcement; the delta-LES-SPH closure; particle shifting.  The energy budget is not
+carried yet: enabling it raises NotImplementedError, and its setter accepts it off.
 
 Beyond the reference's surface, ``advance`` runs a whole span of steps on the device with the
 time step taken there (no host round trip per step), ``split`` refines on the device, and
@@ -219,9 +219,11 @@ class PairSums:
 
     def setShifting(self, enabled: bool, mach: float = 0.1, spacing: float = 1.0, soundSpeed: float = 1.0,
                     local: bool = False) -> None:
-        if enabled:
-            raise NotImplementedError('Particle shifting is not carried by the B200 backend yet.')
-        self.shiftingEnabled = False
+        """Particle shifting (sphSolver.shiftingDisplacement) for every step that follows
+        (src/pysurf/sphGpu.py:1927-1957): size CFL Ma (2h)^2, or 2 h |v_i| dt with `local`."""
+        check(self._lib.sph_set_shifting(self._handle, int(bool(enabled)), float(mach), float(spacing),
+                                         float(soundSpeed), int(bool(local))), 'setShifting')
+        self.shiftingEnabled = bool(enabled)
 
     def setCellsPerSupport(self, cells: int) -> None:
         """Cells per kernel support of the device's cell list (1: 2h wide; 2: h wide; the default 3: 2h/3 wide)."""
@@ -356,7 +358,16 @@ class PairSums:
         return out
 
     def shiftingDisplacement(self, densities, timeStep, velocities):
-        raise NotImplementedError('Particle shifting is not carried by the B200 backend yet.')
+        """This step's shift, density change and velocity change of every particle, zero on the
+        boundary and the free surface (src/pysurf/sphGpu.py:1980-1995)."""
+        n, dim = self.count, self.dimensions
+        shifts, velocityChanges, densityChanges = np.zeros((n, dim)), np.zeros((n, dim)), np.zeros(n)
+        if n:
+            check(self._lib.sph_shifting_displacement(self._handle, dptr(self._scalars(densities)), float(timeStep),
+                                                      dptr(self._vectors(velocities)), dptr(shifts),
+                                                      dptr(densityChanges), dptr(velocityChanges)),
+                  'shiftingDisplacement')
+        return shifts, densityChanges, velocityChanges
 
     def neighborList(self, radius: float | None = None) -> tuple:
         """Every particle's neighbours closer than `radius` (2h by default), itself excluded, as the

@@ -291,3 +291,20 @@ def test_the_closure_run_follows_the_reference_host_steps():
     assert np.abs(state.positions - r['finalPositions']).max() < 1e-6
     assert np.abs(state.velocities - r['finalVelocities']).max() < 1e-3
     assert np.abs(state.densities - r['finalDensities']).max() < 1e-3
+
+
+def test_the_shifting_run_follows_the_reference_host_steps():
+    # a sloshing tank with particle shifting, 30 device steps against the reference's float64 host
+    # steps and the oracle's
+    data = np.load(os.path.join(GOLDEN, 'shifting.npz'))
+    r = golden('shifting.npz', 'shifting')
+    case = caseFromRun(r)
+    case.particleShifting = True
+    case.shiftingMach = float(data['shifting/mach'])
+    case.spacing = float(data['shifting/spacing'])
+    steps = int(r['steps'])
+    state, time, _ = deviceRun(case, steps)
+    assert time == pytest.approx(float(np.sum(r['dts'])), rel=1e-4)
+    assert np.abs(state.positions - r['finalPositions']).max() < 1e-6
+    assert np.abs(state.velocities - r['finalVelocities']).max() < 1e-3
+    assert np.abs(state.densities - r['finalDensities']).max() < 1e-3

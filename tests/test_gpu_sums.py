@@ -280,3 +280,27 @@ def test_closure_sums(tag):
     close(s.pairAccelerations(c['strained'], c['densities'], c['pressures'], c0, alpha, 0.3, g), k['accelerations'])
     # the continuity takes the deltas of the last accelerations, as the reference's device does
     close(s.continuityRate(c['strained'], c['densities']), k['continuity'])
+
+
+SHIFT_CLOUDS = ['2d_cubicSpline', '2d_wendlandC2', '3d_cubicSpline', '3d_wendlandC2']
+
+
+@pytest.mark.parametrize('tag', SHIFT_CLOUDS)
+def test_shifting_displacement(tag):
+    # particle shifting (src/pysurf/sphSolver.py:824-1010) on water over a wall layer: the same
+    # particles shift, by the reference's shifts, density and velocity changes
+    from pysurf_b200.sphGpu import PairSums
+    k = golden('shifting.npz', tag)
+    x = k['positions']
+    kernelType = 'wendlandC2' if int(k['kernel']) == 1 else 'cubicSpline'
+    s = PairSums(x.shape[1], float(k['h']), x.min(axis=0), x.max(axis=0), 0.0, 'float64', 'cuda:0', kernelType)
+    s.update(x, k['masses'], k['isFluid'])
+    h, spacing = float(k['h']), 0.02
+    # size CFL Ma (2h)^2 with CFL = c0 dt / h: the fixture's 0.2 x 0.1 x (2h)^2 at c0 20, Ma 0.1
+    s.setShifting(True, 0.1, spacing, c0, False)
+    dt = 0.2 * h / c0
+    shift, densityChange, velocityChange = s.shiftingDisplacement(k['densities'], dt, k['velocities'])
+    assert np.array_equal(np.abs(shift).sum(1) > 0, np.abs(k['shift']).sum(1) > 0)
+    close(shift, k['shift'])
+    close(densityChange, k['densityChange'])
+    close(velocityChange, k['velocityChange'])
