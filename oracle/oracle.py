@@ -53,7 +53,7 @@ class StepParams(C.Structure):
                 ('upper', C.c_double * 3), ('openTop', C.c_int), ('bed', BedParams), ('field', FieldParams),
                 ('closure', C.c_int), ('viscosity', C.c_double), ('shifting', C.c_int), ('shiftLocal', C.c_int),
                 ('shiftMach', C.c_double), ('spacingKernel', C.c_double), ('shiftThreshold', C.c_double),
-                ('lopsidedness', C.c_double)]
+                ('lopsidedness', C.c_double), ('energy', _vp)]
 
 
 def lib():
@@ -89,6 +89,10 @@ def lib():
         L.or_enforce_bed.argtypes = [C.c_long, C.c_int, _dp, _dp, _u8, C.POINTER(BedParams)]
         L.or_enforce_heightfield.argtypes = [C.c_long, _dp, _dp, _u8, C.POINTER(FieldParams)]
         L.orx_step_size.restype = C.c_long
+        L.or_elastic_energy.argtypes = [C.c_long, _dp, C.c_double, C.c_double, C.c_int, _dp]
+        L.or_elastic_slope.argtypes = [C.c_long, _dp, _dp, C.c_double, C.c_double, C.c_int, _dp]
+        L.or_fluid_energy.argtypes = [C.c_long, C.c_int, _dp, _dp, _dp, _dp, _u8, _dp, C.c_double, C.c_double,
+                                      C.c_int, _dp]
         assert L.orx_step_size() == C.sizeof(StepParams), 'StepParams layout mismatch'
     return _lib
 
@@ -276,6 +280,37 @@ def enforceHeightField(positions, velocities, isFluid, params):
     return x, v
 
 
+# The energy budget's terms the steps keep, in the order of src/pysurf/sphEnergy.py:92-98 (deviceTerms)
+ENERGY_TERMS = ('pressureFluid', 'viscosityFluid', 'pressureWall', 'viscosityWall', 'gravityWork', 'continuityFluid',
+                'continuityWall', 'correction', 'diffusion', 'floor', 'drift', 'clamp', 'shifting', 'filter')
+
+
+def elasticEnergy(densities, rho0, c0, tension=False):
+    """src/pysurf/sphEnergy.py:100-139: the Tait elastic energy per unit mass [J/kg]."""
+    rho = _f64(np.atleast_1d(densities))
+    out = np.empty_like(rho)
+    lib().or_elastic_energy(len(rho), rho, rho0, c0, int(tension), out)
+    return out
+
+
+def elasticSlope(before, after, rho0, c0, tension=False):
+    """src/pysurf/sphEnergy.py:141-160: the secant slope of e, or p / rho^2 for a tiny change."""
+    a, b = np.broadcast_arrays(_f64(np.atleast_1d(before)), _f64(np.atleast_1d(after)))
+    out = np.empty(a.shape)
+    lib().or_elastic_slope(len(out), _f64(a), _f64(b), rho0, c0, int(tension), out)
+    return out
+
+
+def fluidEnergy(state, gravity, rho0, c0, tension=False):
+    """The fluid's kinetic, potential and elastic energy [J] (per unit depth in 2D)."""
+    x = _f64(state['positions'])
+    n, dim = x.shape
+    out = np.empty(3)
+    lib().or_fluid_energy(n, dim, x, _f64(state['velocities']), _f64(state['densities']), _f64(state['masses']),
+                          _u8a(state['isFluid']), _f64(np.resize(gravity, 3)), rho0, c0, int(tension), out)
+    return out
+
+
 class Stepper:
     """The device-resident step of src/pysurf/sphGpu.py:2237-2315 in float64, one call per step."""
 
@@ -304,8 +339,14 @@ class Stepper:
             sp.shiftThreshold = {2: 1.5, 3: 2.4}[dim]
             sp.lopsidedness = 0.4 if kernelType == 'wendlandC2' else 0.3
         self.params, self.filterInterval, self._keep = sp, filterInterval, None
+        self.energy = None
         self.setBoundary(boundary)
         self.time, self.step = 0.0, 0
+
+    def trackEnergy(self, enabled=True):
+        """Keep the energy budget from now on: `energy` holds each term's total since this call."""
+        self.energy = np.zeros(len(ENERGY_TERMS)) if enabled else None
+        self.params.energy = self.energy.ctypes.data if enabled else None
 
     def setBoundary(self, boundary):
         """boundary: None, ('container', lower, upper, openTop), ('bed', BedParams), ('field', FieldParams)."""

@@ -420,12 +420,65 @@ typedef struct {
     int closure;                /* the delta-LES-SPH viscous term on fluid pairs */
     double waterTerm, rho0;     /* 2 (dim + 2) nu / c0, and rho0 */
     const double *alphas;       /* each particle's alpha_i (or_closure_coefficients) */
+    double *parts;              /* energy budget: each fluid row's pressure and viscosity from fluid and
+                                   from boundary neighbours (n x 4 x dim), or NULL */
 } AccelParams;
 
 static double harmonic_mean(double a, double b)
 {
     double both = a + b;
     return both > 0.0 ? 2.0 * a * b / both : 0.0;
+}
+
+/* The energy budget's elastic energy, src/pysurf/sphEnergy.py:100-139 (elasticEnergy): e(rho) per
+ * unit mass = (c0^2 / 7) x^2 (21 + 35 x + 35 x^2 + 21 x^3 + 7 x^4 + x^5) / (6 (1 + x)), x = rho / rho0 - 1,
+ * zero below rho0 unless the fluid carries tension.  scale = c0^2 / 7. */
+static double elastic_energy(double rho, double rho0, double scale, int tension)
+{
+    double x = rho / rho0 - 1.0;
+    double poly = 21.0 + x * (35.0 + x * (35.0 + x * (21.0 + x * (7.0 + x))));
+    double e = scale * x * x * poly / (6.0 * (1.0 + x));
+    return (!tension && x < 0.0) ? 0.0 : e;
+}
+
+/* src/pysurf/sphEnergy.py:141-160 (elasticSlope): the secant (e(after) - e(before)) / (after - before),
+ * or p / rho^2 at the midpoint for a change under 1e-10 rho0. */
+static double elastic_slope(double before, double after, double rho0, double scale, int tension)
+{
+    double change = after - before, mid = 0.5 * (before + after), ratio = mid / rho0;
+    double p = scale * rho0 * (pow(ratio, 7.0) - 1.0);
+    if (!tension && p < 0.0) p = 0.0;
+    if (fabs(change) > 1e-10 * rho0)
+        return (elastic_energy(after, rho0, scale, tension) - elastic_energy(before, rho0, scale, tension)) / change;
+    return p / (mid * mid);
+}
+
+void or_elastic_energy(long n, const double *rho, double rho0, double c0, int tension, double *out)
+{
+    for (long i = 0; i < n; ++i) out[i] = elastic_energy(rho[i], rho0, c0 * c0 / 7.0, tension);
+}
+
+void or_elastic_slope(long n, const double *before, const double *after, double rho0, double c0, int tension,
+                      double *out)
+{
+    for (long i = 0; i < n; ++i) out[i] = elastic_slope(before[i], after[i], rho0, c0 * c0 / 7.0, tension);
+}
+
+/* The fluid's kinetic, potential (-m g . x) and elastic energy [J] (src/pysurf/sphParticles.py:236-255,
+ * src/pysurf/sphSolver.py:2156-2161), summed in particle order. */
+void or_fluid_energy(long n, int dim, const double *x, const double *v, const double *rho, const double *m,
+                     const uint8_t *fluid, const double *g, double rho0, double c0, int tension, double out[3])
+{
+    double k = 0.0, p = 0.0, e = 0.0;
+    for (long i = 0; i < n; ++i) {
+        if (!fluid[i]) continue;
+        double v2 = 0.0, gx = 0.0;
+        for (int c = 0; c < dim; ++c) { v2 += v[i * dim + c] * v[i * dim + c]; gx += g[c] * x[i * dim + c]; }
+        k += 0.5 * m[i] * v2;
+        p -= m[i] * gx;
+        e += m[i] * elastic_energy(rho[i], rho0, c0 * c0 / 7.0, tension);
+    }
+    out[0] = k; out[1] = p; out[2] = e;
 }
 
 /* src/pysurf/sphSolver.py:1232-1274 (closureCoefficients): ||D|| = sqrt(2 D:D), D = (G + G^T) / 2,
@@ -464,7 +517,7 @@ void or_accelerations(const Sys *s, long n, const double *v, const double *rho, 
         for (int c = 0; c < dim; ++c) a[i * dim + c] = 0.0;
         if (!s->fluid[i]) continue;
         double own = p[i] / (rho[i] * rho[i]);
-        double tot[MAXD] = {0};
+        double tot[MAXD] = {0}, part[4][MAXD] = {{0}};
         for (int64_t k = s->off[i]; k < s->off[i + 1]; ++k) {
             long j = s->nbr[k];
             double d[MAXD], r, h;
@@ -506,10 +559,19 @@ void or_accelerations(const Sys *s, long n, const double *v, const double *rho, 
                 visc += -pairAlpha * ap->c0 * h * ap->rho0 * plain / (r * r * rho[i] * rho[j]);
             }
             double coef = -(own + p[j] / (rho[j] * rho[j]) + visc) * s->m[j];
-            double f = coef * kernel_slope(s->kind, dim, r, h) / r;
+            double grad = kernel_slope(s->kind, dim, r, h) / r, f = coef * grad;
             for (int c = 0; c < dim; ++c) tot[c] += f * d[c];
+            if (ap->parts) {
+                /* src/pysurf/sphGpu.py:400-409: pressure and viscosity, from fluid or boundary j */
+                int wall = s->fluid[j] ? 0 : 2;
+                double fp = -(own + p[j] / (rho[j] * rho[j])) * s->m[j] * grad, fv = -visc * s->m[j] * grad;
+                for (int c = 0; c < dim; ++c) { part[wall][c] += fp * d[c]; part[wall + 1][c] += fv * d[c]; }
+            }
         }
         for (int c = 0; c < dim; ++c) a[i * dim + c] = tot[c] + ap->g[c];
+        if (ap->parts)
+            for (int q = 0; q < 4; ++q)
+                for (int c = 0; c < dim; ++c) ap->parts[(i * 4 + q) * dim + c] = part[q][c];
     }
 }
 
@@ -519,6 +581,8 @@ typedef struct {
     int corrected;
     int closure;           /* the pair's delta is the harmonic mean of the two particles' (closure) */
     const double *deltas;
+    double *parts;         /* energy budget: each fluid row's plain sum over fluid and over boundary
+                              neighbours, the correction's part and the diffusion (n x 4), or NULL */
 } ContinuityParams;
 
 /* src/pysurf/sphSolver.py:623-654 (continuityRate), 718-822 (hydrostaticDensityDifference,
@@ -532,7 +596,7 @@ void or_continuity(const Sys *s, long n, const double *v, const double *rho, con
     for (long i = 0; i < n; ++i) {
         int boundaryI = !s->fluid[i];
         int diffuses = cp->mode != 0 && !boundaryI;
-        double total = 0.0;
+        double total = 0.0, plainF = 0.0, plainW = 0.0, diffusive = 0.0;
         for (int64_t k = s->off[i]; k < s->off[i + 1]; ++k) {
             long j = s->nbr[k];
             if (boundaryI && !s->fluid[j]) continue;
@@ -547,9 +611,15 @@ void or_continuity(const Sys *s, long n, const double *v, const double *rho, con
                     for (int b = 0; b < dim; ++b) Ld[a] += L[i * dd + a * dim + b] * d[b];
                 }
             }
-            double dot = 0.0;
-            for (int a = 0; a < dim; ++a) dot += (v[i * dim + a] - v[j * dim + a]) * Ld[a];
+            double dot = 0.0, plainDot = 0.0;
+            for (int a = 0; a < dim; ++a) {
+                dot += (v[i * dim + a] - v[j * dim + a]) * Ld[a];
+                plainDot += (v[i * dim + a] - v[j * dim + a]) * d[a];
+            }
             total += s->m[j] * dot * slope / r;
+            /* src/pysurf/sphGpu.py:508-515: the uncorrected sum, split by the neighbour's kind */
+            if (s->fluid[j]) plainF += s->m[j] * plainDot * slope / r;
+            else plainW += s->m[j] * plainDot * slope / r;
             if (diffuses && s->fluid[j]) {
                 double diff = rho[j] - rho[i];
                 if (cp->mode == 2) {
@@ -562,10 +632,19 @@ void or_continuity(const Sys *s, long n, const double *v, const double *rho, con
                 }
                 double outward = -slope * r;
                 double delta = cp->closure ? harmonic_mean(cp->deltas[i], cp->deltas[j]) : cp->delta;
-                total += 2.0 * delta * h * cp->c0 * diff * outward / (r * r + 0.01 * h * h) * s->m[j] / rho[j];
+                double term = 2.0 * delta * h * cp->c0 * diff * outward / (r * r + 0.01 * h * h) * s->m[j] / rho[j];
+                total += term;
+                diffusive += term;
             }
         }
         out[i] = total;
+        if (cp->parts) {
+            double *q = cp->parts + i * 4;
+            q[0] = boundaryI ? 0.0 : plainF;
+            q[1] = boundaryI ? 0.0 : plainW;
+            q[2] = boundaryI || !cp->corrected ? 0.0 : total - diffusive - plainF - plainW;
+            q[3] = boundaryI ? 0.0 : diffusive;
+        }
     }
 }
 
@@ -869,6 +948,7 @@ typedef struct {
     double viscosity;
     int shifting, shiftLocal;                    /* particle shifting: size c0 dt / h Ma (2h)^2, or 2 h |v| dt */
     double shiftMach, spacingKernel, shiftThreshold, lopsidedness;
+    double *energy;                              /* the energy budget's 14 running totals, or NULL */
 } StepParams;
 
 static double cfl_time_step(double h, double c0, double vmax, double amax, double cfl, double maxdt)
@@ -892,9 +972,20 @@ double or_step(const StepParams *sp, long n, double *x, double *v, double *rho, 
 
     double *tmp = (double *)malloc(sizeof(double) * (size_t)n * 9);
     double *G = NULL, *L = NULL, *gr = NULL;
+    /* The energy budget (src/pysurf/sphGpu.py:1046-1186, 1189-1230): each term's energy, in the
+     * order pressureFluid, viscosityFluid, pressureWall, viscosityWall, gravityWork, continuityFluid,
+     * continuityWall, correction, diffusion, floor, drift, clamp, shifting, filter. */
+    double *E = sp->energy, scale = sp->c0 * sp->c0 / 7.0;
+    double *accParts = E ? (double *)calloc((size_t)n * 4 * dim, sizeof(double)) : NULL;
+    double *rateParts = E ? (double *)calloc((size_t)n * 4, sizeof(double)) : NULL;
     if (sp->filterDensity) {
         or_shepard(&s, n, rho, tmp);
-        for (long i = 0; i < n; ++i) if (fluid[i]) rho[i] = tmp[i];
+        for (long i = 0; i < n; ++i) {
+            if (!fluid[i]) continue;
+            if (E) E[13] += m[i] * (elastic_energy(tmp[i], sp->rho0, scale, sp->tension)
+                                    - elastic_energy(rho[i], sp->rho0, scale, sp->tension));
+            rho[i] = tmp[i];
+        }
     }
     or_equation_of_state(n, rho, fluid, sp->rho0, sp->c0, sp->tension, p);
     if (sp->wallExtrapolated) {
@@ -916,7 +1007,7 @@ double or_step(const StepParams *sp, long n, double *x, double *v, double *rho, 
         or_closure_coefficients(&s, n, G, sp->c0, alphas, deltas);
     }
     AccelParams ap = {sp->c0, sp->alpha, sp->boundaryFactor, {sp->g[0], sp->g[1], sp->g[2]}, sp->limited,
-                      sp->closure, 2.0 * (dim + 2) * sp->viscosity / sp->c0, sp->rho0, alphas};
+                      sp->closure, 2.0 * (dim + 2) * sp->viscosity / sp->c0, sp->rho0, alphas, accParts};
     or_accelerations(&s, n, v, rho, p, G, &ap, a);
     double vmax = 0.0, amax = 0.0;
     for (long i = 0; i < n; ++i) {
@@ -927,8 +1018,25 @@ double or_step(const StepParams *sp, long n, double *x, double *v, double *rho, 
         vmax = sv > vmax ? sv : vmax; amax = sa > amax ? sa : amax;
     }
     double dt = cfl_time_step(sp->hMin, sp->c0, vmax, amax, sp->cfl, sp->maxTimeStep);
-    for (long i = 0; i < n; ++i)
-        if (fluid[i]) for (int c = 0; c < dim; ++c) v[i * dim + c] += a[i * dim + c] * dt;
+    for (long i = 0; i < n; ++i) {
+        if (!fluid[i]) continue;
+        double mean[MAXD];
+        for (int c = 0; c < dim; ++c) {
+            double start = v[i * dim + c];
+            v[i * dim + c] += a[i * dim + c] * dt;
+            mean[c] = 0.5 * (start + v[i * dim + c]);
+        }
+        if (!E) continue;
+        /* work m a . (v + v') / 2 dt of each part of a, and of gravity */
+        for (int q = 0; q < 4; ++q) {
+            double w = 0.0;
+            for (int c = 0; c < dim; ++c) w += accParts[(i * 4 + q) * dim + c] * mean[c];
+            E[q] += m[i] * w * dt;
+        }
+        double w = 0.0;
+        for (int c = 0; c < dim; ++c) w += sp->g[c] * mean[c];
+        E[4] += m[i] * w * dt;
+    }
     int renormalized = sp->diffusion == 3;
     if (sp->corrected || renormalized) {
         L = (double *)malloc(sizeof(double) * (size_t)n * dim * dim);
@@ -939,11 +1047,20 @@ double or_step(const StepParams *sp, long n, double *x, double *v, double *rho, 
         or_density_gradients(&s, n, rho, L, gr);
     }
     ContinuityParams cp = {sp->diffusion, sp->delta, sp->c0, sp->rho0, fabs(sp->g[dim - 1]), sp->corrected,
-                           sp->closure, deltas};
+                           sp->closure, deltas, rateParts};
     or_continuity(&s, n, v, rho, L, gr, &cp, tmp);
     for (long i = 0; i < n; ++i) {
+        double start = rho[i];
         rho[i] += tmp[i] * dt;
+        double unfloored = rho[i];
         if (sp->densityFloor > 0.0 && fluid[i] && rho[i] < sp->densityFloor) rho[i] = sp->densityFloor;
+        if (E && fluid[i]) {
+            /* each part of the rate over the secant slope of e, and the floor's change */
+            double slope = elastic_slope(start, unfloored, sp->rho0, scale, sp->tension);
+            for (int q = 0; q < 4; ++q) E[5 + q] += m[i] * slope * rateParts[i * 4 + q] * dt;
+            E[9] += m[i] * (elastic_energy(rho[i], sp->rho0, scale, sp->tension)
+                            - elastic_energy(unfloored, sp->rho0, scale, sp->tension));
+        }
     }
     const double *transport = v;
     double *xs = NULL;
@@ -961,7 +1078,13 @@ double or_step(const StepParams *sp, long n, double *x, double *v, double *rho, 
     }
     for (long i = 0; i < n; ++i) {
         if (!fluid[i]) continue;
-        for (int c = 0; c < dim; ++c) x[i * dim + c] += transport[i * dim + c] * dt;
+        double gx = 0.0;
+        for (int c = 0; c < dim; ++c) {
+            double start = x[i * dim + c];
+            x[i * dim + c] += transport[i * dim + c] * dt;
+            gx += sp->g[c] * (x[i * dim + c] - start);
+        }
+        if (E) E[10] -= m[i] * gx;
     }
     if (sp->shifting) {
         Sys s0 = {dim, sp->kind, sp->period, start, h, fluid, m, off, nbr};
@@ -981,19 +1104,47 @@ double or_step(const StepParams *sp, long n, double *x, double *v, double *rho, 
         or_shift(&s0, n, rho, v, grad, plain, div, rg, size, sp->shiftThreshold, sp->lopsidedness, shift, drho, dvel);
         for (long i = 0; i < n; ++i) {
             if (!fluid[i]) continue;
+            double k0 = 0.0, k1 = 0.0, gs = 0.0, rho0i = rho[i];
             for (int c = 0; c < dim; ++c) {
+                k0 += v[i * dim + c] * v[i * dim + c];
                 x[i * dim + c] += shift[i * dim + c];
                 v[i * dim + c] += dvel[i * dim + c];
+                k1 += v[i * dim + c] * v[i * dim + c];
+                gs += sp->g[c] * shift[i * dim + c];
             }
             rho[i] += drho[i];
+            if (E) E[12] += m[i] * (0.5 * (k1 - k0) + elastic_energy(rho[i], sp->rho0, scale, sp->tension)
+                                    - elastic_energy(rho0i, sp->rho0, scale, sp->tension) - gs);
         }
         free(grad); free(div);
     }
     for (long i = 0; i < n; ++i)
         if (fluid[i] && sp->period > 0.0) x[i * dim + 1] -= sp->period * floor(x[i * dim + 1] / sp->period);
+    double *before = NULL;
+    if (E && sp->boundaryKind) {
+        before = (double *)malloc(sizeof(double) * (size_t)n * dim * 2);
+        memcpy(before, x, sizeof(double) * (size_t)n * dim);
+        memcpy(before + (size_t)n * dim, v, sizeof(double) * (size_t)n * dim);
+    }
     if (sp->boundaryKind == 1) or_enforce_container(n, dim, x, v, fluid, sp->lower, sp->upper, sp->openTop);
     else if (sp->boundaryKind == 2) or_enforce_bed(n, dim, x, v, fluid, &sp->bed);
     else if (sp->boundaryKind == 3) or_enforce_heightfield(n, x, v, fluid, &sp->field);
+    if (before) {
+        /* the enforcement's change of kinetic and potential energy (clampEnergy) */
+        const double *x0 = before, *v0 = before + (size_t)n * dim;
+        for (long i = 0; i < n; ++i) {
+            if (!fluid[i]) continue;
+            double dk = 0.0, gx = 0.0;
+            for (int c = 0; c < dim; ++c) {
+                long k = i * dim + c;
+                dk += v[k] * v[k] - v0[k] * v0[k];
+                gx += sp->g[c] * (x[k] - x0[k]);
+            }
+            E[11] += m[i] * (0.5 * dk - gx);
+        }
+        free(before);
+    }
+    free(accParts); free(rateParts);
     free(off); free(nbr); free(tmp); free(G); free(L); free(gr); free(xs); free(alphas); free(deltas);
     free(start); free(shift); free(drho);
     return dt;

@@ -591,6 +591,94 @@ def makeShifting():
     np.savez_compressed(os.path.join(HERE, 'shifting.npz'), **out)
 
 
+def solitaryChannel(**options):
+    """tests/testSphEnergy.py:27-52: a solitary wave of H/d = 0.3 in a 12 m channel at 8 particles per
+    depth on the deltaSph scheme, its options replaced by `options`; returns the solver, the particles
+    and the bed's record."""
+    from pysurf import constants, waveTheory
+    from pysurf.bathymetry import Bathymetry
+    from pysurf.sphBoundaries import BedBoundary
+    from pysurf.sphParticles import ParticleSystem
+    from pysurf.sphSolver import SimulationConfig, WcsphSolver
+    from pysurf.waveMakers import solitaryWaveFluid
+    depth, height, spacing = 1.0, 0.3, 1.0 / 8.0
+    crestX = waveTheory.solitaryWaveHalfLength(height, depth, 0.01)
+    channel = Bathymetry([0.0, 12.0], [0.0, 0.0], stillWaterLevel=depth)
+    boundary = BedBoundary(channel, spacing, nLayers=6, wallTop=1.9, endWallTop=1.9)
+    fluid, velocities = solitaryWaveFluid(channel, height, crestX, spacing)
+    particles = ParticleSystem.assemble(fluid, boundary.positions(), spacing, constants.freshwaterDensity, velocities)
+    scheme = dict(kernelType='wendlandC2', smoothingLengthRatio=3.0, densityFilterInterval=0,
+                  densityDiffusion='hydrostatic', xsphEpsilon=0.0, wallPressure='extrapolated',
+                  continuityCorrection=True, densityFloor=0.9, viscosityLimiter=True, alphaViscosity=0.01)
+    scheme.update(options)
+    config = SimulationConfig(domainMin=np.array([-1.0, -1.0]), domainMax=np.array([13.0, 1.9]),
+                              particleSpacing=spacing, maxTimeStep=1.0, backend='numpy',
+                              speedOfSound=10.0 * waveTheory.solitaryWaveSpeed(height, depth),
+                              initialSurface=lambda x: depth + waveTheory.solitaryWaveProfile(x, height, depth, crestX),
+                              **scheme)
+    solver = WcsphSolver(config, boundary=boundary)
+    solver.initialize(particles)
+    clearance = 0.25 * spacing
+    record = dict(kind=2, bedX=channel.x, bedZ=channel.z,
+                  params=[clearance, 0.0, 0.0, 1.0, float(boundary.wallX), 0.0, channel.endX - clearance])
+    return solver, particles, record
+
+
+def makeEnergy():
+    """The energy budget (src/pysurf/sphEnergy.py; its terms in src/pysurf/sphSolver.py:1650-1852 and
+    1909-1936): the elastic energy and its slope on a table of densities, and the array solver's
+    budget over runs that reach every term the device keeps."""
+    from pysurf.sphEnergy import elasticEnergy, elasticSlope, energyTerms
+    out = {'terms': np.array(energyTerms)}
+    densities = np.array([985.0, 999.0, 999.999, 1000.0, 1000.0 + 1e-8, 1000.2, 1003.0, 1030.0, 1100.0])
+    out['elastic/densities'] = densities
+    for tension in (False, True):
+        out[f'elastic/energy_{int(tension)}'] = elasticEnergy(densities, rho0, c0, tension)
+    before = np.array([1001.0, 1002.0, 1002.0, 999.0, 990.0, 1000.0])
+    after = np.array([1003.0, 1002.0 + 1e-9, 1002.0, 998.0, 1010.0, 1000.0 + 1e-5])
+    out['elastic/before'], out['elastic/after'] = before, after
+    for tension in (False, True):
+        out[f'elastic/slope_{int(tension)}'] = elasticSlope(before, after, rho0, c0, tension)
+    out['elastic/rho0'], out['elastic/c0'] = np.array(rho0), np.array(c0)
+    closureForms = {'published': dict(densityDiffusion='antuono', turbulenceClosure='deltaLes', alphaViscosity=0.0,
+                                      viscosityLimiter=False),
+                    'hybrid': dict(densityDiffusion='antuono', turbulenceClosure='deltaLes')}
+
+    def tracked(tag, solver, particles, steps, record):
+        solver.trackEnergy()
+        state = solver.currentState
+        out[f'{tag}/startEnergy'] = np.array([state.kineticEnergy, state.potentialEnergy, solver.elasticEnergy])
+        recordRun(out, tag, solver, particles, steps, record)
+        state = solver.currentState
+        out[f'{tag}/endEnergy'] = np.array([state.kineticEnergy, state.potentialEnergy, solver.elasticEnergy])
+        budget = solver.energyBudget
+        out[f'{tag}/budget'] = np.array([budget[name] for name in energyTerms])
+        out[f'{tag}/closure'] = np.array(int(solver.config.turbulenceClosure == 'deltaLes'))
+        out[f'{tag}/shifting'] = np.array([int(solver.config.particleShifting), solver.config.shiftingMach,
+                                           solver.config.particleSpacing])
+
+    for tag, options in [('channel', {}), ('uncorrected', dict(continuityCorrection=False)),
+                         ('published', closureForms['published']), ('hybrid', closureForms['hybrid'])]:
+        solver, particles, record = solitaryChannel(**options)
+        tracked(tag, solver, particles, 20 if tag == 'uncorrected' else 40, record)
+    # the Shepard filter, XSPH and viscosity against the walls; then shifting
+    solver, particles, boundary = sloshing(boundaryViscosityFactor=0.5)
+    tracked('filtered', solver, particles, 40, containerRecord(boundary))
+    solver, particles, boundary = sloshing(particleShifting=True, densityDiffusion='hydrostatic', **deltaContinuity)
+    tracked('shifted', solver, particles, 30, containerRecord(boundary))
+    # the container's clamp (a corner of the fluid thrown at the walls) and the density floor under
+    # tension (the surface's top row below it)
+    solver, particles, boundary = sloshing(negativePressure=True, densityDiffusion='hydrostatic', **deltaContinuity)
+    fluid = particles.isFluid
+    corner = fluid & (particles.positions[:, 0] < 0.012) & (particles.positions[:, 1] < 0.012)
+    particles.positions[corner] -= 0.003
+    particles.velocities[corner] = [-0.8, -0.8]
+    top = fluid & (particles.positions[:, 1] > particles.positions[fluid, 1].max() - 0.003)
+    particles.densities[top] = 0.88 * particles.densities[top]
+    tracked('clamped', solver, particles, 30, containerRecord(boundary))
+    np.savez_compressed(os.path.join(HERE, 'energy.npz'), **out)
+
+
 def main():
     root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('PYSURF_REFERENCE', '')
     if not root or not os.path.isdir(root):
@@ -598,7 +686,7 @@ def main():
     loadReference(root)
     makers = {'cellkeys': makeCellKeys, 'clouds': makeClouds, 'enforce': makeEnforcement, 'split': makeSplit,
               'beach': makeBeach, 'runs': makeRuns, 'breaking': makeBreaking, 'closure': makeClosure,
-              'shifting': makeShifting}
+              'shifting': makeShifting, 'energy': makeEnergy}
     for name in (sys.argv[2:] or list(makers)):
         makers[name]()
     for name in sorted(os.listdir(HERE)):

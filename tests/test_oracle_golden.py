@@ -114,7 +114,7 @@ def test_split_matches_the_reference(tag):
     assert state['masses'].sum() == pytest.approx(s['masses'].sum(), rel=1e-15)
 
 
-def stepperFor(r):
+def stepperFor(r, **options):
     (dim, kind, h, rho0, c0, alpha, bf, xsph, floor, mode, delta, wall, tension, corrected, limited, cfl, maxdt,
      interval, period) = r['config']
     modes = ['none', 'molteni', 'hydrostatic', 'antuono']
@@ -127,7 +127,7 @@ def stepperFor(r):
                                             bool(offshore), wallX, piston, endLimit))
     return oracle.Stepper(int(dim), 'wendlandC2' if int(kind) == 1 else 'cubicSpline', h, rho0, c0, alpha,
                           r['gravity'], bf, xsph, floor, modes[int(mode)], delta, bool(wall), bool(tension),
-                          bool(corrected), bool(limited), cfl, maxdt, period, int(interval), boundary)
+                          bool(corrected), bool(limited), cfl, maxdt, period, int(interval), boundary, **options)
 
 
 @pytest.mark.parametrize('tag', goldenTags('runs.npz'))
