@@ -96,6 +96,19 @@ int sph_set_shifting(SphSystem *sys, int enabled, double mach, double spacing, d
  * the free surface. */
 int sph_shifting_displacement(SphSystem *sys, const double *densities, double time_step, const double *velocities,
                               double *shifts, double *density_changes, double *velocity_changes);
+/* PairSums.setEnergyBudget (src/pysurf/sphGpu.py:1780-1792): whether the device steps keep the energy
+ * budget (src/pysurf/sphEnergy.py): each fluid particle's running total of every term from the last
+ * sph_push, 120 bytes a particle more while it is on. */
+int sph_set_energy_budget(SphSystem *sys, int enabled);
+/* PairSums.energySums (src/pysurf/sphGpu.py:1805-1825): each term's energy [J] over the device steps
+ * since sph_push, summed over the particles in caller order, into sums[14], in the order pressureFluid,
+ * viscosityFluid, pressureWall, viscosityWall, gravityWork, continuityFluid, continuityWall,
+ * correction, diffusion, floor, drift, clamp, shifting, filter.  SPH_ERR_STATE while the budget is off. */
+int sph_energy_sums(SphSystem *sys, double *sums);
+/* The fluid's kinetic, potential (-m g . x) and elastic energy [J] of the device state into
+ * energies[3] (src/pysurf/sphParticles.py:236-255, src/pysurf/sphSolver.py:2156-2161): the budget's
+ * terms sum to the change of their total, and a split's change of it is the refinement term. */
+int sph_fluid_energy(SphSystem *sys, double *energies);
 /* PairSums.closureCoefficients (src/pysurf/sphGpu.py:1841-1853): alpha_i and delta_i, caller order. */
 int sph_closure_coefficients(SphSystem *sys, const double *velocities, const double *densities, double *alphas,
                              double *deltas);

@@ -74,6 +74,9 @@ SIGNATURES = {
     'sph_set_closure': [_h, _i, _d, _d, _d],
     'sph_set_shifting': [_h, _i, _d, _d, _d, _i],
     'sph_shifting_displacement': [_h, _pd, _d, _pd, _pd, _pd, _pd],
+    'sph_set_energy_budget': [_h, _i],
+    'sph_energy_sums': [_h, _pd],
+    'sph_fluid_energy': [_h, _pd],
     'sph_closure_coefficients': [_h, _pd, _pd, _pd, _pd],
     'sph_surface_tops': [_h, _d, _d, _i64, _pd],
     'sph_split_crest_zone': [_h, _d, _d, _d, _i64, _i64, _d, _d, _d, _d, _pi64],

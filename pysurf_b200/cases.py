@@ -59,6 +59,7 @@ class Case:
     particleShifting: bool = False    # Lind et al.'s shifting, its size CFL Ma (2h)^2 or 2 h |v| dt (local)
     shiftingMach: float = 0.1
     shiftingLocal: bool = False
+    trackEnergy: bool = False         # the device steps keep the energy budget (src/pysurf/sphEnergy.py)
     kinematicViscosity: float = 1.0034e-6     # src/pysurf/constants.py:35, the closure's water term
     info: dict = field(default_factory=dict)
 
@@ -414,6 +415,7 @@ def pairSumsFor(case: Case, cellsPerSupport: int | None = None, device: int = 0)
     sums.setClosure(case.turbulenceClosure == 'deltaLes', case.soundSpeed, case.referenceDensity,
                     case.kinematicViscosity)
     sums.setShifting(case.particleShifting, case.shiftingMach, case.spacing, case.soundSpeed, case.shiftingLocal)
+    sums.setEnergyBudget(case.trackEnergy)
     sums.setPhysics(case.referenceDensity, case.soundSpeed, case.alpha, case.boundaryViscosityFactor, case.gravity,
                     case.xsphEpsilon, case.densityFloor)
     return sums

@@ -92,4 +92,24 @@ __device__ __forceinline__ void enforceOne(const Enforcement &E, int dim, double
     }
 }
 
+// enforceOne on fluid slot i; with the energy budget on, the enforcement's change of kinetic and
+// potential energy, m ((|v'|^2 - |v|^2) / 2 - g . (x' - x)), goes to the clamp's column
+// (src/pysurf/sphGpu.py:1189-1230).
+__device__ __forceinline__ void enforceTracked(const Params &P, const Frame &F, const Enforcement &E, int dim, int i,
+                                               double *x, double *v)
+{
+    if (!P.budget) {
+        enforceOne(E, dim, x, v);
+        return;
+    }
+    const double x0[3] = {x[0], x[1], x[2]}, v0[3] = {v[0], v[1], v[2]};
+    enforceOne(E, dim, x, v);
+    double kinetic = 0.0, lift = 0.0;
+    for (int a = 0; a < dim; ++a) {
+        kinetic += v[a] * v[a] - v0[a] * v0[a];
+        lift += P.gravity64[a] * (x[a] - x0[a]);
+    }
+    addEnergy(P, F, i, kClamp, F.m[i] * (0.5 * kinetic - lift));
+}
+
 }  // namespace sph

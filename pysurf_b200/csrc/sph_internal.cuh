@@ -95,6 +95,10 @@ struct Params {
     // 4 ((k / 4) listStride + i) + k % 4; listCap 0: no table, the sweeps walk the cells
     int listCap;
     int listStride;
+    // energy budget (src/pysurf/sphEnergy.py): each particle's running total of each term, by caller
+    // index, column t at t * energyStride; the momentum sweep's parts of a at q * energyStride + slot
+    int budget;
+    int energyStride;
 };
 
 // The float32 frame and the float64 master state, current buffers.
@@ -114,6 +118,8 @@ struct Frame {
     // shifting: grad C (w unused), grad C0 (w: div r, -1 where the support is lopsided, 1e6 on the
     // boundary), grad rho; the shift (w: the density change) and the velocity change
     float4 *shiftGrad, *shiftPlain, *shiftRhoGrad, *shift, *shiftDv;
+    double *energy;         // energy budget: kEnergyTerms columns, by caller index
+    float4 *parts;          // energy budget: pressure and viscosity of a from fluid and from boundary neighbours
     int *nbr;               // neighbour table (chunks of four), top bit: a pair across the periodic seam
     int *ncount;            // each slot's neighbour count (may exceed the table's capacity)
     // master (current buffers)
@@ -221,6 +227,39 @@ __device__ __forceinline__ double taitPressure(const Params &P, double rho, bool
     double p = P.stiffness * (sq * sq * sq * ratio - 1.0);
     if (!P.tension || !fluid) p = p > 0.0 ? p : 0.0;
     return p;
+}
+
+// The energy budget's terms, the columns of F.energy (src/pysurf/sphEnergy.py:92-98, deviceTerms).
+enum EnergyTerm {
+    kPressureFluid, kViscosityFluid, kPressureWall, kViscosityWall, kGravityWork, kContinuityFluid,
+    kContinuityWall, kCorrection, kDiffusion, kFloor, kDrift, kClamp, kShifting, kFilter, kEnergyTerms
+};
+
+// e(rho), the Tait equation of state's elastic energy per unit mass (src/pysurf/sphEnergy.py:100-139):
+// (c0^2 / 7) x^2 (21 + 35 x + 35 x^2 + 21 x^3 + 7 x^4 + x^5) / (6 (1 + x)), x = rho / rho0 - 1, so no
+// digits cancel near rho0; zero below rho0 unless the fluid carries tension.
+__device__ __forceinline__ double elasticEnergy(const Params &P, double rho)
+{
+    const double x = rho / P.rho0 - 1.0;
+    if (!P.tension && x < 0.0) return 0.0;
+    const double poly = 21.0 + x * (35.0 + x * (35.0 + x * (21.0 + x * (7.0 + x))));
+    return (P.stiffness / P.rho0) * x * x * poly / (6.0 * (1.0 + x));
+}
+
+// The secant slope (e(after) - e(before)) / (after - before), or p / rho^2 at the midpoint for a
+// change under 1e-10 rho0, where the two energies would lose their digits (src/pysurf/sphEnergy.py:141-160).
+__device__ __forceinline__ double elasticSlope(const Params &P, double before, double after)
+{
+    const double change = after - before;
+    if (fabs(change) > 1e-10 * P.rho0) return (elasticEnergy(P, after) - elasticEnergy(P, before)) / change;
+    const double middle = 0.5 * (before + after);
+    return taitPressure(P, middle, true) / (middle * middle);
+}
+
+// Adds to a fluid slot's running total of one term of the budget.
+__device__ __forceinline__ void addEnergy(const Params &P, const Frame &F, int i, int term, double value)
+{
+    F.energy[(size_t)term * P.energyStride + F.orig[i]] += value;
 }
 
 // Cell coordinate of a float64 coordinate along an axis, clamped onto the grid.  Clamping is

@@ -257,14 +257,57 @@ __global__ void refreshDensityKernel(int n, const double *rho, float *out)
 // Pointwise
 // ------------------------------------------------------------------------------------------
 
-__global__ void enforceKernel(int n, int dim, MasterView M, Enforcement E)
+__global__ void enforceKernel(Params P, Frame F, Enforcement E)
 {
     int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n || !M.fluid[i]) return;
+    if (i >= P.n || !F.fluid[i]) return;
+    const int dim = P.dim;
     double x[3] = {0, 0, 0}, v[3] = {0, 0, 0};
-    for (int a = 0; a < dim; ++a) { x[a] = M.x[a][i]; v[a] = M.v[a][i]; }
-    enforceOne(E, dim, x, v);
-    for (int a = 0; a < dim; ++a) { M.x[a][i] = x[a]; M.v[a][i] = v[a]; }
+    for (int a = 0; a < dim; ++a) { x[a] = F.x[a][i]; v[a] = F.v[a][i]; }
+    enforceTracked(P, F, E, dim, i, x, v);
+    for (int a = 0; a < dim; ++a) { F.x[a][i] = x[a]; F.v[a][i] = v[a]; }
+}
+
+// Column sums in a fixed order: block c sums column c (its rows `stride` doubles apart from the
+// last column's) over rows 0 .. n - 1, each thread a strided share, then a tree in shared memory.
+constexpr int kColumnSumThreads = 1024;
+__global__ void __launch_bounds__(kColumnSumThreads) columnSumKernel(const double *columns, long long stride, int n,
+                                                                     double *out)
+{
+    __shared__ double partial[kColumnSumThreads];
+    const double *column = columns + (size_t)blockIdx.x * stride;
+    double sum = 0.0;
+    for (int k = threadIdx.x; k < n; k += kColumnSumThreads) sum += column[k];
+    partial[threadIdx.x] = sum;
+    __syncthreads();
+    for (int width = kColumnSumThreads / 2; width > 0; width >>= 1) {
+        if (threadIdx.x < width) partial[threadIdx.x] += partial[threadIdx.x + width];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[blockIdx.x] = partial[0];
+}
+
+// Each slot's kinetic m |v|^2 / 2, potential -m g . x and elastic m e(rho) energy (zero on the
+// boundary) into three columns, `stride` doubles apart.
+__global__ void fluidEnergyKernel(Params P, Frame F, double *columns, long long stride)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= P.n) return;
+    double kinetic = 0.0, potential = 0.0, elastic = 0.0;
+    if (F.fluid[i]) {
+        const double m = F.m[i];
+        double v2 = 0.0, gx = 0.0;
+        for (int a = 0; a < P.dim; ++a) {
+            v2 += F.v[a][i] * F.v[a][i];
+            gx += P.gravity64[a] * F.x[a][i];
+        }
+        kinetic = 0.5 * m * v2;
+        potential = -m * gx;
+        elastic = m * elasticEnergy(P, F.rho[i]);
+    }
+    columns[i] = kinetic;
+    columns[stride + i] = potential;
+    columns[2 * stride + i] = elastic;
 }
 
 // The step's end: the clock advances, and the next step runs while t < untilTime and the step
@@ -507,10 +550,22 @@ void launchLoadMaster(int n, int dim, const double *x, const double *v, const do
 
 void launchStepEnd(Control *ctl, cudaStream_t st) { stepEndKernel<<<1, 1, 0, st>>>(ctl); }
 
-void launchEnforce(int n, int dim, const MasterView &M, const Enforcement &E, cudaStream_t st)
+void launchEnforce(const Params &P, const Frame &F, const Enforcement &E, cudaStream_t st)
 {
-    if (n == 0 || E.kind == 0) return;
-    enforceKernel<<<blocksFor(n, 256), 256, 0, st>>>(n, dim, M, E);
+    if (P.n == 0 || E.kind == 0) return;
+    enforceKernel<<<blocksFor(P.n, 256), 256, 0, st>>>(P, F, E);
+}
+
+void launchColumnSums(const double *columns, long long stride, int n, int count, double *out, cudaStream_t st)
+{
+    if (count <= 0) return;
+    columnSumKernel<<<count, kColumnSumThreads, 0, st>>>(columns, stride, n, out);
+}
+
+void launchFluidEnergy(const Params &P, const Frame &F, double *columns, long long stride, cudaStream_t st)
+{
+    if (P.n == 0) return;
+    fluidEnergyKernel<<<blocksFor(P.n, 256), 256, 0, st>>>(P, F, columns, stride);
 }
 
 void launchRefreshDensity(int n, const double *rho, float *out, cudaStream_t st)

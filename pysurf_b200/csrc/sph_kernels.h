@@ -68,7 +68,11 @@ void launchLoadFields(const Params &P, int n, const int *orig, const double *v, 
 void launchLoadMaster(int n, int dim, const double *x, const double *v, const double *rho, const double *m,
                       const uint8_t *fluid, const double *h, double hDefault, const MasterView &M, cudaStream_t st);
 void launchStepEnd(Control *ctl, cudaStream_t st);
-void launchEnforce(int n, int dim, const MasterView &M, const Enforcement &E, cudaStream_t st);
+void launchEnforce(const Params &P, const Frame &F, const Enforcement &E, cudaStream_t st);
+// Sums `count` columns of n rows, `stride` doubles apart, each in a fixed order, into out[0 .. count).
+void launchColumnSums(const double *columns, long long stride, int n, int count, double *out, cudaStream_t st);
+// Each slot's kinetic, potential and elastic energy (zero on the boundary) into three columns.
+void launchFluidEnergy(const Params &P, const Frame &F, double *columns, long long stride, cudaStream_t st);
 void launchRefreshDensity(int n, const double *rho, float *out, cudaStream_t st);
 void launchScatterDouble(int n, int dim, const int *orig, const double *const *columns, double *out, cudaStream_t st);
 void launchScatterFloat4(int n, int dim, const int *orig, const float4 *values, double *out, cudaStream_t st);

@@ -196,6 +196,8 @@ __global__ void applyShepardKernel(Params P, Frame F, const Control *ctl)
     if (i >= P.n || !F.fluid[i]) return;
     float filtered = F.scalar[i];
     double rho = (double)filtered;
+    // the filter's change of elastic energy (src/pysurf/sphGpu.py:1043-1056)
+    if (P.budget) addEnergy(P, F, i, kFilter, F.m[i] * (elasticEnergy(P, rho) - elasticEnergy(P, F.rho[i])));
     F.rho[i] = rho;
     storeDensity<D>(F, i, massOf<D>(F, i), rho, P.devReference, (float)taitPressure(P, rho, true));
 }
@@ -362,7 +364,9 @@ gradientKernel(Params P, Frame F, const Control *ctl, int wantG, int wantL, int 
 // Sweep C: accelerations, fluid maxima, time step
 // ------------------------------------------------------------------------------------------
 
-template <int D, int K>
+// BUDGET: the sum split for the energy budget too, into the pressure and the viscosity of fluid
+// and of boundary neighbours (src/pysurf/sphGpu.py:400-414).
+template <int D, int K, bool BUDGET>
 struct MomentumVisit {
     static constexpr bool kSkipCoincident = true;
     static constexpr bool kKinetic = true;
@@ -372,6 +376,7 @@ struct MomentumVisit {
     float alphaI;                               // closure: this particle's eddy alpha
     float Gi[3][3];
     float total[3];
+    float parts[BUDGET ? 4 : 1][3];
     __device__ bool accept(bool) const { return true; }
     __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int, const float4 &B,
                                const float4 &Kj)
@@ -423,9 +428,21 @@ struct MomentumVisit {
                        / (r * r * rhoI * densityIn<D>(Kj));
         }
         const float ratioJ = D == 2 ? Kj.w : __ldg(&F.aux[j].x);
-        float coefficient = -(own + ratioJ + viscosity) * massIn<D>(B);
+        // explicit roundings on the sum's path, so the budget's extra uses of its terms cannot
+        // change how the compiler fuses them: the tracked step is the plain step, bit for bit
+        const float pressureTerm = __fadd_rn(own, ratioJ);
+        float coefficient = -__fadd_rn(pressureTerm, viscosity) * massIn<D>(B);
         float f = coefficient * kernelGradient<K>(q, k);
-        for (int a = 0; a < D; ++a) total[a] += f * d[a];
+        for (int a = 0; a < D; ++a) total[a] = __fmaf_rn(f, d[a], total[a]);
+        if constexpr (BUDGET) {
+            const float grad = massIn<D>(B) * kernelGradient<K>(q, k);
+            const float fp = -pressureTerm * grad, fv = -viscosity * grad;
+            if (fluidJ) {
+                for (int a = 0; a < D; ++a) { parts[0][a] += fp * d[a]; parts[1][a] += fv * d[a]; }
+            } else {
+                for (int a = 0; a < D; ++a) { parts[2][a] += fp * d[a]; parts[3][a] += fv * d[a]; }
+            }
+        }
     }
 };
 
@@ -472,8 +489,8 @@ __device__ __forceinline__ void foldMaxima(Control *ctl, double speed, double ac
 
 // maxima: fold the fluid maxima into ctl and take the time step (the device steps); 0 for the
 // host-step sums.
-template <int D, int K, int T>
-__global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>())
+template <int D, int K, int T, bool BUDGET>
+__global__ void __launch_bounds__(kBlock, BUDGET ? 4 : sweepMinBlocks<D>())
 momentumKernel(Params P, Frame F, Control *ctl, int maxima)
 {
     if (ctl && !ctl->active) return;
@@ -485,7 +502,7 @@ momentumKernel(Params P, Frame F, Control *ctl, int maxima)
         if (hs <= 0.0f) {
             if (G.t == 0) F.acc[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         } else {
-            MomentumVisit<D, K> visit{P, F, Smoothing<K, D>(P)};
+            MomentumVisit<D, K, BUDGET> visit{P, F, Smoothing<K, D>(P)};
             velocityOf<D>(F, i, visit.vi);
             visit.rhoI = densityOf<D>(F, i);
             visit.own = pressureRatioOf<D>(F, i);
@@ -493,8 +510,18 @@ momentumKernel(Params P, Frame F, Control *ctl, int maxima)
             visit.alphaI = P.closure ? F.eddy[i].x : 0.0f;
             if (P.limited) loadMatrix<D>(F.G0, F.G1, F.G2, i, visit.Gi);
             visit.total[0] = visit.total[1] = visit.total[2] = 0.0f;
+            if constexpr (BUDGET)
+                for (int q = 0; q < 4; ++q) visit.parts[q][0] = visit.parts[q][1] = visit.parts[q][2] = 0.0f;
             forEachNeighbour<D, T>(P, F, i, G.t, hs, visit);
             for (int a = 0; a < D; ++a) visit.total[a] = groupSum<T>(visit.total[a], G.mask);
+            if constexpr (BUDGET) {
+                for (int q = 0; q < 4; ++q) {
+                    for (int a = 0; a < D; ++a) visit.parts[q][a] = groupSum<T>(visit.parts[q][a], G.mask);
+                    if (G.t == 0)
+                        F.parts[(size_t)q * P.energyStride + i] =
+                            make_float4(visit.parts[q][0], visit.parts[q][1], D == 3 ? visit.parts[q][2] : 0.0f, 0.0f);
+                }
+            }
             if (G.t == 0) {
                 float a[3] = {visit.total[0] + P.g[0], visit.total[1] + P.g[1],
                               D == 3 ? visit.total[2] + P.g[2] : 0.0f};
@@ -546,11 +573,27 @@ __global__ void kickKernel(Params P, Frame F, Control *ctl)
     if (i >= P.n || !F.fluid[i]) return;
     double dt = ctl->dt;
     float4 a = F.acc[i];
-    double v[3] = {0.0, 0.0, 0.0};
+    double v[3] = {0.0, 0.0, 0.0}, mean[3] = {0.0, 0.0, 0.0};
     float av[3] = {a.x, a.y, a.z};
     for (int c = 0; c < D; ++c) {
-        v[c] = F.v[c][i] + (double)av[c] * dt;
+        const double start = F.v[c][i];
+        v[c] = start + (double)av[c] * dt;
         F.v[c][i] = v[c];
+        mean[c] = 0.5 * (start + v[c]);
+    }
+    if (P.budget) {
+        // each part of a, and gravity, does the work m a . (v + v') / 2 dt (src/pysurf/sphGpu.py:1084-1109)
+        const double m = F.m[i];
+        for (int q = 0; q < 4; ++q) {
+            const float4 part = F.parts[(size_t)q * P.energyStride + i];
+            const float pv[3] = {part.x, part.y, part.z};
+            double work = 0.0;
+            for (int c = 0; c < D; ++c) work += (double)pv[c] * mean[c];
+            addEnergy(P, F, i, kPressureFluid + q, m * work * dt);
+        }
+        double work = 0.0;
+        for (int c = 0; c < D; ++c) work += (double)P.g[c] * mean[c];
+        addEnergy(P, F, i, kGravityWork, m * work * dt);
     }
     float4 k = F.kin[i];
     k.x = (float)v[0]; k.y = (float)v[1];
@@ -563,13 +606,17 @@ template <int D>
 __device__ __forceinline__ void driftAndEnforce(const Params &P, const Frame &F, const Enforcement &E, int i, double dt,
                                                 const double *transport, Control *ctl)
 {
-    double x[3] = {0.0, 0.0, 0.0}, v[3] = {0.0, 0.0, 0.0};
+    double x[3] = {0.0, 0.0, 0.0}, v[3] = {0.0, 0.0, 0.0}, lift = 0.0;
     for (int a = 0; a < D; ++a) {
         v[a] = F.v[a][i];
-        x[a] = F.x[a][i] + (transport ? transport[a] : v[a]) * dt;
+        const double start = F.x[a][i];
+        x[a] = start + (transport ? transport[a] : v[a]) * dt;
+        lift += P.gravity64[a] * (x[a] - start);
     }
+    // the drift's change of potential energy, from the displacement as stored (src/pysurf/sphGpu.py:1168-1170)
+    if (P.budget) addEnergy(P, F, i, kDrift, -F.m[i] * lift);
     if (P.period > 0.0) x[1] = x[1] - P.period * floor(x[1] / P.period);
-    enforceOne(E, D, x, v);
+    enforceTracked(P, F, E, D, i, x, v);
     bool finite = true;
     for (int a = 0; a < D; ++a) {
         F.x[a][i] = x[a];
@@ -583,7 +630,10 @@ __device__ __forceinline__ void driftAndEnforce(const Params &P, const Frame &F,
 // Sweep D: continuity with the density update, drift and enforcement
 // ------------------------------------------------------------------------------------------
 
-template <int D, int K>
+// BUDGET: the rate split for the energy budget too: the plain sum over fluid and over boundary
+// neighbours, the corrected sum (the correction's part is its difference) and the diffusion
+// (src/pysurf/sphGpu.py:476-545).
+template <int D, int K, bool BUDGET>
 struct ContinuityVisit {
     static constexpr bool kSkipCoincident = true;
     static constexpr bool kKinetic = true;
@@ -593,6 +643,7 @@ struct ContinuityVisit {
     float vi[3], devI, Li[3][3], gi[3];
     float deltaI;           // closure: this particle's eddy delta
     float total;
+    float plainFluid, plainWall, continuity, diffusive;     // BUDGET
     __device__ bool accept(bool fluidJ) const { return !(boundaryI && !fluidJ); }
     __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int, const float4 &B,
                                const float4 &Kj)
@@ -611,7 +662,19 @@ struct ContinuityVisit {
         } else {
             for (int a = 0; a < D; ++a) dot += (vi[a] - vj[a]) * d[a];
         }
-        total += massIn<D>(B) * dot * grad;
+        // explicit roundings on the sum's path (see the momentum sweep)
+        const float massDot = massIn<D>(B) * dot;
+        total = __fmaf_rn(massDot, grad, total);
+        if constexpr (BUDGET) {
+            float plainDot = dot;
+            if (corrected) {
+                plainDot = 0.0f;
+                for (int a = 0; a < D; ++a) plainDot += (vi[a] - vj[a]) * d[a];
+            }
+            const float plain = massIn<D>(B) * plainDot * grad;
+            continuity = __fmaf_rn(massDot, grad, continuity);
+            if (fluidJ) plainFluid += plain; else plainWall += plain;
+        }
         if (diffuses && fluidJ) {
             const float4 X = auxRow<D>(F, j);
             float devJ = deviationIn<D>(B, X);
@@ -635,14 +698,16 @@ struct ContinuityVisit {
                 factor = both > 0.0f ? 2.0f * P.closureC0 * (2.0f * deltaI * deltaJ / both) : 0.0f;
             }
             const float r2 = r * r;
-            total += factor * h * volumeIn<D>(B, X) * difference * (-grad) * __fdividef(r2, r2 + k.soft);
+            const float head = factor * h * volumeIn<D>(B, X) * difference * (-grad), ratio = __fdividef(r2, r2 + k.soft);
+            total = __fmaf_rn(head, ratio, total);
+            if constexpr (BUDGET) diffusive = __fmaf_rn(head, ratio, diffusive);
         }
     }
 };
 
 // mode 0: the rate only; 1: advance the density; 2: advance, drift and enforce.
-template <int D, int K, int T>
-__global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>())
+template <int D, int K, int T, bool BUDGET>
+__global__ void __launch_bounds__(kBlock, BUDGET ? 4 : sweepMinBlocks<D>())
 continuityKernel(Params P, Frame F, Control *ctl, Enforcement E, int mode)
 {
     if (ctl && !ctl->active) return;
@@ -650,7 +715,7 @@ continuityKernel(Params P, Frame F, Control *ctl, Enforcement E, int mode)
     const int i = G.i;
     if (i >= P.n) return;
     float hs = signedLength<D>(F, i);
-    ContinuityVisit<D, K> visit{P, F, Smoothing<K, D>(P)};
+    ContinuityVisit<D, K, BUDGET> visit{P, F, Smoothing<K, D>(P)};
     visit.boundaryI = hs <= 0.0f;
     visit.diffuses = P.diffusion != 0 && !visit.boundaryI;
     visit.corrected = P.corrected && !visit.boundaryI;
@@ -664,16 +729,35 @@ continuityKernel(Params P, Frame F, Control *ctl, Enforcement E, int mode)
         visit.gi[0] = g.x; visit.gi[1] = g.y; visit.gi[2] = g.z;
     }
     visit.total = 0.0f;
+    visit.plainFluid = visit.plainWall = visit.continuity = visit.diffusive = 0.0f;
     forEachNeighbour<D, T>(P, F, i, G.t, fabsf(hs), visit);
     const float rate = groupSum<T>(visit.total, G.mask);
+    float parts[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+    if constexpr (BUDGET) {
+        const float plainFluid = groupSum<T>(visit.plainFluid, G.mask);
+        const float plainWall = groupSum<T>(visit.plainWall, G.mask);
+        const float continuity = groupSum<T>(visit.continuity, G.mask);
+        parts[0] = plainFluid;
+        parts[1] = plainWall;
+        parts[2] = visit.corrected ? continuity - plainFluid - plainWall : 0.0f;
+        parts[3] = groupSum<T>(visit.diffusive, G.mask);
+    }
     if (G.t != 0) return;
     F.rate[i] = rate;
     if (mode == 0) return;
     double dt = ctl->dt;
-    double rho = F.rho[i] + (double)rate * dt;
+    const double start = F.rho[i];
+    double rho = start + (double)rate * dt;
+    const double unfloored = rho;
     bool fluid = hs > 0.0f;
     if (P.densityFloor > 0.0 && fluid) rho = fmax(rho, P.densityFloor);
     F.rho[i] = rho;
+    if (BUDGET && fluid) {
+        // each part of the rate over the secant slope of e, and the floor's change (src/pysurf/sphGpu.py:1111-1140)
+        const double m = F.m[i], slope = elasticSlope(P, start, unfloored);
+        for (int q = 0; q < 4; ++q) addEnergy(P, F, i, kContinuityFluid + q, m * slope * (double)parts[q] * dt);
+        addEnergy(P, F, i, kFloor, m * (elasticEnergy(P, rho) - elasticEnergy(P, unfloored)));
+    }
     if (!isfinite(rho)) atomicOr(&ctl->error, kErrNonFinite);
     if (mode == 2 && fluid) driftAndEnforce<D>(P, F, E, i, dt, nullptr, ctl);
 }
@@ -937,16 +1021,28 @@ __global__ void shiftDriftKernel(Params P, Frame F, Control *ctl, Enforcement E,
     const float4 s = F.shift[i], dv = F.shiftDv[i];
     const float4 u = F.vec[i];
     const float sh[3] = {s.x, s.y, s.z}, dvel[3] = {dv.x, dv.y, dv.z}, ut[3] = {u.x, u.y, u.z};
-    double x[3] = {0.0, 0.0, 0.0}, v[3] = {0.0, 0.0, 0.0};
+    double x[3] = {0.0, 0.0, 0.0}, v[3] = {0.0, 0.0, 0.0}, lift = 0.0, kinetic = 0.0, shiftLift = 0.0;
     for (int a = 0; a < D; ++a) {
-        const double velocity = useTransport ? (double)ut[a] : F.v[a][i];
-        x[a] = F.x[a][i] + velocity * dt;
+        const double velocity = useTransport ? (double)ut[a] : F.v[a][i], start = F.x[a][i];
+        x[a] = start + velocity * dt;
+        lift += P.gravity64[a] * (x[a] - start);
         x[a] = x[a] + (double)sh[a];
+        shiftLift += P.gravity64[a] * (double)sh[a];
         v[a] = F.v[a][i] + (double)dvel[a];
+        kinetic += v[a] * v[a] - F.v[a][i] * F.v[a][i];
     }
-    F.rho[i] = F.rho[i] + (double)s.w;
+    const double rhoStart = F.rho[i];
+    F.rho[i] = rhoStart + (double)s.w;
+    if (P.budget) {
+        // the drift's change of potential energy, and the shift's of kinetic, elastic and potential
+        // energy (src/pysurf/sphGpu.py:1166-1183)
+        const double m = F.m[i];
+        addEnergy(P, F, i, kDrift, -m * lift);
+        addEnergy(P, F, i, kShifting,
+                  m * (0.5 * kinetic + elasticEnergy(P, F.rho[i]) - elasticEnergy(P, rhoStart) - shiftLift));
+    }
     if (P.period > 0.0) x[1] = x[1] - P.period * floor(x[1] / P.period);
-    enforceOne(E, D, x, v);
+    enforceTracked(P, F, E, D, i, x, v);
     bool finite = isfinite(F.rho[i]);
     for (int a = 0; a < D; ++a) {
         F.x[a][i] = x[a];
@@ -997,9 +1093,16 @@ static void launchT(const LaunchArgs &A, Stage stage)
     case Stage::Gradients:
         gradientKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.wantG, A.wantL, A.wantRho, A.floorDet);
         break;
-    case Stage::Momentum: momentumKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.maxima); break;
+    case Stage::Momentum:
+        if (P.budget && A.maxima) momentumKernel<D, K, T, true><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.maxima);
+        else momentumKernel<D, K, T, false><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.maxima);
+        break;
     case Stage::Kick: kickKernel<D><<<pointwise, kBlock, 0, st>>>(P, F, A.ctl); break;
-    case Stage::Continuity: continuityKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.flag); break;
+    case Stage::Continuity:
+        // the budget's parts matter only where the step advances the density
+        if (P.budget && A.flag != 0) continuityKernel<D, K, T, true><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.flag);
+        else continuityKernel<D, K, T, false><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.flag);
+        break;
     case Stage::Xsph: xsphKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.densities, A.flag); break;
     case Stage::List: launchList<D>(A); break;
     case Stage::Closure: closureKernel<D><<<pointwise, kBlock, 0, st>>>(P, F, A.ctl); break;

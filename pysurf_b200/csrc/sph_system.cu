@@ -110,6 +110,13 @@ struct SphSystem {
     int closure = 0;            // delta-LES-SPH closure, with its sound speed, rho0 and the water's viscosity
     double closureC0 = 1.0, closureRho0 = 1000.0, closureNu = 0.0;
     float2 *eddy = nullptr;
+    // the energy budget (src/pysurf/sphEnergy.py): each particle's running total of each term, by
+    // caller index, and the momentum sweep's parts of a; energyCap rows, made while it is on
+    int budget = 0;
+    double *energy = nullptr;
+    float4 *parts = nullptr;
+    int energyCap = 0;
+    double *dSums = nullptr;    // the column sums' results (kEnergyTerms doubles)
     bool physicsSet = false;
     Enforcement enforcement{};
     double *bedX = nullptr, *bedZ = nullptr, *table = nullptr;
@@ -280,6 +287,32 @@ struct SphSystem {
         CUDA_TRY(cudaMemsetAsync(eddy, 0, sizeof(float2) * cap, stream));
         graphDirty = true;
         framed = false;
+        return reserveBudget(preserve);
+    }
+
+    // The energy budget's arrays for the capacity, while the budget is on; with `preserve` the
+    // running totals of the first n caller indices survive, every other row starts at zero.
+    int reserveBudget(bool preserve)
+    {
+        if (!budget || (energy && energyCap >= capacity)) return SPH_OK;
+        const int cap = std::max(capacity, 1);
+        double *fresh = nullptr;
+        float4 *freshParts = nullptr;
+        TRY(deviceAlloc(&fresh, (size_t)kEnergyTerms * cap));
+        TRY(deviceAlloc(&freshParts, (size_t)4 * cap));
+        CUDA_TRY(cudaMemsetAsync(fresh, 0, sizeof(double) * kEnergyTerms * cap, stream));
+        CUDA_TRY(cudaMemsetAsync(freshParts, 0, sizeof(float4) * 4 * cap, stream));
+        if (preserve && energy && n > 0)
+            CUDA_TRY(cudaMemcpy2DAsync(fresh, sizeof(double) * cap, energy, sizeof(double) * energyCap,
+                                       sizeof(double) * std::min(n, energyCap), kEnergyTerms,
+                                       cudaMemcpyDeviceToDevice, stream));
+        CUDA_TRY(cudaStreamSynchronize(stream));
+        cudaFree(energy);
+        cudaFree(parts);
+        energy = fresh;
+        parts = freshParts;
+        energyCap = cap;
+        graphDirty = true;
         return SPH_OK;
     }
 
@@ -387,6 +420,8 @@ struct SphSystem {
         P.xsphEpsilon = (float)xsphEpsilon;
         P.listCap = listCap;
         P.listStride = capacity;
+        P.budget = budget && energy ? 1 : 0;
+        P.energyStride = energyCap;
         return P;
     }
 
@@ -401,6 +436,7 @@ struct SphSystem {
         F.shiftGrad = shiftGrad; F.shiftPlain = shiftPlain; F.shiftRhoGrad = shiftRhoGrad; F.shift = shiftOut;
         F.shiftDv = shiftDv;
         F.nbr = nbr; F.ncount = ncount;
+        F.energy = energy; F.parts = parts;
         const MasterView &M = master[cur];
         for (int a = 0; a < 3; ++a) { F.x[a] = M.x[a]; F.v[a] = M.v[a]; }
         F.rho = M.rho; F.m = M.m; F.h = M.h; F.fluid = M.fluid; F.orig = M.orig;
@@ -608,6 +644,9 @@ int sph_destroy(SphSystem *sys)
             if (sys->stageEvents[b][k]) cudaEventDestroy(sys->stageEvents[b][k]);
     }
     sys->freeArrays();
+    cudaFree(sys->energy);
+    cudaFree(sys->parts);
+    cudaFree(sys->dSums);
     cudaFree(sys->cellStart);
     cudaFree(sys->sortBuffers.cellCount);
     cudaFree(sys->sortBuffers.partials);
@@ -747,6 +786,49 @@ int sph_set_shifting(SphSystem *sys, int enabled, double mach, double spacing, d
         sys->shiftScale = sound_speed * mach * 4.0 * sys->h;
     }
     sys->graphDirty = true;
+    return SPH_OK;
+}
+
+int sph_set_energy_budget(SphSystem *sys, int enabled)
+{
+    CHECK_SYS(sys);
+    sys->budget = enabled ? 1 : 0;
+    if (enabled) TRY(sys->reserveBudget(true));
+    sys->graphDirty = true;
+    return SPH_OK;
+}
+
+int sph_energy_sums(SphSystem *sys, double *sums)
+{
+    CHECK_SYS(sys);
+    if (!sums) return fail(SPH_ERR_INVALID, "null argument");
+    if (!sys->budget) return fail(SPH_ERR_STATE, "the energy budget is off; see sph_set_energy_budget");
+    for (int t = 0; t < kEnergyTerms; ++t) sums[t] = 0.0;
+    if (sys->n == 0 || !sys->energy) return SPH_OK;
+    if (!sys->dSums) TRY(deviceAlloc(&sys->dSums, kEnergyTerms));
+    double *out = sys->dSums;
+    launchColumnSums(sys->energy, sys->energyCap, sys->n, kEnergyTerms, out, sys->stream);
+    CUDA_TRY(cudaGetLastError());
+    TRY(sys->download(sums, out, sizeof(double) * kEnergyTerms));
+    CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    return SPH_OK;
+}
+
+int sph_fluid_energy(SphSystem *sys, double *energies)
+{
+    CHECK_SYS(sys);
+    if (!energies) return fail(SPH_ERR_INVALID, "null argument");
+    if (!sys->resident) return fail(SPH_ERR_STATE, "no device state: call sph_push first");
+    if (!sys->physicsSet) return fail(SPH_ERR_STATE, "call sph_set_physics first");
+    energies[0] = energies[1] = energies[2] = 0.0;
+    if (sys->n == 0) return SPH_OK;
+    if (!sys->dSums) TRY(deviceAlloc(&sys->dSums, kEnergyTerms));
+    double *columns = sys->stage(SphSystem::kOutSlot), *out = sys->dSums;
+    launchFluidEnergy(sys->params(), sys->frame(), columns, sys->capacity, sys->stream);
+    launchColumnSums(columns, sys->capacity, sys->n, 3, out, sys->stream);
+    CUDA_TRY(cudaGetLastError());
+    TRY(sys->download(energies, out, sizeof(double) * 3));
+    CUDA_TRY(cudaStreamSynchronize(sys->stream));
     return SPH_OK;
 }
 
@@ -1075,6 +1157,9 @@ int sph_push(SphSystem *sys, int64_t n, const double *positions, const double *v
     if (n > 0 && (!velocities || !densities)) return fail(SPH_ERR_INVALID, "null state array");
     TRY(loadState(sys, n, positions, velocities, densities, masses, is_fluid, lengths));
     sys->resident = true;
+    // the energy budget counts from the push (src/pysurf/sphGpu.py:2207-2221)
+    if (sys->budget && sys->energy)
+        CUDA_TRY(cudaMemsetAsync(sys->energy, 0, sizeof(double) * kEnergyTerms * sys->energyCap, sys->stream));
     // the frame follows at the first step; make the cell list now so host-step calls work too
     sys->rebuild();
     TRY(sys->sizeList());
@@ -1230,7 +1315,7 @@ int sph_enforce_boundary(SphSystem *sys)
 {
     CHECK_SYS(sys);
     if (sys->n == 0) return SPH_OK;
-    launchEnforce(sys->n, sys->dim, sys->master[sys->cur], sys->enforcement, sys->stream);
+    launchEnforce(sys->params(), sys->frame(), sys->enforcement, sys->stream);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(sys->stream));
     sys->cellsFresh = false;    // the positions moved; the next step re-sorts anyway
@@ -1747,6 +1832,9 @@ int sph_split(SphSystem *sys, const uint8_t *mask, double reference_density, dou
     long long grown = (long long)n + (long long)count * perMother;
     if (grown > 0x3FFFFFFF) return fail(SPH_ERR_INVALID, "too many particles after the split");
     TRY(sys->reserve((int)grown, true));
+    if (sys->budget && sys->energy)     // the daughters' totals start at zero; the mothers keep theirs
+        CUDA_TRY(cudaMemset2DAsync(sys->energy + n, sizeof(double) * sys->energyCap, 0,
+                                   sizeof(double) * (size_t)(grown - n), kEnergyTerms, sys->stream));
     const MasterView &M = sys->master[sys->cur];
     CUDA_TRY(cudaMemcpyAsync(sys->dStageU8, chosen.data(), n, cudaMemcpyHostToDevice, sys->stream));
     CUDA_TRY(cudaMemcpyAsync(sys->dRank, rank.data(), sizeof(int) * n, cudaMemcpyHostToDevice, sys->stream));

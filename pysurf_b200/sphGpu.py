@@ -11,8 +11,7 @@ What it carries: the cubic spline and the Wendland C2 kernels; the plain and the
 artificial viscosity; the continuity sum plain and corrected; the delta-SPH diffusive term in its
 'molteni', 'hydrostatic' and 'antuono' forms; the extrapolated wall pressure; negative pressure;
 the Shepard filter; XSPH; a periodic y axis; mixed smoothing lengths; container, bed and height
-field enforcement; the delta-LES-SPH closure; particle shifting.  The energy budget is not
-carried yet: enabling it raises NotImplementedError, and its setter accepts it off.
+field enforcement; the delta-LES-SPH closure; particle shifting; the energy budget.
 
 Beyond the reference's surface, ``advance`` runs a whole span of steps on the device with the
 time step taken there (no host round trip per step), ``split`` refines on the device, and
@@ -29,6 +28,9 @@ from pysurf_b200._lib import check, dptr, f64, u8
 
 maxGridCells = 2 ** 25
 diffusionModes = {'none': 0, 'molteni': 1, 'hydrostatic': 2, 'antuono': 3}
+# The energy budget's terms the device steps keep (src/pysurf/sphEnergy.py:88-98, deviceTerms)
+energyTerms = ('pressureFluid', 'viscosityFluid', 'pressureWall', 'viscosityWall', 'gravityWork', 'continuityFluid',
+               'continuityWall', 'correction', 'diffusion', 'floor', 'drift', 'clamp', 'shifting', 'filter')
 taitExponent = 7.0
 
 
@@ -194,12 +196,28 @@ class PairSums:
         self.closureEnabled = bool(enabled)
 
     def setEnergyBudget(self, enabled: bool) -> None:
-        if enabled:
-            raise NotImplementedError('The energy budget is not carried by the B200 backend yet.')
-        self.trackEnergy = False
+        """Whether the device steps keep the energy budget (src/pysurf/sphGpu.py:1780-1792): each fluid
+        particle's running total of every term in `energyTerms`, from `push` to `energySums`."""
+        check(self._lib.sph_set_energy_budget(self._handle, int(bool(enabled))), 'setEnergyBudget')
+        self.trackEnergy = bool(enabled)
 
     def energySums(self) -> np.ndarray:
-        raise ValueError('The energy budget is off; see setEnergyBudget.')
+        """Each term's energy over the device steps since `push` [J] (per unit depth in 2D), summed
+        over the particles, in `energyTerms` order (src/pysurf/sphGpu.py:1805-1825).
+
+        Raises ValueError while the budget is off."""
+        if not self.trackEnergy:
+            raise ValueError('The energy budget is off; see setEnergyBudget.')
+        out = np.zeros(len(energyTerms))
+        check(self._lib.sph_energy_sums(self._handle, dptr(out)), 'energySums')
+        return out
+
+    def fluidEnergy(self) -> np.ndarray:
+        """The device state's fluid kinetic, potential and elastic energy [J] (per unit depth in 2D):
+        the budget's terms sum to the change of their total."""
+        out = np.zeros(3)
+        check(self._lib.sph_fluid_energy(self._handle, dptr(out)), 'fluidEnergy')
+        return out
 
     def setDiffusion(self, mode: str, delta: float, soundSpeed: float, referenceDensity: float, gravity: float) -> None:
         if mode not in diffusionModes:
