@@ -70,16 +70,29 @@ def parseArgs():
                    help='the served requests horizons, U(2, 6) s of simulated time times this')
     p.add_argument('--refine', action='store_true',
                    help='split the crest zone (surface above 0.3 H) into daughters of h/2 before timing')
+    p.add_argument('--options', default='',
+                   help='opt-in parts of the step, comma separated: closure (delta-LES-SPH), shifting, energy '
+                        '(the energy budget)')
     p.add_argument('--no-e2e', action='store_true')
     p.add_argument('--no-cpu', action='store_true')
     return p.parse_args()
 
 
+OPTIONS = ('closure', 'shifting', 'energy')
+
+
 def buildCase(args):
     from pysurf_b200 import cases
-    if args.case == 'ridge':
-        return cases.ridgeWave3D(args.ppd or 24)
-    return cases.solitaryBeach(args.ppd or 64)
+    case = cases.ridgeWave3D(args.ppd or 24) if args.case == 'ridge' else cases.solitaryBeach(args.ppd or 64)
+    options = [o for o in args.options.split(',') if o]
+    unknown = set(options) - set(OPTIONS)
+    if unknown:
+        raise SystemExit(f'unknown --options {sorted(unknown)}; choose from {OPTIONS}')
+    case.turbulenceClosure = 'deltaLes' if 'closure' in options else case.turbulenceClosure
+    case.particleShifting = 'shifting' in options or case.particleShifting
+    case.trackEnergy = 'energy' in options or case.trackEnergy
+    case.info['options'] = options
+    return case
 
 
 def config(case, flush: bool = True) -> dict:
@@ -93,6 +106,9 @@ def config(case, flush: bool = True) -> dict:
         workload = (f'solitary wave H/d 0.5 over a Gaussian ridge (0.6 d, sigma 3 d, axis at 25 degrees) in a '
                     f'40 d x 10 d tank, 3D, {scheme}')
         extent = {'tank_d': info['tank']}
+    if info.get('options'):
+        workload += ', with ' + ' and '.join({'closure': 'the delta-LES-SPH closure', 'shifting': 'particle shifting',
+                                               'energy': 'the energy budget'}[o] for o in info['options'])
     return {'workload': workload, 'particles_per_depth': info['ppd'], 'fluid_particles': case.fluidCount,
             'boundary_particles': int(case.state.nParticles - case.fluidCount), 'boundary_layers': info['layers'],
             'smoothing_length_over_dx': round(case.smoothingLength / case.spacing, 6), **extent,
@@ -125,10 +141,15 @@ def oracleStepper(case):
         enforcement = ('field', oracle.fieldParams(field.z, field.x[0], field.y[0], field.spacingX, field.spacingY,
                                                    clearance, startY + clearance, endY - clearance, True,
                                                    startX + clearance, endX - clearance))
-    return oracle.Stepper(case.dimensions, case.kernelType, case.smoothingLength, case.referenceDensity,
-                          case.soundSpeed, case.alpha, case.gravity, 0.0, 0.0, case.densityFloor,
-                          case.densityDiffusion, case.diffusionDelta, True, False, True, True, case.cflNumber,
-                          case.maxTimeStep, 0.0, 0, enforcement)
+    stepper = oracle.Stepper(case.dimensions, case.kernelType, case.smoothingLength, case.referenceDensity,
+                             case.soundSpeed, case.alpha, case.gravity, 0.0, 0.0, case.densityFloor,
+                             case.densityDiffusion, case.diffusionDelta, True, False, True, True, case.cflNumber,
+                             case.maxTimeStep, 0.0, 0, enforcement, closure=case.turbulenceClosure == 'deltaLes',
+                             viscosity=case.kinematicViscosity, shifting=case.particleShifting,
+                             shiftingMach=case.shiftingMach, spacing=case.spacing, shiftingLocal=case.shiftingLocal)
+    if case.trackEnergy:
+        stepper.trackEnergy()
+    return stepper
 
 
 def sweepConfig(sums, table: bool, threads: int) -> dict:

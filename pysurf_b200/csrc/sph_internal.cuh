@@ -62,6 +62,18 @@ struct Params {
     int nc[3];
     int ncs;                // cells per support: the stencil is +-ncs cells
     int precise;            // separations from point + remainder (1) or the float32 points alone (0)
+    // the fine level, for mixed smoothing lengths: a particle whose h is below fineBelow is sorted
+    // into a second grid of fineWidth-wide cells (ncs to the fine level's longest h, fineMax),
+    // numbered from fineFirst after the coarse grid's; a particle searches each grid only as far as
+    // that grid's particles reach.  levels is 1 when no particle is on the fine level.
+    int levels;
+    double fineOrigin[3];
+    double fineWidth;
+    int fineNc[3];
+    int fineFirst;
+    int cells;              // both grids' cells
+    float fineMax;
+    double fineBelow;
     double period;          // periodic y axis length, 0 for none
     float periodF;
     // physics
@@ -271,6 +283,57 @@ __device__ __forceinline__ int cellCoordinate(double value, double origin, doubl
     if (f < 0.0) return 0;
     if (f > (double)(count - 1)) return count - 1;
     return (int)f;
+}
+
+// A box of cells of one grid around a centre cell, clamped to the grid: rows (y, z) of the
+// x range [x0, x1]; the grid's cells are numbered from `first`, x fastest.
+struct CellBox {
+    int first, nx, ny;
+    int cx, cy, cz;
+    int x0, x1, y0, y1, z0, z1;
+};
+
+// The half-width in cells of a particle's search of a level's grid: the coarse grid's ncs (its
+// cells are 2 hMax / ncs wide, and no pair reaches past 2 hMax), the fine grid's as many cells as
+// hI + fineMax, the farthest a fine neighbour can be, spans.
+__device__ __forceinline__ int searchCells(const Params &P, int level, float hI)
+{
+    if (level == 0) return P.ncs;
+    return (int)ceil(((double)hI + (double)P.fineMax) / P.fineWidth - 1e-9);
+}
+
+// The box of +-n cells of a level's grid (0 coarse, 1 fine) around the cell holding pos; in the
+// particle's own grid the centre is its sorted cell ownCell (y taken from pos when `image`, the
+// search of a periodic image).  single: there is one level, so the own grid is the searched one.
+__device__ __forceinline__ CellBox cellBox(const Params &P, int level, int ownCell, const double pos[3], bool image,
+                                           int dim, int n, bool single = false)
+{
+    CellBox B;
+    const bool fine = level == 1;
+    B.nx = fine ? P.fineNc[0] : P.nc[0];
+    B.ny = fine ? P.fineNc[1] : P.nc[1];
+    const int nz = fine ? P.fineNc[2] : P.nc[2];
+    B.first = fine ? P.fineFirst : 0;
+    const double width = fine ? P.fineWidth : P.cellWidth;
+    const double *origin = fine ? P.fineOrigin : P.origin;
+    if (single || (ownCell >= P.fineFirst) == fine) {
+        const int local = ownCell - B.first;
+        B.cx = local % B.nx;
+        B.cy = (local / B.nx) % B.ny;
+        B.cz = local / (B.nx * B.ny);
+        if (image) B.cy = cellCoordinate(pos[1], origin[1], width, B.ny);
+    } else {
+        B.cx = cellCoordinate(pos[0], origin[0], width, B.nx);
+        B.cy = cellCoordinate(pos[1], origin[1], width, B.ny);
+        B.cz = dim == 3 ? cellCoordinate(pos[2], origin[2], width, nz) : 0;
+    }
+    B.x0 = max(B.cx - n, 0);
+    B.x1 = min(B.cx + n, B.nx - 1);
+    B.y0 = max(B.cy - n, 0);
+    B.y1 = min(B.cy + n, B.ny - 1);
+    B.z0 = dim == 3 ? max(B.cz - n, 0) : 0;
+    B.z1 = dim == 3 ? min(B.cz + n, nz - 1) : 0;
+    return B;
 }
 
 // ------------------------------------------------------------------------------------------

@@ -37,16 +37,21 @@ namespace sph {
 //          function of the state alone
 // A cell holds a handful of slots, so the rank's loop over the cell is short; its cost grows with
 // the square of a cell's count, as the sweeps' candidate tests over that cell already do.
-__global__ void cellCountKernel(Params P, int n, const double *x0, const double *x1, const double *x2, int *slotCell,
-                                int *slotWithin, int *cellCount, const Control *ctl)
+// A slot whose h is below P.fineBelow goes to the fine grid's cells, numbered after the coarse grid's.
+__global__ void cellCountKernel(Params P, int n, const double *x0, const double *x1, const double *x2,
+                                const double *h, int *slotCell, int *slotWithin, int *cellCount, const Control *ctl)
 {
     if (ctl && !ctl->active) return;
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
-    int cx = cellCoordinate(x0[s], P.origin[0], P.cellWidth, P.nc[0]);
-    int cy = cellCoordinate(x1[s], P.origin[1], P.cellWidth, P.nc[1]);
-    int cz = P.dim == 3 ? cellCoordinate(x2[s], P.origin[2], P.cellWidth, P.nc[2]) : 0;
-    int c = (cz * P.nc[1] + cy) * P.nc[0] + cx;
+    const bool fine = P.levels > 1 && h[s] < P.fineBelow;
+    const double width = fine ? P.fineWidth : P.cellWidth;
+    const double *origin = fine ? P.fineOrigin : P.origin;
+    const int *nc = fine ? P.fineNc : P.nc;
+    int cx = cellCoordinate(x0[s], origin[0], width, nc[0]);
+    int cy = cellCoordinate(x1[s], origin[1], width, nc[1]);
+    int cz = P.dim == 3 ? cellCoordinate(x2[s], origin[2], width, nc[2]) : 0;
+    int c = (fine ? P.fineFirst : 0) + (cz * nc[1] + cy) * nc[0] + cx;
     slotCell[s] = c;
     slotWithin[s] = atomicAdd(&cellCount[c], 1);
 }
@@ -404,31 +409,30 @@ __global__ void neighbourRowsKernel(Params P, Frame F, const int64_t *offsets, i
     int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= P.n) return;
     double xi[3] = {F.x[0][i], F.x[1][i], D == 3 ? F.x[2][i] : 0.0};
-    const int nx = P.nc[0], ny = P.nc[1], nz = P.nc[2];
-    const int c = F.cell[i];
-    const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
-    const int ncs = P.ncs;
-    const int x0 = max(cx - ncs, 0), x1 = min(cx + ncs, nx - 1);
-    const int z0 = D == 3 ? max(cz - ncs, 0) : 0, z1 = D == 3 ? min(cz + ncs, nz - 1) : 0;
-    int images = 1, cyImage = cy;
-    double radius = sqrt(radius2);
+    int images = 1;
+    double radius = sqrt(radius2), imageY = xi[1];
     if (P.period > 0.0) {
         double y = xi[1] - P.period * floor(xi[1] / P.period);
         if (y < radius || y > P.period - radius) {
             images = 2;
-            cyImage = cellCoordinate(xi[1] + (y < 0.5 * P.period ? P.period : -P.period), P.origin[1], P.cellWidth, ny);
+            imageY = xi[1] + (y < 0.5 * P.period ? P.period : -P.period);
         }
     }
     long long found = 0;
     long long write = counts ? 0 : offsets[F.orig[i]];
-    for (int image = 0; image < images; ++image) {
-        const int yc = image == 0 ? cy : cyImage;
-        const int y0 = max(yc - ncs, 0), y1 = min(yc + ncs, ny - 1);
-        for (int zz = z0; zz <= z1; ++zz)
-            for (int yy = y0; yy <= y1; ++yy) {
-                if (image == 1 && yy >= cy - ncs && yy <= cy + ncs) continue;
-                const int row = (zz * ny + yy) * nx;
-                const int begin = F.cellStart[row + x0], end = F.cellStart[row + x1 + 1];
+    // each grid level (coarse, then fine), the particle's own cells and then its image's
+    for (int level = 0; level < P.levels; ++level) {
+        // the coarse grid's ncs cells cover 2 h; the fine grid's as many cells as the radius spans
+        const int n = level == 0 ? P.ncs : (int)ceil(radius / P.fineWidth);
+        const CellBox own = cellBox(P, level, F.cell[i], xi, false, D, n);
+        for (int image = 0; image < images; ++image) {
+            const double pos[3] = {xi[0], image ? imageY : xi[1], xi[2]};
+            const CellBox box = image ? cellBox(P, level, F.cell[i], pos, true, D, n) : own;
+            for (int zz = box.z0; zz <= box.z1; ++zz)
+            for (int yy = box.y0; yy <= box.y1; ++yy) {
+                if (image == 1 && yy >= own.y0 && yy <= own.y1) continue;
+                const int row = box.first + (zz * box.ny + yy) * box.nx;
+                const int begin = F.cellStart[row + box.x0], end = F.cellStart[row + box.x1 + 1];
                 for (int j = begin; j < end; ++j) {
                     if (j == i) continue;
                     double dx = __dsub_rn(xi[0], F.x[0][j]);
@@ -443,6 +447,7 @@ __global__ void neighbourRowsKernel(Params P, Frame F, const int64_t *offsets, i
                     }
                 }
             }
+        }
     }
     if (counts) counts[F.orig[i]] = found;
 }
@@ -518,8 +523,8 @@ void launchCellSort(const Params &P, int n, const MasterView &M, const CellSortB
                     int *sortedCell, const Control *ctl, cudaStream_t st)
 {
     if (n == 0) return;
-    const int total = P.nc[0] * P.nc[1] * P.nc[2] + 1, tiles = scanTiles(total);
-    cellCountKernel<<<blocksFor(n, 256), 256, 0, st>>>(P, n, M.x[0], M.x[1], M.x[2], B.slotCell, B.slotWithin,
+    const int total = P.cells + 1, tiles = scanTiles(total);
+    cellCountKernel<<<blocksFor(n, 256), 256, 0, st>>>(P, n, M.x[0], M.x[1], M.x[2], M.h, B.slotCell, B.slotWithin,
                                                        B.cellCount, ctl);
     cellScanReduceKernel<<<tiles, kScanThreads, 0, st>>>(B.cellCount, total, B.partials, ctl);
     cellScanApplyKernel<<<tiles, kScanThreads, 0, st>>>(B.cellCount, total, B.partials, cellStart, ctl);

@@ -24,6 +24,11 @@
 
 namespace sph {
 
+// Blocks an SM the energy budget's momentum and continuity sweeps are built for: their extra
+// accumulators need about 100 registers a thread in 2D (5 blocks of 128 threads leave 102).
+template <int D>
+constexpr int budgetMinBlocks() { return D == 2 ? 5 : 4; }
+
 // ------------------------------------------------------------------------------------------
 // The neighbour table
 // ------------------------------------------------------------------------------------------
@@ -66,40 +71,45 @@ __global__ void __launch_bounds__(kBlock) listKernel(Params P, Frame F, const Co
         seam = true;
         shift64 = pi[1] < 0.5f * P.periodF ? P.period : -P.period;
     }
-    const int nx = P.nc[0], ny = P.nc[1], ncs = P.ncs;
-    const int c = F.cell[i];
-    const int cx = c % nx, cy = (c / nx) % ny, cz = c / (nx * ny);
-    const int x0 = max(cx - ncs, 0), x1 = min(cx + ncs, nx - 1);
-    const int z0 = D == 3 ? max(cz - ncs, 0) : 0, z1 = D == 3 ? min(cz + ncs, P.nc[2] - 1) : 0;
-    const int cyImage = seam ? cellCoordinate((double)pi[1] + (double)li[1] + shift64, P.origin[1], P.cellWidth, ny) : cy;
-    // the particle's place in its cell, in cell widths, and the reach in cell widths with slack
-    const float invW = (float)(1.0 / P.cellWidth);
-    const float fx = (float)(((double)pi[0] - P.origin[0]) / P.cellWidth) - (float)cx;
-    const float fz = D == 3 ? (float)(((double)pi[2] - P.origin[2]) / P.cellWidth) - (float)cz : 0.5f;
-    const float R = (1.001f * sqrtf(limit) + 5.0e-7f * (fabsf(pi[0]) + fabsf(pi[1]) + fabsf(pi[2]))) * invW + 1.0e-3f;
+    const int ownCell = F.cell[i];
+    const float fineReach = hI + P.fineMax, fineLimit = kCandidateMargin * fineReach * fineReach;
     int *column = F.nbr + 4 * (size_t)i;
     int count = 0;
-    for (int image = 0; image < (seam ? 2 : 1); ++image) {
-        const int yc = image == 0 ? cy : cyImage;
+    // search s: grid level s >> 1 (coarse, fine), origin s & 1 (the particle, its periodic image)
+    for (int search = 0; search < (MIXED ? 4 : 2); ++search) {
+        const int level = MIXED ? search >> 1 : 0, image = search & 1;
+        if (level >= P.levels || (image && !seam)) continue;
+        const double pos[3] = {(double)pi[0] + (double)li[0], (double)pi[1] + (double)li[1] + (image ? shift64 : 0.0),
+                               D == 3 ? (double)pi[2] + (double)li[2] : 0.0};
+        const CellBox box = cellBox(P, level, ownCell, pos, image != 0, D, searchCells(P, level, hI), !MIXED);
+        const float searchLimit = level ? fineLimit : limit;
+        const double width = level ? P.fineWidth : P.cellWidth;
+        const double *origin = level ? P.fineOrigin : P.origin;
+        // the particle's place in the centre cell, in cell widths, and the reach in cell widths with slack
+        const float invW = (float)(1.0 / width);
+        const float fx = (float)(((double)pi[0] - origin[0]) / width) - (float)box.cx;
+        const float fz = D == 3 ? (float)(((double)pi[2] - origin[2]) / width) - (float)box.cz : 0.5f;
+        const float R = (1.001f * sqrtf(searchLimit) + 5.0e-7f * (fabsf(pi[0]) + fabsf(pi[1]) + fabsf(pi[2]))) * invW +
+                        1.0e-3f;
         const float offset = image ? (float)shift64 : 0.0f;
-        const float fy = (float)(((double)pi[1] + (image ? shift64 : 0.0) - P.origin[1]) / P.cellWidth) - (float)yc;
+        const float fy = (float)(((double)pi[1] + (image ? shift64 : 0.0) - origin[1]) / width) - (float)box.cy;
         const bool trim = SPH_LIST_TRIM && fx >= 0.0f && fx < 1.0f && fy >= 0.0f && fy < 1.0f && fz >= 0.0f &&
                           fz < 1.0f;
-        for (int zz = z0; zz <= z1; ++zz) {
-            const int oz = zz - cz;
+        for (int zz = box.z0; zz <= box.z1; ++zz) {
+            const int oz = zz - box.cz;
             const float dz = oz > 0 ? (float)oz - fz : (oz < 0 ? fz - (float)(oz + 1) : 0.0f);
-            for (int yy = max(yc - ncs, 0); yy <= min(yc + ncs, ny - 1); ++yy) {
-                int xa = x0, xb = x1;
+            for (int yy = box.y0; yy <= box.y1; ++yy) {
+                int xa = box.x0, xb = box.x1;
                 if (trim) {
-                    const int oy = yy - yc;
+                    const int oy = yy - box.cy;
                     const float dy = oy > 0 ? (float)oy - fy : (oy < 0 ? fy - (float)(oy + 1) : 0.0f);
                     const float rem = R * R - dy * dy - dz * dz;
                     if (rem < 0.0f) continue;
                     const float ext = sqrtf(rem);
-                    xa = max(x0, cx + (int)floorf(fx - ext));
-                    xb = min(x1, cx + (int)floorf(fx + ext));
+                    xa = max(box.x0, box.cx + (int)floorf(fx - ext));
+                    xb = min(box.x1, box.cx + (int)floorf(fx + ext));
                 }
-                const int row = (zz * ny + yy) * nx;
+                const int row = box.first + (zz * box.ny + yy) * box.nx;
                 const int first = __ldg(&F.cellStart[row + xa]), end = __ldg(&F.cellStart[row + xb + 1]);
                 for (int base = first; base < end; base += L) {
                     const int j = base + t;
@@ -109,7 +119,7 @@ __global__ void __launch_bounds__(kBlock) listKernel(Params P, Frame F, const Co
                         float pj[3];
                         pointIn<D>(A, pj);
                         const float coarse = coarseDistance2<D>(pi, pj, offset);
-                        if (coarse < limit) {
+                        if (coarse < searchLimit) {
                             const float4 B = (D == 3 && PRECISE) || MIXED ? __ldg(&F.pb[j]) : A;
                             float r2 = coarse;      // the float32 points' separation is the coarse one
                             if (PRECISE) {
@@ -167,7 +177,7 @@ struct ShepardVisit {
     }
 };
 
-template <int D, int K, int T>
+template <int D, int K, int T, bool FINE>
 __global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>()) shepardKernel(Params P, Frame F, const Control *ctl)
 {
     if (!filterDue(ctl)) return;
@@ -180,7 +190,7 @@ __global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>()) shepardKernel(Par
     float mi = massOf<D>(F, i);
     ShepardVisit<D, K> visit{F, Smoothing<K, D>(P), G.t == 0 ? mi * own : 0.0f,
                              G.t == 0 ? volumeOf<D>(F, i) * own : 0.0f};
-    forEachNeighbour<D, T>(P, F, i, G.t, hI, visit);
+    forEachNeighbour<D, T, FINE>(P, F, i, G.t, hI, visit);
     float num = groupSum<T>(visit.num, G.mask), den = groupSum<T>(visit.den, G.mask);
     if (G.t != 0) return;
     F.scalar[i] = num / den;
@@ -226,7 +236,7 @@ struct WallVisit {
 
 // Boundary rows only write their own entries and only fluid entries are read, so the frame is
 // updated in place.  writeDensity: the master float64 density takes Tait^-1(p_w) too.
-template <int D, int K, int T>
+template <int D, int K, int T, bool FINE>
 __global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>())
 wallPressureKernel(Params P, Frame F, const Control *ctl, int writeDensity)
 {
@@ -237,7 +247,7 @@ wallPressureKernel(Params P, Frame F, const Control *ctl, int writeDensity)
     float hs = signedLength<D>(F, i);
     if (hs > 0.0f) return;
     WallVisit<D, K> visit{P, F, Smoothing<K, D>(P), 0.0f, 0.0f};
-    forEachNeighbour<D, T>(P, F, i, G.t, -hs, visit);
+    forEachNeighbour<D, T, FINE>(P, F, i, G.t, -hs, visit);
     float weight = groupSum<T>(visit.weight, G.mask), total = groupSum<T>(visit.total, G.mask);
     if (G.t != 0) return;
     float p = 0.0f;
@@ -302,7 +312,7 @@ __device__ __forceinline__ void groupSumMatrix(float M[3][3], unsigned mask)
         for (int b = 0; b < D; ++b) M[a][b] = groupSum<T>(M[a][b], mask);
 }
 
-template <int D, int K, int T>
+template <int D, int K, int T, bool FINE>
 __global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>())
 gradientKernel(Params P, Frame F, const Control *ctl, int wantG, int wantL, int wantRho, float floorDet)
 {
@@ -327,7 +337,7 @@ gradientKernel(Params P, Frame F, const Control *ctl, int wantG, int wantL, int 
         visit.gsum[a] = 0.0f;
         for (int b = 0; b < 3; ++b) { visit.S[a][b] = 0.0f; visit.Mf[a][b] = 0.0f; visit.M[a][b] = 0.0f; }
     }
-    forEachNeighbour<D, T>(P, F, i, G.t, hs, visit);
+    forEachNeighbour<D, T, FINE>(P, F, i, G.t, hs, visit);
     if (wantG) { groupSumMatrix<D, T>(visit.S, G.mask); groupSumMatrix<D, T>(visit.Mf, G.mask); }
     if (wantL || wantRho) groupSumMatrix<D, T>(visit.M, G.mask);
     if (wantRho)
@@ -489,8 +499,8 @@ __device__ __forceinline__ void foldMaxima(Control *ctl, double speed, double ac
 
 // maxima: fold the fluid maxima into ctl and take the time step (the device steps); 0 for the
 // host-step sums.
-template <int D, int K, int T, bool BUDGET>
-__global__ void __launch_bounds__(kBlock, BUDGET ? 4 : sweepMinBlocks<D>())
+template <int D, int K, int T, bool BUDGET, bool FINE>
+__global__ void __launch_bounds__(kBlock, BUDGET ? budgetMinBlocks<D>() : sweepMinBlocks<D>())
 momentumKernel(Params P, Frame F, Control *ctl, int maxima)
 {
     if (ctl && !ctl->active) return;
@@ -512,7 +522,7 @@ momentumKernel(Params P, Frame F, Control *ctl, int maxima)
             visit.total[0] = visit.total[1] = visit.total[2] = 0.0f;
             if constexpr (BUDGET)
                 for (int q = 0; q < 4; ++q) visit.parts[q][0] = visit.parts[q][1] = visit.parts[q][2] = 0.0f;
-            forEachNeighbour<D, T>(P, F, i, G.t, hs, visit);
+            forEachNeighbour<D, T, FINE>(P, F, i, G.t, hs, visit);
             for (int a = 0; a < D; ++a) visit.total[a] = groupSum<T>(visit.total[a], G.mask);
             if constexpr (BUDGET) {
                 for (int q = 0; q < 4; ++q) {
@@ -706,8 +716,8 @@ struct ContinuityVisit {
 };
 
 // mode 0: the rate only; 1: advance the density; 2: advance, drift and enforce.
-template <int D, int K, int T, bool BUDGET>
-__global__ void __launch_bounds__(kBlock, BUDGET ? 4 : sweepMinBlocks<D>())
+template <int D, int K, int T, bool BUDGET, bool FINE>
+__global__ void __launch_bounds__(kBlock, BUDGET ? budgetMinBlocks<D>() : sweepMinBlocks<D>())
 continuityKernel(Params P, Frame F, Control *ctl, Enforcement E, int mode)
 {
     if (ctl && !ctl->active) return;
@@ -730,7 +740,7 @@ continuityKernel(Params P, Frame F, Control *ctl, Enforcement E, int mode)
     }
     visit.total = 0.0f;
     visit.plainFluid = visit.plainWall = visit.continuity = visit.diffusive = 0.0f;
-    forEachNeighbour<D, T>(P, F, i, G.t, fabsf(hs), visit);
+    forEachNeighbour<D, T, FINE>(P, F, i, G.t, fabsf(hs), visit);
     const float rate = groupSum<T>(visit.total, G.mask);
     float parts[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     if constexpr (BUDGET) {
@@ -788,7 +798,7 @@ struct XsphVisit {
 
 // densities: the float32 densities the sum divides by (null: the frame's).  mode 0: the transport
 // velocity into F.vec only; 2: drift with it and enforce.
-template <int D, int K, int T>
+template <int D, int K, int T, bool FINE>
 __global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>())
 xsphKernel(Params P, Frame F, Control *ctl, Enforcement E, const float *densities, int mode)
 {
@@ -807,7 +817,7 @@ xsphKernel(Params P, Frame F, Control *ctl, Enforcement E, const float *densitie
     visit.vi[0] = v[0]; visit.vi[1] = v[1]; visit.vi[2] = v[2];
     visit.rhoI = densities ? densities[i] : densityOf<D>(F, i);
     visit.corr[0] = visit.corr[1] = visit.corr[2] = 0.0f;
-    forEachNeighbour<D, T>(P, F, i, G.t, hs, visit);
+    forEachNeighbour<D, T, FINE>(P, F, i, G.t, hs, visit);
     for (int a = 0; a < D; ++a) visit.corr[a] = groupSum<T>(visit.corr[a], G.mask);
     if (G.t != 0) return;
     float t[3];
@@ -865,7 +875,7 @@ struct ShiftFieldsVisit {
     }
 };
 
-template <int D, int K, int T>
+template <int D, int K, int T, bool FINE>
 __global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>()) shiftFieldsKernel(Params P, Frame F, const Control *ctl)
 {
     if (ctl && !ctl->active) return;
@@ -885,7 +895,7 @@ __global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>()) shiftFieldsKernel
     visit.devI = deviationOf<D>(F, i);
     for (int a = 0; a < 3; ++a) visit.gradient[a] = visit.plain[a] = visit.densityGradient[a] = 0.0f;
     visit.total = 0.0f;
-    forEachNeighbour<D, T>(P, F, i, G.t, hs, visit);
+    forEachNeighbour<D, T, FINE>(P, F, i, G.t, hs, visit);
     float c[3] = {0.0f, 0.0f, 0.0f}, g[3] = {0.0f, 0.0f, 0.0f}, rg[3] = {0.0f, 0.0f, 0.0f};
     for (int a = 0; a < D; ++a) {
         c[a] = groupSum<T>(visit.plain[a], G.mask);
@@ -954,7 +964,7 @@ struct ShiftedVelocityVisit {
 // surface particle (none where h |grad C| > 0.03 there), with the density change shift . grad rho
 // and the velocity change at the new position.  size: CFL Ma (2h)^2 with CFL = c0 dt / h, or
 // 2 h |v_i| dt (local).
-template <int D, int K, int T>
+template <int D, int K, int T, bool FINE>
 __global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>()) shiftKernel(Params P, Frame F, const Control *ctl)
 {
     if (ctl && !ctl->active) return;
@@ -970,7 +980,7 @@ __global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>()) shiftKernel(Param
     SurfaceVisit<D, K> surface{P, F, Smoothing<K, D>(P)};
     surface.normal[0] = surface.normal[1] = surface.normal[2] = 0.0f;
     surface.vicinity = 0;
-    forEachNeighbour<D, T>(P, F, i, G.t, hs, surface);
+    forEachNeighbour<D, T, FINE>(P, F, i, G.t, hs, surface);
     float normal[3];
     for (int a = 0; a < 3; ++a) normal[a] = groupSum<T>(surface.normal[a], G.mask);
     const bool vicinity = groupSum<T>((float)surface.vicinity, G.mask) > 0.0f;
@@ -1001,7 +1011,7 @@ __global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>()) shiftKernel(Param
     if (shift[0] != 0.0f || shift[1] != 0.0f || shift[2] != 0.0f) {
         ShiftedVelocityVisit<D, K> velocity{P, F, Smoothing<K, D>(P)};
         for (int a = 0; a < 3; ++a) { velocity.vi[a] = vi[a]; velocity.shift[a] = shift[a]; velocity.change[a] = 0.0f; }
-        forEachNeighbour<D, T>(P, F, i, G.t, hs, velocity);
+        forEachNeighbour<D, T, FINE>(P, F, i, G.t, hs, velocity);
         for (int a = 0; a < D; ++a) change[a] = groupSum<T>(velocity.change[a], G.mask);
     }
     if (G.t != 0) return;
@@ -1078,7 +1088,7 @@ static void launchList(const LaunchArgs &A)
     else listKernel<D, L, false, true><<<grid, kBlock, 0, st>>>(A.P, A.F, A.ctl, A.maxCount);
 }
 
-template <int D, int K, int T>
+template <int D, int K, int T, bool FINE>
 static void launchT(const LaunchArgs &A, Stage stage)
 {
     const Params &P = A.P;
@@ -1087,27 +1097,27 @@ static void launchT(const LaunchArgs &A, Stage stage)
     if (P.n == 0) return;
     cudaStream_t st = A.stream;
     switch (stage) {
-    case Stage::ShepardSum: shepardKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl); break;
+    case Stage::ShepardSum: shepardKernel<D, K, T, FINE><<<grid, kBlock, 0, st>>>(P, F, A.ctl); break;
     case Stage::ShepardApply: applyShepardKernel<D><<<pointwise, kBlock, 0, st>>>(P, F, A.ctl); break;
-    case Stage::Wall: wallPressureKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.flag); break;
+    case Stage::Wall: wallPressureKernel<D, K, T, FINE><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.flag); break;
     case Stage::Gradients:
-        gradientKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.wantG, A.wantL, A.wantRho, A.floorDet);
+        gradientKernel<D, K, T, FINE><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.wantG, A.wantL, A.wantRho, A.floorDet);
         break;
     case Stage::Momentum:
-        if (P.budget && A.maxima) momentumKernel<D, K, T, true><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.maxima);
-        else momentumKernel<D, K, T, false><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.maxima);
+        if (P.budget && A.maxima) momentumKernel<D, K, T, true, FINE><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.maxima);
+        else momentumKernel<D, K, T, false, FINE><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.maxima);
         break;
     case Stage::Kick: kickKernel<D><<<pointwise, kBlock, 0, st>>>(P, F, A.ctl); break;
     case Stage::Continuity:
         // the budget's parts matter only where the step advances the density
-        if (P.budget && A.flag != 0) continuityKernel<D, K, T, true><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.flag);
-        else continuityKernel<D, K, T, false><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.flag);
+        if (P.budget && A.flag != 0) continuityKernel<D, K, T, true, FINE><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.flag);
+        else continuityKernel<D, K, T, false, FINE><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.flag);
         break;
-    case Stage::Xsph: xsphKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.densities, A.flag); break;
+    case Stage::Xsph: xsphKernel<D, K, T, FINE><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.densities, A.flag); break;
     case Stage::List: launchList<D>(A); break;
     case Stage::Closure: closureKernel<D><<<pointwise, kBlock, 0, st>>>(P, F, A.ctl); break;
-    case Stage::ShiftFields: shiftFieldsKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl); break;
-    case Stage::Shift: shiftKernel<D, K, T><<<grid, kBlock, 0, st>>>(P, F, A.ctl); break;
+    case Stage::ShiftFields: shiftFieldsKernel<D, K, T, false><<<grid, kBlock, 0, st>>>(P, F, A.ctl); break;
+    case Stage::Shift: shiftKernel<D, K, T, false><<<grid, kBlock, 0, st>>>(P, F, A.ctl); break;
     case Stage::ShiftDrift: shiftDriftKernel<D><<<pointwise, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.flag); break;
     case Stage::FrameDensity: frameDensityKernel<D><<<pointwise, kBlock, 0, st>>>(P, F, A.ctl); break;
     }
@@ -1116,10 +1126,18 @@ static void launchT(const LaunchArgs &A, Stage stage)
 template <int D, int K>
 static void launchDK(const LaunchArgs &A, Stage stage)
 {
-    if (A.threads >= 8) launchT<D, K, 8>(A, stage);
-    else if (A.threads == 4) launchT<D, K, 4>(A, stage);
-    else if (A.threads == 2) launchT<D, K, 2>(A, stage);
-    else launchT<D, K, 1>(A, stage);
+    if (A.P.levels > 1) {
+        // the shifting sweeps never see two levels (shifting needs one smoothing length)
+        if (A.threads >= 8) launchT<D, K, 8, true>(A, stage);
+        else if (A.threads == 4) launchT<D, K, 4, true>(A, stage);
+        else if (A.threads == 2) launchT<D, K, 2, true>(A, stage);
+        else launchT<D, K, 1, true>(A, stage);
+    } else {
+        if (A.threads >= 8) launchT<D, K, 8, false>(A, stage);
+        else if (A.threads == 4) launchT<D, K, 4, false>(A, stage);
+        else if (A.threads == 2) launchT<D, K, 2, false>(A, stage);
+        else launchT<D, K, 1, false>(A, stage);
+    }
 }
 
 void launchStage(const LaunchArgs &A, Stage stage)

@@ -111,9 +111,21 @@ __device__ __forceinline__ float support2(float h)
     return __fmul_rn(w, w);
 }
 
+// What a walk needs to set up each of a particle's searches: its sorted cell, point, remainder,
+// length, and the periodic image's shift when it lies near the seam.
+struct Origin {
+    int cell;
+    float hI;
+    bool seam;
+    double shift64;
+};
+
 // The candidates of slot i, one at a time: its table row when the row holds them all, else the
-// cells of its stencil (then twice for an image search across a periodic seam).
-template <int D>
+// cells of its searches.  Search s is of grid level s >> 1 (coarse, then fine when the particles
+// carry two levels of smoothing length) from origin s & 1 (the particle, then its periodic image
+// when it lies near the seam).
+// FINE: the particles carry two levels of smoothing length (else only the coarse grid is searched).
+template <int D, bool FINE>
 struct Candidates {
     // table
     const int4 *column;
@@ -121,26 +133,44 @@ struct Candidates {
     int4 chunk;         // the entries still to visit of the current chunk, first in x
     // walk
     bool walking;
-    int images, image, cyImage, cy, ncs, nx, ny, x0, x1, z0, z1, zz, yy, j, end;
+    int search, first, nx, ny, x0, x1, y0, y1, z1, zz, yy, j, end;
     const int *cellStart;
 
     __device__ __forceinline__ void startRow()
     {
-        const int row = (zz * ny + yy) * nx;
+        const int row = first + (zz * ny + yy) * nx;
         j = __ldg(&cellStart[row + x0]) - 1;
         end = __ldg(&cellStart[row + x1 + 1]);
     }
 
-    __device__ __forceinline__ void startImage()
+    // Starts search s when it applies (its level is present, its image is wanted); false if not.
+    __device__ __forceinline__ bool startSearch(const Params &P, const Origin &O, const float pi[3], const float li[3],
+                                                int s)
     {
-        const int yc = image == 0 ? cy : cyImage;
-        yy = max(yc - ncs, 0);
-        zz = z0;
+        const int level = FINE ? s >> 1 : 0, image = s & 1;
+        if ((!FINE && s >= 2) || level >= P.levels || (image && !O.seam)) return false;
+        const double pos[3] = {(double)pi[0] + (double)li[0],
+                               (double)pi[1] + (double)li[1] + (image ? O.shift64 : 0.0),
+                               D == 3 ? (double)pi[2] + (double)li[2] : 0.0};
+        const CellBox B = cellBox(P, level, O.cell, pos, image != 0, D, searchCells(P, level, O.hI), !FINE);
+        first = B.first;
+        nx = B.nx;
+        ny = B.ny;
+        x0 = B.x0;
+        x1 = B.x1;
+        y0 = B.y0;
+        y1 = B.y1;
+        z1 = B.z1;
+        zz = B.z0;
+        yy = B.y0;
+        search = s;
         startRow();
+        return true;
     }
 
-    // The next candidate into (jOut, imageOut); false when there are none left.
-    __device__ __forceinline__ bool next(int &jOut, int &imageOut)
+    // The next candidate into (jOut, imageOut, levelOut); false when there are none left.
+    __device__ __forceinline__ bool next(const Params &P, const Origin &O, const float pi[3], const float li[3],
+                                         int &jOut, int &imageOut, int &levelOut)
     {
         if (!walking) {
             if (k >= count) return false;
@@ -151,25 +181,27 @@ struct Candidates {
             k = (k & 3) == 3 ? k + 1 + 4 * (step - 1) : k + 1;
             jOut = entry & 0x7FFFFFFF;
             imageOut = entry < 0 ? 1 : 0;
+            levelOut = 0;
             return true;
         }
         while (true) {
             if (++j < end) {
                 jOut = j;
-                imageOut = image;
+                imageOut = search & 1;
+                levelOut = FINE ? search >> 1 : 0;
                 return true;
             }
-            const int yc = image == 0 ? cy : cyImage;
-            if (yy < min(yc + ncs, ny - 1)) {
+            if (yy < y1) {
                 ++yy;
             } else if (zz < z1) {
                 ++zz;
-                yy = max(yc - ncs, 0);
-            } else if (++image < images) {
-                startImage();
-                continue;
+                yy = y0;
             } else {
-                return false;
+                constexpr int searches = FINE ? 4 : 2;
+                int s = search + 1;
+                while (s < searches && !startSearch(P, O, pi, li, s)) ++s;
+                if (s >= searches) return false;
+                continue;
             }
             startRow();
         }
@@ -182,7 +214,7 @@ struct Candidates {
 // image, pb row of j, kin row of j when Visitor::kKinetic) when Visitor::accept(fluidJ), and
 // r >= 1e-12 where Visitor::kSkipCoincident.
 // useTable: false forces the walk (the table kernel itself).
-template <int D, int T, class Visitor>
+template <int D, int T, bool FINE, class Visitor>
 __device__ __forceinline__ void forEachNeighbour(const Params &P, const Frame &F, int i, int t, float hI,
                                                  Visitor &visit, bool useTable = true)
 {
@@ -191,14 +223,21 @@ __device__ __forceinline__ void forEachNeighbour(const Params &P, const Frame &F
     remainderOf<D>(F, i, li);
     const float reach = P.mixedH ? hI + P.hMax : 2.0f * P.hMax;
     const float limit = kCandidateMargin * reach * reach;
-    double shift64 = 0.0;
-    bool seam = false;
+    // the coarse test's bound for fine candidates: no fine neighbour lies past hI + fineMax
+    const float fineReach = hI + P.fineMax;
+    const float fineLimit = kCandidateMargin * fineReach * fineReach;
+    Origin O;
+    O.cell = 0;
+    O.hI = hI;
+    O.shift64 = 0.0;
+    O.seam = false;
     if (D == 3 && P.period > 0.0 && (pi[1] < reach || pi[1] > P.periodF - reach)) {
-        seam = true;
-        shift64 = pi[1] < 0.5f * P.periodF ? P.period : -P.period;
+        O.seam = true;
+        O.shift64 = pi[1] < 0.5f * P.periodF ? P.period : -P.period;
     }
+    const double shift64 = O.shift64;
 
-    Candidates<D> C;
+    Candidates<D, FINE> C;
     const int count = useTable && P.listCap > 0 ? __ldg(&F.ncount[i]) : 0;
     C.walking = !(useTable && P.listCap > 0 && count <= P.listCap);
     if (!C.walking) {
@@ -208,31 +247,18 @@ __device__ __forceinline__ void forEachNeighbour(const Params &P, const Frame &F
         C.k = 4 * t;
         C.step = T;
     } else {
-        C.nx = P.nc[0];
-        C.ny = P.nc[1];
-        const int c = F.cell[i];
-        const int cx = c % C.nx, cz = c / (C.nx * C.ny);
-        C.cy = (c / C.nx) % C.ny;
-        C.ncs = P.ncs;
-        C.x0 = max(cx - C.ncs, 0);
-        C.x1 = min(cx + C.ncs, C.nx - 1);
-        C.z0 = D == 3 ? max(cz - C.ncs, 0) : 0;
-        C.z1 = D == 3 ? min(cz + C.ncs, P.nc[2] - 1) : 0;
+        O.cell = F.cell[i];
         C.cellStart = F.cellStart;
-        C.images = seam ? 2 : 1;
-        C.cyImage = seam ? cellCoordinate((double)pi[1] + (double)li[1] + shift64, P.origin[1], P.cellWidth, C.ny)
-                         : C.cy;
-        C.image = 0;
-        C.startImage();
+        C.startSearch(P, O, pi, li, 0);
     }
 
-    int counted = 0, j = 0, image = 0;
-    while (C.next(j, image)) {
+    int counted = 0, j = 0, image = 0, level = 0;
+    while (C.next(P, O, pi, li, j, image, level)) {
         const float offset = image ? (float)shift64 : 0.0f;     // the search's origin: particle or image
         const float4 A = __ldg(&F.pa[j]);
         float pj[3];
         pointIn<D>(A, pj);
-        if (C.walking && (coarseDistance2<D>(pi, pj, offset) >= limit || j == i)) continue;
+        if (C.walking && (coarseDistance2<D>(pi, pj, offset) >= (FINE && level ? fineLimit : limit) || j == i)) continue;
         const float4 B = __ldg(&F.pb[j]);
         // the kinematic row too, with the others, when the visitor reads it
         const float4 Kj = Visitor::kKinetic ? __ldg(&F.kin[j]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);

@@ -87,6 +87,9 @@ namespace sph {
 void recordError(const std::string &message) { lastError = message; }
 }  // namespace sph
 
+// The shortest neighbour table row worth keeping when memory caps the row below the largest count.
+constexpr int kMinTableRow = 64;
+
 struct SphSystem {
     // configuration
     int device = 0;
@@ -131,7 +134,13 @@ struct SphSystem {
     // grid
     double origin[3] = {0, 0, 0}, cellWidth = 0.0;
     int nc[3] = {1, 1, 1};
-    int numCells = 1;
+    int numCells = 1;           // the coarse grid's cells
+    // the fine level (particles shorter than h): its longest h, its grid, and its cells
+    double fineMax = 0.0;
+    int levels = 1;
+    double fineOrigin[3] = {0, 0, 0}, fineWidth = 0.0;
+    int fineNc[3] = {1, 1, 1};
+    int fineCells = 0;
     // device memory
     MasterView master[2]{};
     float4 *pa = nullptr, *pb = nullptr, *kin = nullptr, *G[3] = {}, *L[3] = {}, *gradRho = nullptr, *acc = nullptr,
@@ -342,19 +351,7 @@ struct SphSystem {
             }
         }
         numCells = (int)total;
-        if (numCells + 1 > cellStartCapacity) {
-            cudaFree(cellStart);
-            cudaFree(sortBuffers.cellCount);
-            cudaFree(sortBuffers.partials);
-            cellStart = sortBuffers.cellCount = sortBuffers.partials = nullptr;
-            cellStartCapacity = 0;
-            TRY(deviceAlloc(&cellStart, numCells + 1));
-            TRY(deviceAlloc(&sortBuffers.cellCount, numCells + 1));
-            TRY(deviceAlloc(&sortBuffers.partials, scanTiles(numCells + 1)));
-            // the counts are zero between sorts: each sort's scan clears what its count added
-            CUDA_TRY(cudaMemsetAsync(sortBuffers.cellCount, 0, sizeof(int) * (numCells + 1), stream));
-            cellStartCapacity = numCells + 1;
-        }
+        TRY(setupLevels());
         // the reference's hash grid shape (src/pysurf/sphGpu.py:1466-1478)
         double extent[3] = {0, 0, 0};
         for (int a = 0; a < dim; ++a) extent[a] = domainMax[a] - domainMin[a];
@@ -373,6 +370,61 @@ struct SphSystem {
         return SPH_OK;
     }
 
+    // The fine level's grid, when some particles are shorter than h (a split's daughters): cells
+    // 2 fineMax / ncs wide over the same domain, capped as the coarse grid is; then the cell
+    // list's arrays for both grids.
+    int setupLevels()
+    {
+        levels = fineMax > 0.0 ? 2 : 1;
+        long long fine = 0;
+        fineWidth = 0.0;
+        for (int a = 0; a < 3; ++a) { fineOrigin[a] = 0.0; fineNc[a] = 1; }
+        if (levels == 2) {
+            fineWidth = 2.0 * fineMax / ncs;
+            while (true) {
+                fine = 1;
+                for (int a = 0; a < dim; ++a) {
+                    fineOrigin[a] = domainMin[a] - fineWidth;
+                    fineNc[a] = (int)ceil((domainMax[a] - domainMin[a]) / fineWidth) + 3;
+                    fine *= fineNc[a];
+                }
+                if (fine <= (1ll << 25)) break;
+                fineWidth *= 1.25;
+            }
+        }
+        fineCells = (int)fine;
+        const int total = numCells + fineCells;
+        if (total + 1 > cellStartCapacity) {
+            cudaFree(cellStart);
+            cudaFree(sortBuffers.cellCount);
+            cudaFree(sortBuffers.partials);
+            cellStart = sortBuffers.cellCount = sortBuffers.partials = nullptr;
+            cellStartCapacity = 0;
+            TRY(deviceAlloc(&cellStart, total + 1));
+            TRY(deviceAlloc(&sortBuffers.cellCount, total + 1));
+            TRY(deviceAlloc(&sortBuffers.partials, scanTiles(total + 1)));
+            // the counts are zero between sorts: each sort's scan clears what its count added
+            CUDA_TRY(cudaMemsetAsync(sortBuffers.cellCount, 0, sizeof(int) * (total + 1), stream));
+            cellStartCapacity = total + 1;
+        }
+        graphDirty = true;
+        cellsFresh = false;
+        listDirty = true;
+        return SPH_OK;
+    }
+
+    // The fine level from the particles' lengths: the longest below h (0 for none).
+    int takeLevels(const double *lengths, int count)
+    {
+        double longest = 0.0;
+        if (lengths)
+            for (int i = 0; i < count; ++i)
+                if (lengths[i] < h && lengths[i] > longest) longest = lengths[i];
+        if (longest == fineMax) return SPH_OK;
+        fineMax = longest;
+        return setupLevels();
+    }
+
     // ---- parameters ----------------------------------------------------------------------------
 
     Params params() const
@@ -388,6 +440,13 @@ struct SphSystem {
         P.cellWidth = cellWidth;
         P.ncs = ncs;
         P.precise = precise;
+        P.levels = levels;
+        for (int a = 0; a < 3; ++a) { P.fineOrigin[a] = fineOrigin[a]; P.fineNc[a] = fineNc[a]; }
+        P.fineWidth = fineWidth;
+        P.fineFirst = numCells;
+        P.cells = numCells + fineCells;
+        P.fineMax = (float)fineMax;
+        P.fineBelow = h;
         P.period = period;
         P.periodF = (float)period;
         P.c0 = (float)c0;
@@ -483,8 +542,8 @@ struct SphSystem {
     }
 
     // Take the neighbour table's size from the current cell list: the largest count now, with room
-    // to grow by a quarter, if it fits in three quarters of the free device memory; otherwise no
-    // table.  Syncs.
+    // to grow by a quarter, or as many entries a particle as three quarters of the free device
+    // memory holds when that is less (the particles with more walk their cells).  Syncs.
     int sizeList()
     {
         listDirty = false;
@@ -507,12 +566,15 @@ struct SphSystem {
         int cap = ((most + most / 4 + 8) + 7) & ~7;
         size_t entries = (size_t)cap * (size_t)capacity;
         if (entries > nbrEntries) {
-            size_t freeBytes = 0, totalBytes = 0;
-            cudaMemGetInfo(&freeBytes, &totalBytes);
             cudaFree(nbr);
             nbr = nullptr;
             nbrEntries = 0;
-            if (entries * sizeof(int) > freeBytes / 4 * 3 || deviceAlloc(&nbr, entries) != SPH_OK) {
+            size_t freeBytes = 0, totalBytes = 0;
+            cudaMemGetInfo(&freeBytes, &totalBytes);
+            const size_t room = freeBytes / 4 * 3 / sizeof(int) / (size_t)std::max(capacity, 1);
+            if ((size_t)cap > room) cap = (int)(room & ~(size_t)7);
+            entries = (size_t)cap * (size_t)capacity;
+            if (cap < kMinTableRow || deviceAlloc(&nbr, entries) != SPH_OK) {
                 nbr = nullptr;
                 cap = 0;
                 cudaGetLastError();
@@ -885,6 +947,7 @@ static int loadState(SphSystem *sys, int64_t count, const double *positions, con
     if (mixed && sys->shifting)
         return fail(SPH_ERR_INVALID, "particle shifting needs one smoothing length for every particle");
     TRY(sys->reserve(n, false));
+    TRY(sys->takeLevels(lengths, n));
     if (sys->n != n) sys->graphDirty = true;
     sys->n = n;
     sys->mixedH = mixed;
@@ -1852,6 +1915,7 @@ int sph_split(SphSystem *sys, const uint8_t *mask, double reference_density, dou
     for (double v : lengths) { hMin = std::min(hMin, v); if (v != sys->h) mixed = true; }
     sys->hMin = hMin;
     sys->mixedH = mixed;
+    TRY(sys->takeLevels(lengths.data(), sys->n));
     sys->framed = false;
     sys->cellsFresh = false;    // the daughters have no cell yet: the next use sorts again
     sys->graphDirty = true;
