@@ -155,6 +155,11 @@ int sph_push(SphSystem *sys, int64_t n, const double *positions, const double *v
 int sph_pull(SphSystem *sys, double *positions, double *velocities, double *densities, double *pressures,
              double *accelerations, double *masses, double *lengths, uint8_t *is_fluid);
 int sph_count(const SphSystem *sys, int64_t *n);
+/* FrameWriter.write's arrays from the device state (src/pysurf/sphFrames.py:60-100): every
+ * particle's float32 position (n x dim) and float32 speed, the speed |v| taken in float64 as numpy
+ * takes it, and its fluid flag, in caller order; the caller keeps the fluid rows.  17 bytes a
+ * particle in 3D cross the bus instead of a float64 pull's 48. */
+int sph_frame(SphSystem *sys, float *positions, float *speeds, uint8_t *is_fluid);
 
 /* PairSums.setBoundary (src/pysurf/sphGpu.py:2121-2171), one call per kind. */
 int sph_clear_boundary(SphSystem *sys);

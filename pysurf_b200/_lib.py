@@ -30,6 +30,7 @@ _pd = C.POINTER(C.c_double)
 _pi64 = C.POINTER(C.c_int64)
 _pu8 = C.POINTER(C.c_uint8)
 _pi32 = C.POINTER(C.c_int32)
+_pf = C.POINTER(C.c_float)
 _h = C.c_void_p
 
 SIGNATURES = {
@@ -60,6 +61,7 @@ SIGNATURES = {
     'sph_push': [_h, _i64, _pd, _pd, _pd, _pd, _pu8, _pd],
     'sph_pull': [_h, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pu8],
     'sph_count': [_h, _pi64],
+    'sph_frame': [_h, _pf, _pf, _pu8],
     'sph_clear_boundary': [_h],
     'sph_set_boundary_container': [_h, _pd, _pd, _i],
     'sph_set_boundary_bed': [_h, _pd, _pd, _i64, _d, _i, _d, _i, _d, _d, _d],

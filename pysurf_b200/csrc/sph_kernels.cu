@@ -344,6 +344,21 @@ __global__ void scatterFloat4Kernel(int n, int dim, const int *orig, const float
     for (int a = 0; a < dim; ++a) out[o * dim + a] = (double)c[a];
 }
 
+// A frame of the run in caller order (src/pysurf/sphFrames.py:60-100): each particle's position in
+// float32, its speed |v| taken in float64 as numpy's norm takes it ((vx^2 + vy^2) + vz^2, then the
+// square root) and rounded to float32, and its fluid flag.
+__global__ void frameKernel(int n, int dim, MasterView M, float *positions, float *speeds, uint8_t *fluid)
+{
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n) return;
+    const int o = M.orig[s];
+    double v2 = __dmul_rn(M.v[0][s], M.v[0][s]);
+    for (int a = 1; a < dim; ++a) v2 = __dadd_rn(v2, __dmul_rn(M.v[a][s], M.v[a][s]));
+    speeds[o] = (float)sqrt(v2);
+    for (int a = 0; a < dim; ++a) positions[(size_t)o * dim + a] = (float)M.x[a][s];
+    fluid[o] = M.fluid[s];
+}
+
 __global__ void scatterFloatKernel(int n, const int *orig, const float *values, double *out)
 {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
@@ -589,6 +604,12 @@ void launchScatterFloat4(int n, int dim, const int *orig, const float4 *values, 
 {
     if (n == 0) return;
     scatterFloat4Kernel<<<blocksFor(n, 256), 256, 0, st>>>(n, dim, orig, values, out);
+}
+
+void launchFrame(int n, int dim, const MasterView &M, float *positions, float *speeds, uint8_t *fluid, cudaStream_t st)
+{
+    if (n == 0) return;
+    frameKernel<<<blocksFor(n, 256), 256, 0, st>>>(n, dim, M, positions, speeds, fluid);
 }
 
 void launchScatterFloat(int n, const int *orig, const float *values, double *out, cudaStream_t st)

@@ -77,6 +77,8 @@ void launchRefreshDensity(int n, const double *rho, float *out, cudaStream_t st)
 void launchScatterDouble(int n, int dim, const int *orig, const double *const *columns, double *out, cudaStream_t st);
 void launchScatterFloat4(int n, int dim, const int *orig, const float4 *values, double *out, cudaStream_t st);
 void launchScatterFloat(int n, const int *orig, const float *values, double *out, cudaStream_t st);
+// Caller-order float32 positions (n x dim), float32 speeds and fluid flags of every particle.
+void launchFrame(int n, int dim, const MasterView &M, float *positions, float *speeds, uint8_t *fluid, cudaStream_t st);
 void launchScatterMatrix(int n, int dim, const int *orig, const Frame &F, int which, double *out, cudaStream_t st);
 void launchScatterPressure(int n, int dim, const int *orig, const Frame &F, double *out, cudaStream_t st);
 void launchNeighbourRows(const Params &P, const Frame &F, const int64_t *offsets, int *rows, long long *counts,

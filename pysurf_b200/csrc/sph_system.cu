@@ -1231,6 +1231,25 @@ int sph_push(SphSystem *sys, int64_t n, const double *positions, const double *v
     return SPH_OK;
 }
 
+int sph_frame(SphSystem *sys, float *positions, float *speeds, uint8_t *is_fluid)
+{
+    CHECK_SYS(sys);
+    if (!positions || !speeds || !is_fluid) return fail(SPH_ERR_INVALID, "null argument");
+    if (!sys->resident) return fail(SPH_ERR_STATE, "no device state: call sph_push first");
+    const int n = sys->n, dim = sys->dim;
+    if (n == 0) return SPH_OK;
+    // float32 rows in the output staging: positions, then speeds
+    float *pos = reinterpret_cast<float *>(sys->stage(SphSystem::kOutSlot));
+    float *speed = reinterpret_cast<float *>(sys->stage(SphSystem::kOutSlot + 2));
+    launchFrame(n, dim, sys->master[sys->cur], pos, speed, sys->dStageU8, sys->stream);
+    CUDA_TRY(cudaGetLastError());
+    TRY(sys->download(positions, pos, sizeof(float) * (size_t)n * dim));
+    TRY(sys->download(speeds, speed, sizeof(float) * (size_t)n));
+    TRY(sys->download(is_fluid, sys->dStageU8, (size_t)n));
+    CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    return SPH_OK;
+}
+
 int sph_count(const SphSystem *sys, int64_t *n)
 {
     if (!sys || !n) return fail(SPH_ERR_INVALID, "null argument");

@@ -632,6 +632,18 @@ class PairSums:
         self.count = int(total.value)
         return int(count.value)
 
+    def frame(self) -> tuple:
+        """The fluid particles' float32 positions (m, dim) and speeds (m,) from the device state, in the
+        caller's order: the arrays of a run's frame (src/pysurf/sphFrames.py:60-100), without a float64 pull."""
+        n, dim = self.count, self.dimensions
+        positions, speeds = np.empty((n, dim), dtype=np.float32), np.empty(n, dtype=np.float32)
+        flags = np.empty(n, dtype=np.uint8)
+        if n:
+            check(self._lib.sph_frame(self._handle, positions.ctypes.data_as(_lib._pf), speeds.ctypes.data_as(_lib._pf),
+                                      flags.ctypes.data_as(_lib._pu8)), 'frame')
+        fluid = flags.astype(bool)
+        return positions[fluid], speeds[fluid]
+
     def pullState(self) -> dict:
         """The whole device state in the caller's order, masses, lengths and flags included."""
         n, dim = self.count, self.dimensions

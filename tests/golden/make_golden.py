@@ -679,6 +679,40 @@ def makeEnergy():
     np.savez_compressed(os.path.join(HERE, 'energy.npz'), **out)
 
 
+def makeFrames():
+    """A run's frame files (src/pysurf/sphFrames.py:38-121), written by the reference's FrameWriter
+    from the split fixture's particles, with a field and a scalar; and its checkpoint layout
+    (src/pysurf/BreakingWave3D.py:204, 785-858): the format tag and the ParticleSystem fields."""
+    import dataclasses
+    import json
+    import tempfile
+    from pysurf import BreakingWave3D
+    from pysurf.sphFrames import FrameWriter, readFrame
+    from pysurf.sphParticles import ParticleSystem
+    out = {}
+    split = np.load(os.path.join(HERE, 'split.npz'))
+    for dimensions in (2, 3):
+        tag, key = f'frames{dimensions}d', f'split{dimensions}d_0.5'
+        p = ParticleSystem(**{name: split[f'{key}/split_{name}'] for name in
+                              ('positions', 'velocities', 'accelerations', 'densities', 'pressures', 'masses',
+                               'isFluid', 'lengths')})
+        fluidCount = int(p.isFluid.sum())
+        with tempfile.TemporaryDirectory() as directory:
+            writer = FrameWriter(directory)
+            writer.write(0.25, p, step=7, fields={'ids': np.arange(fluidCount)}, scalars={'energy': 1.5})
+            writer.write(0.5, p, step=9)
+            for frame in (0, 1):
+                for name, values in readFrame(directory, frame).items():
+                    out[f'{tag}/frame{frame}_{name}'] = values
+            with open(os.path.join(directory, 'frames.json'), encoding='utf-8') as handle:
+                out[f'{tag}/index'] = np.array(handle.read())
+        for name in ('positions', 'velocities', 'masses', 'isFluid', 'lengths'):
+            out[f'{tag}/state_{name}'] = getattr(p, name)
+    out['checkpoint/format'] = np.array(BreakingWave3D.checkpointFormat)
+    out['checkpoint/particleFields'] = np.array([f.name for f in dataclasses.fields(ParticleSystem)])
+    np.savez_compressed(os.path.join(HERE, 'frames.npz'), **out)
+
+
 def main():
     root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('PYSURF_REFERENCE', '')
     if not root or not os.path.isdir(root):
@@ -686,7 +720,7 @@ def main():
     loadReference(root)
     makers = {'cellkeys': makeCellKeys, 'clouds': makeClouds, 'enforce': makeEnforcement, 'split': makeSplit,
               'beach': makeBeach, 'runs': makeRuns, 'breaking': makeBreaking, 'closure': makeClosure,
-              'shifting': makeShifting, 'energy': makeEnergy}
+              'shifting': makeShifting, 'energy': makeEnergy, 'frames': makeFrames}
     for name in (sys.argv[2:] or list(makers)):
         makers[name]()
     for name in sorted(os.listdir(HERE)):
