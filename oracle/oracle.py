@@ -421,3 +421,88 @@ def splitParticles(state, mask, rho0, referenceLength, lengthRatio=1.0):
     state['isFluid'] = np.concatenate([fluid, np.ones(chosen.size * (count - 1), dtype=bool)])
     state['lengths'] = np.concatenate([lengths, rep(length)])
     return int(chosen.size)
+
+
+def refinementLevels(masses, referenceMass, dim):
+    """src/pysurf/sphRefinement.py:123-134: how many times each particle has split, from its mass."""
+    return np.rint(np.log2(referenceMass / _f64(masses)) / dim).astype(int)
+
+
+def _cellGroups(points, cell, offset, size):
+    """src/pysurf/sphRefinement.py:192-217: bin the points into cubes `cell` across (the grid moved by
+    `offset` cells); in every cube holding `size` or more, the `size` nearest its centre, ties to the
+    lower index.  Rows of point indices, the cubes in their raveled order."""
+    u = points / cell + offset
+    base = np.floor(u)
+    keys = base.astype(np.int64)
+    keys -= keys.min(axis=0)
+    flat = np.ravel_multi_index(keys.T, keys.max(axis=0) + 1)
+    off = np.sum((u - base - 0.5) ** 2, axis=1)
+    order = np.lexsort((np.arange(len(points)), off, flat))
+    cubes, first, counts = np.unique(flat[order], return_index=True, return_counts=True)
+    rows = [order[f:f + size] for f, c in zip(first, counts) if c >= size]
+    return np.array(rows, dtype=np.int64).reshape(-1, size)
+
+
+def mergeParticles(state, mask, rho0, referenceMass, referenceLength, lengthRatio=1.0, offsets=(0.0, 0.5)):
+    """src/pysurf/sphRefinement.py:219-311 on a dict state: the chosen split fluid particles of each
+    level, 2^dim to a cube one level coarser, merge into one at the group's first place; fluid from the
+    end fills the places the others leave among the boundary's.  Returns (groups, removed kinetic
+    energy, source), source the old index of each particle after."""
+    x = _f64(state['positions'])
+    n, dim = x.shape
+    size = 2 ** dim
+    fluid = np.asarray(state['isFluid'], dtype=bool)
+    levels = refinementLevels(state['masses'], referenceMass, dim)
+    eligible = np.asarray(mask, dtype=bool) & fluid & (levels > 0)
+    found = []
+    for level in sorted(set(levels[eligible].tolist())):
+        cell = (referenceMass / size ** (level - 1) / rho0) ** (1.0 / dim)
+        free = np.flatnonzero(eligible & (levels == level))
+        for offset in offsets:
+            if free.size < size:
+                break
+            rows = free[_cellGroups(x[free], cell, offset, size)]
+            if rows.size:
+                found.append(rows)
+                free = free[~np.isin(free, rows.ravel())]
+    if not found:
+        return 0, 0.0, np.arange(n)
+    members = np.sort(np.vstack(found), axis=1)
+    m = _f64(state['masses'])[members]
+    total = m.sum(axis=1)
+    w = m / total[:, None]
+    v = _f64(state['velocities'])[members]
+    mean = np.sum(w[:, :, None] * v, axis=1)
+    removed = 0.5 * float(np.sum(m * np.sum((v - mean[:, None, :]) ** 2, axis=2)))
+    lengths = np.full(n, referenceLength) if state.get('lengths') is None else _f64(state['lengths']).copy()
+    head = members[:, 0]
+    out = {key: np.array(state[key], dtype=float) for key in ('positions', 'velocities', 'accelerations',
+                                                               'densities', 'pressures', 'masses')}
+    out['positions'][head] = np.sum(w[:, :, None] * x[members], axis=1)
+    out['accelerations'][head] = np.sum(w[:, :, None] * _f64(state['accelerations'])[members], axis=1)
+    out['pressures'][head] = np.sum(w * _f64(state['pressures'])[members], axis=1)
+    out['densities'][head] = total / np.sum(m / _f64(state['densities'])[members], axis=1)
+    out['velocities'][head] = mean
+    out['masses'][head] = total
+    lengths[head] = lengths[members].mean(axis=1) / lengthRatio
+    out['lengths'] = lengths
+    out['isFluid'] = fluid.copy()
+    # the compaction: the group's others go; fluid from the end takes the places among the boundary's
+    gone = np.zeros(n, dtype=bool)
+    gone[members[:, 1:].ravel()] = True
+    last = int(np.flatnonzero(~fluid).max()) if (~fluid).any() else -1
+    holes = np.flatnonzero(gone[:last + 1])
+    tail = np.flatnonzero(~gone[last + 1:]) + last + 1
+    if tail.size < holes.size:
+        raise RuntimeError('too few fluid particles after the boundary to fill its places')
+    movers = tail[tail.size - holes.size:]
+    keep = ~gone
+    keep[holes] = True
+    keep[movers] = False
+    source = np.arange(n)
+    source[holes] = movers
+    source = source[keep]
+    for key, values in out.items():
+        state[key] = values[source]
+    return int(len(members)), removed, source

@@ -713,6 +713,52 @@ def makeFrames():
     np.savez_compressed(os.path.join(HERE, 'frames.npz'), **out)
 
 
+def makeMerge():
+    """mergeParticles (src/pysurf/sphRefinement.py:192-311): a lattice with its boundary, split in part
+    (h kept, and h halved), jittered, then merged in part; a second level split and merged; and a
+    merge straight after a split."""
+    from pysurf.sphParticles import ParticleSystem
+    from pysurf.sphRefinement import mergeParticles, splitParticles
+    out = {}
+    fields = ('positions', 'velocities', 'accelerations', 'densities', 'pressures', 'masses', 'isFluid', 'lengths')
+    for dimensions in (2, 3):
+        for ratio, twice in ((1.0, False), (0.5, False), (0.5, True)):
+            rng = np.random.default_rng(40 + dimensions + (2 if twice else 0) + int(ratio * 4))
+            s = 0.05
+            side = 12 if dimensions == 2 else 6
+            axes = [np.arange(side) * s + 0.5 * s for _ in range(dimensions)]
+            fluid = np.stack(np.meshgrid(*axes, indexing='ij'), axis=-1).reshape(-1, dimensions) + 0.3
+            wall = rng.uniform(0.0, 0.25, (40, dimensions))
+            particles = ParticleSystem.assemble(fluid, wall, s, 1000.0, rng.normal(0.0, 1.0, (len(fluid), dimensions)))
+            n = len(particles.masses)
+            particles.densities = 1000.0 + rng.uniform(-5, 5, n)
+            particles.pressures = rng.uniform(0, 10, n)
+            particles.accelerations = rng.normal(0.0, 1.0, (n, dimensions))
+            referenceMass = 1000.0 * s ** dimensions
+            length = 1.3 * s
+            splitParticles(particles, rng.uniform(size=n) < 0.7, 1000.0, length, ratio)
+            if twice:
+                splitParticles(particles, rng.uniform(size=len(particles.masses)) < 0.5, 1000.0, length, ratio)
+            count = len(particles.masses)
+            fluidRows = particles.isFluid
+            particles.positions[fluidRows] += rng.uniform(-0.1, 0.1, (int(fluidRows.sum()), dimensions)) * s
+            particles.velocities[fluidRows] += rng.normal(0.0, 0.2, (int(fluidRows.sum()), dimensions))
+            particles.densities = 1000.0 + rng.uniform(-5, 5, count)
+            mask = rng.uniform(size=count) < 0.85
+            tag = f'merge{dimensions}d_{ratio}{"_twice" if twice else ""}'
+            for name in fields:
+                out[f'{tag}/{name}'] = np.array(getattr(particles, name))
+            out[f'{tag}/mask'] = mask
+            out[f'{tag}/reference'] = np.array([1000.0, referenceMass, length, ratio])
+            result = mergeParticles(particles, mask, 1000.0, referenceMass, length, ratio)
+            out[f'{tag}/groups'] = np.array(result.groups)
+            out[f'{tag}/removedEnergy'] = np.array(result.removedEnergy)
+            out[f'{tag}/source'] = np.asarray(result.source)
+            for name in fields:
+                out[f'{tag}/merged_{name}'] = np.array(getattr(particles, name))
+    np.savez_compressed(os.path.join(HERE, 'merge.npz'), **out)
+
+
 def main():
     root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('PYSURF_REFERENCE', '')
     if not root or not os.path.isdir(root):
@@ -720,7 +766,8 @@ def main():
     loadReference(root)
     makers = {'cellkeys': makeCellKeys, 'clouds': makeClouds, 'enforce': makeEnforcement, 'split': makeSplit,
               'beach': makeBeach, 'runs': makeRuns, 'breaking': makeBreaking, 'closure': makeClosure,
-              'shifting': makeShifting, 'energy': makeEnergy, 'frames': makeFrames}
+              'shifting': makeShifting, 'energy': makeEnergy, 'frames': makeFrames,
+              'merge': makeMerge}
     for name in (sys.argv[2:] or list(makers)):
         makers[name]()
     for name in sorted(os.listdir(HERE)):
