@@ -208,6 +208,17 @@ int sph_neighbor_list(SphSystem *sys, double radius, int64_t *offsets, int32_t *
  * and the rest appended in the caller's order.  *split returns how many split. */
 int sph_split(SphSystem *sys, const uint8_t *mask, double reference_density, double length_ratio, int64_t *split);
 
+/* mergeParticles (src/pysurf/sphRefinement.py:219-311; WcsphSolver.merge, src/pysurf/sphSolver.py:2046-2092)
+ * on the device-resident state: the split fluid particles mask (caller order, n bytes) selects merge,
+ * 2^dim of one level into one particle of the level above (cubes one coarser particle across,
+ * two passes, the 2^dim nearest each cube's centre); the merged particle takes its group's first
+ * place, and fluid from the end fills the places the others leave among the boundary's.  *groups
+ * and *removed_energy (the members' kinetic energy about their centres of mass) come back, and
+ * source, when not NULL, takes the caller index before the merge of each particle after (the new
+ * count of entries, sph_count).  Refused with particle shifting on. */
+int sph_merge(SphSystem *sys, const uint8_t *mask, double reference_density, double reference_mass,
+              double length_ratio, int64_t *groups, double *removed_energy, int64_t *source);
+
 /* Crest-zone refinement on the device: every fluid particle of mass at least min_mass (one not yet
  * split) whose column -- columns `width` across from (x0, y0), nx by ny of them (ny 1 in 2D) --
  * has its highest fluid particle above `threshold` (the surface's height), splits as sph_split

@@ -73,6 +73,7 @@ SIGNATURES = {
     'sph_cell_order_key': [_pd, _i64, _i, _d, _pi64, _pi64, _i],
     'sph_neighbor_list': [_h, _d, _pi64, _pi32, _i64, _pi64],
     'sph_split': [_h, _pu8, _d, _d, _pi64],
+    'sph_merge': [_h, _pu8, _d, _d, _d, _pi64, _pd, _pi64],
     'sph_set_closure': [_h, _i, _d, _d, _d],
     'sph_set_shifting': [_h, _i, _d, _d, _d, _i],
     'sph_shifting_displacement': [_h, _pd, _d, _pd, _pd, _pd, _pd],

@@ -15,7 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 LIBRARY = os.path.join(HERE, 'libpysurf_b200.so')
 SOURCES = ['csrc/sph_kernels.cu', 'csrc/sph_sweep_kernels.cu', 'csrc/sph_system.cu', 'csrc/sph_noalloc.cu',
-           'csrc/sph_surface.cu']
+           'csrc/sph_surface.cu', 'csrc/sph_merge.cu']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 FLAGS = ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC', '-shared']
 

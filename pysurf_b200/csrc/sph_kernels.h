@@ -50,6 +50,32 @@ struct LaunchArgs {
 };
 
 void launchStage(const LaunchArgs &A, Stage stage);
+
+// A merge of split particles (sph_merge.cu): the current master and the buffer it moves into, with
+// that buffer's frame, the step's parameters, the frame's accelerations and pressures, the energy
+// budget's rows (null when off), the caller-order mask on the device, and where the caller-order
+// source of each particle after goes.
+struct MergeArgs {
+    int n, dim;
+    MasterView master, next;
+    Frame nextFrame;
+    Params params;
+    float4 *acc;
+    const float *pres;
+    double *energy;
+    int energyStride, energyTerms;
+    const uint8_t *mask;
+    double referenceDensity, referenceMass, lengthRatio;
+    long long *source;
+    cudaStream_t stream;
+};
+struct MergeResultDevice {
+    int groups, newCount;
+    double removedEnergy;
+    const char *error;
+};
+// 0, or -1 with out.error set; with no group found the state is untouched.
+int runMerge(const MergeArgs &in, MergeResultDevice &out);
 // The counting sort's scratch: slotCell, slotWithin, perm (n entries), bucket (n pairs), cellCount
 // (numCells + 1 entries, all zero between sorts), partials (scanTiles(numCells + 1) entries).
 struct CellSortBuffers {

@@ -1943,4 +1943,77 @@ int sph_split(SphSystem *sys, const uint8_t *mask, double reference_density, dou
     return SPH_OK;
 }
 
+int sph_merge(SphSystem *sys, const uint8_t *mask, double reference_density, double reference_mass,
+              double length_ratio, int64_t *groups, double *removed_energy, int64_t *source)
+{
+    CHECK_SYS(sys);
+    if (!mask || !groups || !removed_energy) return fail(SPH_ERR_INVALID, "null argument");
+    if (!sys->resident) return fail(SPH_ERR_STATE, "no device state: call sph_push first");
+    if (!(reference_density > 0.0) || !(reference_mass > 0.0) || !(length_ratio > 0.0) || length_ratio > 1.0)
+        return fail(SPH_ERR_INVALID, "the reference density and mass must be positive, the length ratio in (0, 1]");
+    if (sys->shifting) return fail(SPH_ERR_INVALID, "particle shifting takes one smoothing length throughout");
+    *groups = 0;
+    *removed_energy = 0.0;
+    const int n = sys->n;
+    if (n == 0) return SPH_OK;
+    if (!sys->framed) sys->rebuild();       // the frame's pressures in the master's order
+    TRY(sys->upload(sys->dStageU8, mask, n));
+    long long *dSource = nullptr;
+    TRY(deviceAlloc(&dSource, n));
+    MergeArgs in{};
+    in.n = n;
+    in.dim = sys->dim;
+    in.master = sys->master[sys->cur];
+    in.next = sys->master[1 - sys->cur];
+    in.nextFrame = sys->frame();
+    for (int a = 0; a < 3; ++a) { in.nextFrame.x[a] = in.next.x[a]; in.nextFrame.v[a] = in.next.v[a]; }
+    in.nextFrame.rho = in.next.rho; in.nextFrame.m = in.next.m; in.nextFrame.h = in.next.h;
+    in.nextFrame.fluid = in.next.fluid; in.nextFrame.orig = in.next.orig;
+    in.params = sys->params();
+    in.acc = sys->acc;
+    in.pres = sys->pres;
+    in.energy = sys->budget && sys->energy ? sys->energy : nullptr;
+    in.energyStride = sys->energyCap;
+    in.energyTerms = kEnergyTerms;
+    in.mask = sys->dStageU8;
+    in.referenceDensity = reference_density;
+    in.referenceMass = reference_mass;
+    in.lengthRatio = length_ratio;
+    in.source = dSource;
+    in.stream = sys->stream;
+    MergeResultDevice out{};
+    const int status = runMerge(in, out);
+    if (status != 0) {
+        cudaFree(dSource);
+        return fail(SPH_ERR_CUDA, std::string("merge: ") + (out.error ? out.error : "failed"));
+    }
+    if (out.groups > 0) {
+        sys->cur = 1 - sys->cur;
+        sys->n = out.newCount;
+        sys->framed = true;
+        sys->cellsFresh = false;
+        sys->listDirty = true;
+        sys->graphDirty = true;
+        std::vector<double> lengths(sys->n);
+        CUDA_TRY(cudaMemcpy(lengths.data(), sys->master[sys->cur].h, sizeof(double) * sys->n, cudaMemcpyDeviceToHost));
+        double hMin = lengths.empty() ? sys->h : lengths[0];
+        bool mixed = false;
+        for (double v : lengths) { hMin = std::min(hMin, v); if (v != sys->h) mixed = true; }
+        sys->hMin = hMin;
+        sys->mixedH = mixed;
+        TRY(sys->takeLevels(lengths.data(), sys->n));
+        if (source) {
+            std::vector<long long> from(sys->n);
+            CUDA_TRY(cudaMemcpy(from.data(), dSource, sizeof(long long) * sys->n, cudaMemcpyDeviceToHost));
+            for (int k = 0; k < sys->n; ++k) source[k] = from[k];
+        }
+    } else if (source) {
+        for (int k = 0; k < n; ++k) source[k] = k;
+    }
+    cudaFree(dSource);
+    *groups = out.groups;
+    *removed_energy = out.removedEnergy;
+    return SPH_OK;
+}
+
 }  // extern "C"

@@ -619,6 +619,23 @@ class PairSums:
         self.count = int(total.value)
         return int(count.value)
 
+    def merge(self, mask, referenceDensity: float, referenceMass: float, lengthRatio: float = 1.0):
+        """mergeParticles (src/pysurf/sphRefinement.py:219-311) on the device-resident state: returns
+        (groups, removed kinetic energy, source), source the caller index before the merge of each
+        particle after."""
+        flags, flagPtr = u8(mask)
+        if len(flags) != self.count:
+            raise ValueError('the mask must hold one flag per particle')
+        groups, removed = _lib.C.c_int64(0), _lib.C.c_double(0.0)
+        source = np.empty(max(self.count, 1), dtype=np.int64)
+        check(self._lib.sph_merge(self._handle, flagPtr, float(referenceDensity), float(referenceMass),
+                                  float(lengthRatio), _lib.C.byref(groups), _lib.C.byref(removed),
+                                  source.ctypes.data_as(_lib._pi64)), 'merge')
+        count = _lib.C.c_int64(0)
+        check(self._lib.sph_count(self._handle, _lib.C.byref(count)))
+        self.count = int(count.value)
+        return int(groups.value), float(removed.value), source[:self.count]
+
     def splitCrestZone(self, x0: float, y0: float, width: float, nx: int, ny: int, threshold: float,
                        minMass: float, referenceDensity: float, lengthRatio: float = 0.5) -> int:
         """Split, on the device, every unsplit fluid particle (mass at least `minMass`) whose column
