@@ -168,6 +168,7 @@ struct SphSystem {
     int listCap = 0;
     int tableMode = 1;          // 0 never build the table, 1 build it when it fits the budget
     bool listDirty = true;      // the table's size must be taken again before the next step
+    int listSizedFor = -1;      // the particle count the table's size was taken for
     int threads = 4;            // threads per particle in the sweeps
     int cellStartCapacity = 0;
     // execution
@@ -285,7 +286,7 @@ struct SphSystem {
         TRY(deviceAlloc(&sortBuffers.slotWithin, cap));
         TRY(deviceAlloc(&sortBuffers.perm, cap));
         TRY(deviceAlloc(&sortBuffers.bucket, cap));
-        TRY(deviceAlloc(&dStage, (size_t)kStageSlots * cap));
+        TRY(deviceAlloc(&dStage, (size_t)kStageSlots * cap + 4));    // + the pointer table of a tiny capacity
         TRY(deviceAlloc(&dStageU8, cap));
         TRY(deviceAlloc(&dRank, cap));
         TRY(deviceAlloc(&ncount, cap));
@@ -547,6 +548,7 @@ struct SphSystem {
     int sizeList()
     {
         listDirty = false;
+        listSizedFor = n;
         if (n == 0 || tableMode == 0) {
             if (listCap) graphDirty = true;
             listCap = 0;
@@ -984,8 +986,7 @@ int sph_update(SphSystem *sys, int64_t n, const double *positions, const double 
 
 static int needFrame(SphSystem *sys)
 {
-    if (!sys->framed && sys->n > 0) return fail(SPH_ERR_STATE, "no particles: call sph_update or sph_push first");
-    if (!sys->cellsFresh && sys->n > 0) sys->rebuild();
+    if (sys->n > 0 && (!sys->framed || !sys->cellsFresh)) sys->rebuild();
     return SPH_OK;
 }
 
@@ -1220,12 +1221,12 @@ int sph_push(SphSystem *sys, int64_t n, const double *positions, const double *v
     if (n > 0 && (!velocities || !densities)) return fail(SPH_ERR_INVALID, "null state array");
     TRY(loadState(sys, n, positions, velocities, densities, masses, is_fluid, lengths));
     sys->resident = true;
+    // the cell list, the frame and the table follow at the first step or host-step call; the table
+    // keeps its row length unless the count changed (a particle whose row is too short walks)
+    if (sys->listCap == 0 || sys->listSizedFor != sys->n) sys->listDirty = true;
     // the energy budget counts from the push (src/pysurf/sphGpu.py:2207-2221)
     if (sys->budget && sys->energy)
         CUDA_TRY(cudaMemsetAsync(sys->energy, 0, sizeof(double) * kEnergyTerms * sys->energyCap, sys->stream));
-    // the frame follows at the first step; make the cell list now so host-step calls work too
-    sys->rebuild();
-    TRY(sys->sizeList());
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(sys->stream));
     return SPH_OK;
@@ -1264,18 +1265,20 @@ int sph_pull(SphSystem *sys, double *positions, double *velocities, double *dens
     int n = sys->n, dim = sys->dim;
     if (n == 0) return SPH_OK;
     const MasterView &M = sys->master[sys->cur];
-    // device-side scatter of each field into caller order, then one copy out each
-    double *out = sys->stage(SphSystem::kOutSlot);
+    // each field scattered into caller order in its own staging rows (0 .. 14; 15 holds the column
+    // pointers), copied out in stream order, and one sync at the end
+    int slot = 0;
+    auto rows = [&](int width) { double *p = sys->stage(slot); slot += width; return p; };
     auto scatterColumns = [&](double *const *src, int width, double *host) -> int {
         if (!host) return SPH_OK;
-        // the column pointers go to the device through the u8 staging's tail
+        double *out = rows(width);
+        // the column pointers go to the device through the staging's last row; stream order keeps
+        // each launch's table until it has run
         const double *ptrs[3] = {src[0], src[1], src[2]};
         double **dptrs = (double **)sys->stage(15);
         CUDA_TRY(cudaMemcpyAsync(dptrs, ptrs, sizeof(ptrs), cudaMemcpyHostToDevice, sys->stream));
         launchScatterDouble(n, width, M.orig, (const double *const *)dptrs, out, sys->stream);
-        TRY(sys->download(host, out, sizeof(double) * n * width));
-        CUDA_TRY(cudaStreamSynchronize(sys->stream));
-        return SPH_OK;
+        return sys->download(host, out, sizeof(double) * n * width);
     };
     double *xcols[3] = {M.x[0], M.x[1], M.x[2]};
     double *vcols[3] = {M.v[0], M.v[1], M.v[2]};
@@ -1288,14 +1291,14 @@ int sph_pull(SphSystem *sys, double *positions, double *velocities, double *dens
     TRY(scatterColumns(mcol, 1, masses));
     TRY(scatterColumns(hcol, 1, lengths));
     if (pressures && sys->framed) {
+        double *out = rows(1);
         launchScatterPressure(n, dim, M.orig, sys->frame(), out, sys->stream);
         TRY(sys->download(pressures, out, sizeof(double) * n));
-        CUDA_TRY(cudaStreamSynchronize(sys->stream));
     }
     if (accelerations) {
+        double *out = rows(dim);
         launchScatterFloat4(n, dim, M.orig, sys->acc, out, sys->stream);
         TRY(sys->download(accelerations, out, sizeof(double) * n * dim));
-        CUDA_TRY(cudaStreamSynchronize(sys->stream));
     }
     if (is_fluid) {
         // fluid flags: gather through a float scatter of 0/1
