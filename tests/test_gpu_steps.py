@@ -308,3 +308,28 @@ def test_the_shifting_run_follows_the_reference_host_steps():
     assert np.abs(state.positions - r['finalPositions']).max() < 1e-6
     assert np.abs(state.velocities - r['finalVelocities']).max() < 1e-3
     assert np.abs(state.densities - r['finalDensities']).max() < 1e-3
+
+
+def test_the_dam_break_follows_the_oracle():
+    # the 1 x 2 m column in the 4 x 3 m tank at 0.02 m (5,000 fluid particles,
+    # jittered from seed 0), Wendland C2 at h = 1.3 dx, hydrostatic delta-SPH, 100 device steps
+    # against the float64 oracle's
+    from oracle import oracle
+    case = cases.damBreak()
+    steps = 100
+    state, time, _ = deviceRun(case, steps)
+    b = case.boundary
+    stepper = oracle.Stepper(2, case.kernelType, case.smoothingLength, case.referenceDensity, case.soundSpeed,
+                             case.alpha, case.gravity, case.boundaryViscosityFactor, case.xsphEpsilon,
+                             case.densityFloor, case.densityDiffusion, case.diffusionDelta, case.wallExtrapolated,
+                             case.negativePressure, case.continuityCorrection, case.viscosityLimiter, case.cflNumber,
+                             case.maxTimeStep, 0.0, case.densityFilterInterval,
+                             ('container', b.containerMin, b.containerMax, b.openTop))
+    ref = {k: np.array(getattr(case.state, k), copy=True) for k in ('positions', 'velocities', 'densities', 'masses',
+                                                                    'isFluid')}
+    for _ in range(steps):
+        stepper(ref)
+    assert time == pytest.approx(stepper.time, rel=1e-5)
+    assert np.abs(state.positions - ref['positions']).max() < 1e-6
+    assert np.abs(state.velocities - ref['velocities']).max() < 1e-3
+    assert np.abs(state.densities - ref['densities']).max() < 1e-2
