@@ -618,7 +618,9 @@ struct MomentumVisit {
             if (slopeI * slopeJ > 0.0f) {
                 // 4 R / (1 + R)^2 at R = slopeI / slopeJ, as 4 slopeI slopeJ / (slopeI + slopeJ)^2
                 const float sum = slopeI + slopeJ;
-                limiter = fminf(1.0f, 4.0f * slopeI * slopeJ / (sum * sum));
+                // the fast division (2 ulp) takes 8% off the momentum sweep; its range limit (a
+                // denominator past 2^126) lies far beyond any pair's slopes
+                limiter = fminf(1.0f, __fdividef(4.0f * slopeI * slopeJ, sum * sum));
                 if (q < kCloseDistance) {
                     float fade = (q - kCloseDistance) * (1.0f / kFoldWidth);
                     limiter *= expf(-fade * fade);
