@@ -302,7 +302,7 @@ def toBreaking(args) -> None:
 
 
 def sweepBench(args) -> None:
-    """BASELINE config 4 at the size asked: the first --sweep cases of the seeded sweep (slope
+    """The batched sweep at the size asked: the first --sweep cases of the seeded sweep (slope
     log-U(1/35, 1/8), H/d U(0.2, 0.6), 16-64 ppd) to their breaking points, first one after another,
     then --slots at a time; every batched result must equal its case-by-case one."""
     import numpy as np
@@ -337,7 +337,7 @@ def ridgeRequest(spec):
 
 
 def serveBench(args) -> None:
-    """BASELINE config 5 at a reduced size: --serve requests arriving as a Poisson stream at 20 a
+    """The served stream at a reduced size: --serve requests arriving as a Poisson stream at 20 a
     second (seed 0), 80% 2D beaches drawn as the sweep draws them and 20% 3D ridges at 8-16 ppd (0.4M
     to 2.4M particles), each run for U(2, 6) s of simulated time times --horizon-scale; admitted as
     slots (--slots) and device memory free up, solved beside the requests in flight."""

@@ -383,7 +383,7 @@ def ridgeWave3D(particlesPerDepth: int = 32, depth: float = 1.0, height: float =
 
 
 def refineCrestZone(sums, case: Case, share: float = 0.3, lengthRatio: float = 0.5) -> int:
-    """The crest-zone split of BASELINE's 3D ridge workload: every fluid particle not yet split, in a
+    """The crest-zone split of the 3D ridge workload: every fluid particle not yet split, in a
     column (one spacing across) whose surface stands more than `share` H above still water, splits
     into 2^dim daughters of h times `lengthRatio` (src/pysurf/sphRefinement.py:136-190), on the
     device.  Returns how many split."""

@@ -1,4 +1,4 @@
-"""A full run to the breaking point: the device against the float64 step (the north star's 1%).
+"""A full run to the breaking point: the device against the float64 step, to 1% in time and crest.
 
 The 16-ppd solitary wave (H/d 0.45, 1:15 beach, deltaSph scheme) runs from its start until the
 breaking tracker (the reference's 'cells' face measure, pysurf_b200.breaking) records the breaking

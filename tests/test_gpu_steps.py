@@ -311,7 +311,7 @@ def test_the_shifting_run_follows_the_reference_host_steps():
 
 
 def test_the_dam_break_follows_the_oracle():
-    # the 1 x 2 m column in the 4 x 3 m tank at 0.02 m (5,000 fluid particles,
+    # the CPU-runnable dam break: the 1 x 2 m column in the 4 x 3 m tank at 0.02 m (5,000 fluid particles,
     # jittered from seed 0), Wendland C2 at h = 1.3 dx, hydrostatic delta-SPH, 100 device steps
     # against the float64 oracle's
     from oracle import oracle
