@@ -280,7 +280,7 @@ __device__ __forceinline__ void addEnergy(const Params &P, const Frame &F, int i
 __device__ __forceinline__ int cellCoordinate(double value, double origin, double width, int count)
 {
     double f = floor((value - origin) / width);
-    if (f < 0.0) return 0;
+    if (!(f >= 0.0)) return 0;      // below the grid, or not a number: never an index outside it
     if (f > (double)(count - 1)) return count - 1;
     return (int)f;
 }
