@@ -60,6 +60,8 @@ __global__ void __launch_bounds__(kBlock) listKernel(Params P, Frame F, const Co
     const unsigned lower = (1u << t) - 1u;
     const float4 Ai = __ldg(&F.pa[i]), Bi = __ldg(&F.pb[i]);
     const float hI = fabsf(signedLengthIn<D>(Ai, Bi));
+    // a boundary row holds its fluid neighbours only (forEachNeighbour says why)
+    const bool fluidOnly = signedLengthIn<D>(Ai, Bi) <= 0.0f;
     float pi[3], li[3];
     pointIn<D>(Ai, pi);
     remainderIn<D>(Ai, Bi, li);
@@ -119,7 +121,8 @@ __global__ void __launch_bounds__(kBlock) listKernel(Params P, Frame F, const Co
                         const float4 A = __ldg(&F.pa[j]);
                         float pj[3];
                         pointIn<D>(A, pj);
-                        const float coarse = coarseDistance2<D>(pi, pj, offset);
+                        const bool inRow = !fluidOnly || (D == 3 ? A.w > 0.0f : __ldg(&F.fluid[j]) != 0);
+                        const float coarse = inRow ? coarseDistance2<D>(pi, pj, offset) : searchLimit;
                         if (coarse < searchLimit) {
                             const float4 B = (D == 3 && PRECISE) || MIXED ? __ldg(&F.pb[j]) : A;
                             float r2 = coarse;      // the float32 points' separation is the coarse one
@@ -168,6 +171,7 @@ struct BatchMember {
     float pi[3], li[3];
     float hI, limit, fineLimit, offset;
     int slot, seam;
+    int fluidOnly;          // a boundary member: its row holds fluid neighbours only
     int runA, runB;         // this row's run of candidates for the member, [runA, runB)
 };
 
@@ -223,8 +227,14 @@ __global__ void __launch_bounds__(kBlock) cellListKernel(Params P, Frame F, cons
             m.offset = (float)shiftp;
             m.slot = i;
             m.seam = seamp ? 1 : 0;
+            m.fluidOnly = signedLengthIn<D>(Ai, Bi) <= 0.0f ? 1 : 0;
         }
         const bool anySeam = __any_sync(0xFFFFFFFFu, seamp);
+        // the batch's boundary members, whose rows hold fluid neighbours only: a mask in a register for
+        // one smoothing length; with mixed lengths the register costs more than the shared-memory
+        // read it saves (measured), so that form reads each member's flag
+        const unsigned boundaryMembers =
+            MIXED ? 0u : __ballot_sync(0xFFFFFFFFu, lane < count && mine[lane < count ? lane : 0].fluidOnly);
         int counted[kBatch];
 #pragma unroll
         for (int p = 0; p < kBatch; ++p) counted[p] = 0;
@@ -295,12 +305,14 @@ __global__ void __launch_bounds__(kBlock) cellListKernel(Params P, Frame F, cons
                         const bool valid = j < uB;
                         float4 A = make_float4(0, 0, 0, 0), B = A;
                         float pj[3] = {0, 0, 0}, lj[3] = {0, 0, 0}, hJ = 0.0f;
+                        bool fluidJ = false;
                         if (valid) {
                             A = __ldg(&F.pa[j]);
                             pointIn<D>(A, pj);
                             if ((D == 3 && PRECISE) || MIXED) B = __ldg(&F.pb[j]);
                             if (PRECISE) remainderIn<D>(A, D == 3 ? B : A, lj);
                             if (MIXED) hJ = fabsf(signedLengthIn<D>(A, B));
+                            fluidJ = D == 3 ? A.w > 0.0f : __ldg(&F.fluid[j]) != 0;
                         }
 #pragma unroll
                         for (int p = 0; p < kBatch; ++p) {
@@ -310,7 +322,8 @@ __global__ void __launch_bounds__(kBlock) cellListKernel(Params P, Frame F, cons
                             if (ra >= rb || rb <= base || ra >= base + 32) continue;     // the whole warp
                             if (image && !m.seam) continue;
                             bool accepted = false;
-                            if (valid && j >= ra && j < rb && j != m.slot) {
+                            const bool boundaryMember = MIXED ? m.fluidOnly != 0 : ((boundaryMembers >> p) & 1u) != 0;
+                            if (valid && j >= ra && j < rb && j != m.slot && (fluidJ || !boundaryMember)) {
                                 const float offset = image ? m.offset : 0.0f;
                                 const float coarse = coarseDistance2<D>(m.pi, pj, offset);
                                 if (coarse < (level ? m.fineLimit : m.limit)) {
@@ -368,6 +381,8 @@ template <int D, int K>
 struct ShepardVisit {
     static constexpr bool kSkipCoincident = false;
     static constexpr bool kKinetic = false;
+    static constexpr bool kBoundaryRows = true;
+    static constexpr bool kWholeBoundaryRows = true;    // the host-step call returns boundary rows too
     const Frame &F;
     Smoothing<K, D> S;
     float num, den;
@@ -425,6 +440,7 @@ template <int D, int K>
 struct WallVisit {
     static constexpr bool kSkipCoincident = false;
     static constexpr bool kKinetic = true;
+    static constexpr bool kBoundaryRows = true;         // it runs boundary rows only
     const Params &P; const Frame &F;
     Smoothing<K, D> S;
     float weight, total;
@@ -854,6 +870,7 @@ template <int D, int K, bool BUDGET>
 struct ContinuityVisit {
     static constexpr bool kSkipCoincident = true;
     static constexpr bool kKinetic = true;
+    static constexpr bool kBoundaryRows = true;         // every row
     const Params &P; const Frame &F;
     Smoothing<K, D> S;
     bool boundaryI, diffuses, corrected;

@@ -30,6 +30,8 @@
 // keeps.  The table marks such pairs in the entry's top bit.
 #pragma once
 
+#include <type_traits>
+
 #include "sph_internal.cuh"
 
 namespace sph {
@@ -214,10 +216,36 @@ struct Candidates {
 // image, pb row of j, kin row of j when Visitor::kKinetic) when Visitor::accept(fluidJ), and
 // r >= 1e-12 where Visitor::kSkipCoincident.
 // useTable: false forces the walk (the table kernel itself).
+// A boundary particle's row holds its fluid neighbours only: every sweep that reads boundary rows
+// takes fluid neighbours alone (the wall pressure, continuity), except a visitor that says
+// kWholeBoundaryRows (the Shepard sum, whose boundary rows the host-step call returns), which walks
+// a boundary row's cells for all of them.
+template <class V, class = void>
+struct WholeBoundaryRows {
+    static constexpr bool value = false;
+};
+template <class V>
+struct WholeBoundaryRows<V, std::void_t<decltype(V::kWholeBoundaryRows)>> {
+    static constexpr bool value = V::kWholeBoundaryRows;
+};
+// Whether a sweep walks boundary rows at all (kBoundaryRows); the others run fluid rows only and
+// skip the row's kind at compile time.
+template <class V, class = void>
+struct BoundaryRows {
+    static constexpr bool value = false;
+};
+template <class V>
+struct BoundaryRows<V, std::void_t<decltype(V::kBoundaryRows)>> {
+    static constexpr bool value = V::kBoundaryRows;
+};
+
 template <int D, int T, bool FINE, class Visitor>
 __device__ __forceinline__ void forEachNeighbour(const Params &P, const Frame &F, int i, int t, float hI,
                                                  Visitor &visit, bool useTable = true)
 {
+    const bool boundaryRow = BoundaryRows<Visitor>::value && signedLength<D>(F, i) <= 0.0f;
+    const bool wholeRow = WholeBoundaryRows<Visitor>::value && boundaryRow;
+    const bool fluidOnly = boundaryRow && !wholeRow;     // the row the table holds, in the walk too
     float pi[3], li[3];
     pointOf<D>(F, i, pi);
     remainderOf<D>(F, i, li);
@@ -238,8 +266,8 @@ __device__ __forceinline__ void forEachNeighbour(const Params &P, const Frame &F
     const double shift64 = O.shift64;
 
     Candidates<D, FINE> C;
-    const int count = useTable && P.listCap > 0 ? __ldg(&F.ncount[i]) : 0;
-    C.walking = !(useTable && P.listCap > 0 && count <= P.listCap);
+    const int count = useTable && P.listCap > 0 && !wholeRow ? __ldg(&F.ncount[i]) : 0;
+    C.walking = wholeRow || !(useTable && P.listCap > 0 && count <= P.listCap);
     if (!C.walking) {
         C.column = reinterpret_cast<const int4 *>(F.nbr) + i;
         C.stride = P.listStride;
@@ -264,6 +292,7 @@ __device__ __forceinline__ void forEachNeighbour(const Params &P, const Frame &F
         const float4 Kj = Visitor::kKinetic ? __ldg(&F.kin[j]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         const float hs = signedLengthIn<D>(A, B);
         const bool fluidJ = hs > 0.0f;
+        if (C.walking && fluidOnly && !fluidJ) continue;     // not in the row: not counted either
         // a lone lane may skip a rejected neighbour before its separation; a group counts every one
         if ((T == 1 || !C.walking) && !visit.accept(fluidJ)) continue;
         float lj[3];
