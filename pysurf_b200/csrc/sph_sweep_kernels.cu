@@ -404,7 +404,10 @@ __global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>()) shepardKernel(Par
     const Group<T> G = groupOf<T>();
     const int i = G.i;
     if (i >= P.n) return;
-    float hI = fabsf(signedLength<D>(F, i));
+    const float hs = signedLength<D>(F, i);
+    // a device step filters the fluid alone; the host-step call (no control block) returns every row
+    if (ctl && hs <= 0.0f) return;
+    float hI = fabsf(hs);
     // the particle itself first, as the reference's sums start (src/pysurf/sphGpu.py:781-783)
     float own = sigmaAt(P.sigmaUnit, hI, D);
     float mi = massOf<D>(F, i);
