@@ -215,7 +215,9 @@ int sph_split(SphSystem *sys, const uint8_t *mask, double reference_density, dou
  * place, and fluid from the end fills the places the others leave among the boundary's.  *groups
  * and *removed_energy (the members' kinetic energy about their centres of mass) come back, and
  * source, when not NULL, takes the caller index before the merge of each particle after (the new
- * count of entries, sph_count).  Refused with particle shifting on. */
+ * count of entries, sph_count).  Refused with particle shifting on.  When too few fluid particles follow
+ * the boundary in caller order to fill the places a merge leaves among it, the call fails
+ * (SPH_ERR_CUDA, as the reference raises) and the state is as it was. */
 int sph_merge(SphSystem *sys, const uint8_t *mask, double reference_density, double reference_mass,
               double length_ratio, int64_t *groups, double *removed_energy, int64_t *source);
 

@@ -74,7 +74,9 @@ struct MergeResultDevice {
     double removedEnergy;
     const char *error;
 };
-// 0, or -1 with out.error set; with no group found the state is untouched.
+// 0, or -1 with out.error set.  With no group found, or a failure before the merge itself (no
+// memory for the scratch, too few fluid particles after the boundary to fill its places), the state
+// is untouched.
 int runMerge(const MergeArgs &in, MergeResultDevice &out);
 // The counting sort's scratch: slotCell, slotWithin, perm (n entries), bucket (n pairs), cellCount
 // (numCells + 1 entries, all zero between sorts), partials (scanTiles(numCells + 1) entries).

@@ -126,17 +126,28 @@ __global__ void recordKernel(int nf, const int *order, const int *F, const int *
     taken[o] = 1;
 }
 
-// One group: its members in caller order; the merged particle into the first's slot.
+// One group's members in caller order (np.sort, axis 1), in place; all but the first go.
+__global__ void orderGroupsKernel(int groups, int size, int *members, uint8_t *gone)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= groups) return;
+    int o[kMaxGroup];
+    for (int k = 0; k < size; ++k) o[k] = members[(size_t)g * size + k];
+    for (int k = 1; k < size; ++k)
+        for (int q = k; q > 0 && o[q - 1] > o[q]; --q) { const int t = o[q]; o[q] = o[q - 1]; o[q - 1] = t; }
+    for (int k = 0; k < size; ++k) members[(size_t)g * size + k] = o[k];
+    for (int k = 1; k < size; ++k) gone[o[k]] = 1;
+}
+
+// One group (its members in caller order): the merged particle into the first's slot.
 __global__ void groupsKernel(int groups, int size, int dim, const int *members, const int *slotOf, MasterView M,
-                             float4 *acc, double lengthRatio, double *removed, uint8_t *gone, float *mergedPressure,
+                             float4 *acc, double lengthRatio, double *removed, float *mergedPressure,
                              const float *pres, double *energy, int energyStride, int energyTerms)
 {
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= groups) return;
     int o[kMaxGroup], s[kMaxGroup];
     for (int k = 0; k < size; ++k) o[k] = members[(size_t)g * size + k];
-    for (int k = 1; k < size; ++k)          // the members in caller order (np.sort, axis 1)
-        for (int q = k; q > 0 && o[q - 1] > o[q]; --q) { const int t = o[q]; o[q] = o[q - 1]; o[q - 1] = t; }
     for (int k = 0; k < size; ++k) s[k] = slotOf[o[k]];
     double total = 0.0, volume = 0.0, length = 0.0;
     for (int k = 0; k < size; ++k) {
@@ -178,7 +189,6 @@ __global__ void groupsKernel(int groups, int size, int dim, const int *members, 
     M.h[first] = length / size / lengthRatio;
     acc[first] = make_float4((float)a[0], (float)a[1], (float)a[2], 0.0f);
     mergedPressure[o[0]] = (float)p;
-    for (int k = 1; k < size; ++k) gone[o[k]] = 1;
     if (energy) {
         // the members' running energy totals go with the merged particle
         for (int t = 0; t < energyTerms; ++t) {
@@ -390,24 +400,21 @@ int runMerge(const MergeArgs &in, MergeResultDevice &out)
     }
     if (groups == 0) return 0;
 
-    // the merged particles
-    double *removed = scratch.get<double>(groups), *energyOld = nullptr;
+    // everything the rest needs, before anything of the state changes: a failure from here to the
+    // merge itself (no memory, too few fluid particles to fill the boundary's places) leaves it whole
+    double *removed = scratch.get<double>(groups);
+    double *energyOld = in.energy ? scratch.get<double>((size_t)in.energyTerms * in.energyStride) : nullptr;
     float *mergedPressure = scratch.get<float>(n);
-    MERGE_NEED(removed && mergedPressure);
-    fillFloatKernel<<<blocks(n, 256), 256, 0, st>>>(n, mergedPressure, nanf(""));
-    groupsKernel<<<blocks(groups, 128), 128, 0, st>>>(groups, size, dim, members, slotOf, in.master, in.acc,
-                                                       in.lengthRatio, removed, gone, mergedPressure, in.pres,
-                                                       in.energy, in.energyStride, in.energyTerms);
-    MERGE_TRY(cudaGetLastError());
-    std::vector<double> perGroup(groups);
-    if (download(perGroup.data(), removed, groups, st)) { out.error = "merge: removed energy"; return -1; }
-    for (double e : perGroup) out.removedEnergy += e;
-
-    // the compaction in caller order
     int *hole = scratch.get<int>(n), *holeRank = scratch.get<int>(n), *tail = scratch.get<int>(n),
         *tailRank = scratch.get<int>(n), *alive = scratch.get<int>(n), *newIndex = scratch.get<int>(n),
         *newCaller = scratch.get<int>(n), *holeOf = scratch.get<int>(n), *moverOf = scratch.get<int>(n);
-    MERGE_NEED(hole && holeRank && tail && tailRank && alive && newIndex && newCaller && holeOf && moverOf);
+    int *perm = scratch.get<int>(n), *kept = scratch.get<int>(1);
+    float4 *accNew = scratch.get<float4>(n);
+    MERGE_NEED(removed && (energyOld || !in.energy) && mergedPressure && hole && holeRank && tail && tailRank &&
+               alive && newIndex && newCaller && holeOf && moverOf && perm && kept && accNew);
+    orderGroupsKernel<<<blocks(groups, 128), 128, 0, st>>>(groups, size, members, gone);
+
+    // the compaction in caller order
     holesKernel<<<blocks(n, 256), 256, 0, st>>>(n, gone, lastBoundary, hole, tail);
     size_t bytes = tempBytes;
     MERGE_TRY(cub::DeviceScan::ExclusiveSum(temp, bytes, hole, holeRank, n, st));
@@ -437,10 +444,17 @@ int runMerge(const MergeArgs &in, MergeResultDevice &out)
     MERGE_TRY(cudaMemsetAsync(newCaller, 0xFF, sizeof(int) * n, st));
     renumberKernel<<<blocks(n, 256), 256, 0, st>>>(n, hole, holeRank, moverOf, alive, newIndex, newCaller, in.source);
 
+    // the merged particles, into their groups' first slots
+    fillFloatKernel<<<blocks(n, 256), 256, 0, st>>>(n, mergedPressure, nanf(""));
+    groupsKernel<<<blocks(groups, 128), 128, 0, st>>>(groups, size, dim, members, slotOf, in.master, in.acc,
+                                                       in.lengthRatio, removed, mergedPressure, in.pres,
+                                                       in.energy, in.energyStride, in.energyTerms);
+    MERGE_TRY(cudaGetLastError());
+    std::vector<double> perGroup(groups);
+    if (download(perGroup.data(), removed, groups, st)) { out.error = "merge: removed energy"; return -1; }
+    for (double e : perGroup) out.removedEnergy += e;
+
     // the master into its new order: the surviving slots, in slot order, gathered
-    int *perm = scratch.get<int>(newCount), *kept = scratch.get<int>(1);
-    float4 *accNew = scratch.get<float4>(newCount);
-    MERGE_NEED(perm && kept && accNew);
     survivorsKernel<<<blocks(n, 256), 256, 0, st>>>(n, in.master.orig, newCaller, flag);
     bytes = tempBytes;
     MERGE_TRY(cub::DeviceSelect::Flagged(temp, bytes, callers, flag, perm, kept, n, st));
@@ -451,8 +465,6 @@ int runMerge(const MergeArgs &in, MergeResultDevice &out)
                                                               in.nextFrame.pres, perm, in.acc, accNew);
     MERGE_TRY(cudaMemcpyAsync(in.acc, accNew, sizeof(float4) * newCount, cudaMemcpyDeviceToDevice, st));
     if (in.energy) {
-        energyOld = scratch.get<double>((size_t)in.energyTerms * in.energyStride);
-        MERGE_NEED(energyOld);
         MERGE_TRY(cudaMemcpyAsync(energyOld, in.energy, sizeof(double) * in.energyTerms * in.energyStride,
                                   cudaMemcpyDeviceToDevice, st));
         MERGE_TRY(cudaMemsetAsync(in.energy, 0, sizeof(double) * in.energyTerms * in.energyStride, st));

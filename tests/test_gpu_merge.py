@@ -108,3 +108,30 @@ def test_a_split_step_merge_step_run_follows_the_oracle():
     assert time == pytest.approx(stepper.time, rel=1e-4)
     assert np.abs(out['positions'] - ref['positions']).max() < 1e-6
     assert np.abs(out['velocities'] - ref['velocities']).max() < 1e-3
+
+
+def test_a_merge_that_cannot_fill_the_boundarys_places_fails_and_changes_nothing():
+    # src/pysurf/sphRefinement.py:296-297 raises when too few fluid particles follow the boundary to
+    # fill the places a merge leaves among it; here every daughter stands before the boundary
+    from pysurf_b200 import _lib
+    from pysurf_b200.sphGpu import PairSums
+    s, rho0 = 0.05, 1000.0
+    referenceMass = rho0 * s * s
+    axes = np.arange(16) * 0.5 * s + 0.25 * s
+    daughters = np.stack(np.meshgrid(axes, axes, indexing='ij'), axis=-1).reshape(-1, 2) + 0.3
+    wall = np.stack([np.linspace(0.0, 1.5, 40), np.zeros(40)], axis=1)
+    n = len(daughters) + len(wall)
+    state = ParticleState(np.vstack([daughters, wall]), np.zeros((n, 2)), np.zeros((n, 2)), np.full(n, rho0),
+                          np.zeros(n), np.full(n, referenceMass / 4), np.r_[np.ones(len(daughters), bool),
+                                                                           np.zeros(len(wall), bool)],
+                          np.full(n, 0.65 * s))
+    x = state.positions
+    sums = PairSums(2, 1.3 * s, x.min(axis=0) - 0.1, x.max(axis=0) + 0.1, device='cuda:0')
+    sums.push(state)
+    before = sums.pullState()
+    with pytest.raises(_lib.SphError):
+        sums.merge(np.ones(n, dtype=bool), rho0, referenceMass, 0.5)
+    after = sums.pullState()
+    assert sums.count == n
+    for name in ('positions', 'velocities', 'densities', 'masses', 'lengths', 'isFluid'):
+        assert np.array_equal(after[name], before[name]), name
