@@ -113,6 +113,32 @@ __device__ __forceinline__ float support2(float h)
     return __fmul_rn(w, w);
 }
 
+// A squared distance under which the coarse test's float32 points alone decide a pair at one
+// smoothing length: a coarse r^2 below it leaves the precise r^2 (separation2, points plus
+// remainders, not across the seam) below `support`.  The frame's remainders are the float32 rest
+// of each float64 coordinate, |l| <= 2^-24 |x| (gatherKernel), so each axis of the separation
+// moves by at most 6e-8 (|p_i| + |p_j|) over the points' difference, and a candidate under the
+// bound has |p_j| <= |p_i| + 2h per axis; 1e-5 of 2h covers the roundings of both distances and of
+// the bound itself (a few float32 roundings).  So a table built with it holds the same entries.
+__device__ __forceinline__ float sureSupport2(float support, const float pi[3])
+{
+    const float s = sqrtf(support);
+    const float spread = 6.0e-8f * (2.0f * (fabsf(pi[0]) + fabsf(pi[1]) + fabsf(pi[2])) + 3.0f * s) + 1.0e-37f;
+    const float edge = fmaxf(s * (1.0f - 1.0e-5f) - spread, 0.0f);
+    return edge * edge;
+}
+
+// The table kernels' bound for a particle of length hI at point pi: sureSupport2 of the support its
+// coarse-grid candidates share.  One smoothing length: (2 h)^2.  Two grid levels: every particle on
+// the coarse grid has h >= P.fineBelow, so its float32 length is at least P.hMax and each pair's
+// support is at least that of (hI + P.hMax) / 2 (the roundings are monotone); the fine grid's
+// candidates take the precise test.  Mixed lengths on one grid: none (0).
+__device__ __forceinline__ float sureBound(const Params &P, float support, float hI, const float pi[3])
+{
+    if (P.mixedH) return P.levels > 1 ? sureSupport2(support2(0.5f * (hI + P.hMax)), pi) : 0.0f;
+    return sureSupport2(support, pi);
+}
+
 // What a walk needs to set up each of a particle's searches: its sorted cell, point, remainder,
 // length, and the periodic image's shift when it lies near the seam.
 struct Origin {
