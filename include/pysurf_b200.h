@@ -147,7 +147,8 @@ int sph_density_gradients(SphSystem *sys, const double *densities, double *out);
 
 /* ---- Device-resident steps (the state lives on the device between push and pull) --------- */
 
-/* PairSums.push (src/pysurf/sphGpu.py:2207-2221): the whole state, caller order. */
+/* PairSums.push (src/pysurf/sphGpu.py:2207-2221): the whole state, caller order.  Returns once the
+ * host arrays have been read; the device's own work on them follows in stream order. */
 int sph_push(SphSystem *sys, int64_t n, const double *positions, const double *velocities, const double *densities,
              const double *masses, const uint8_t *is_fluid, const double *lengths);
 /* PairSums.pull (src/pysurf/sphGpu.py:2223-2235): any output may be NULL.  masses, lengths and

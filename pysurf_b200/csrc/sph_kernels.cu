@@ -326,12 +326,25 @@ __global__ void stepEndKernel(Control *ctl)
 }
 
 // Caller-order float64 rows from the sorted master or frame.
-__global__ void scatterDoubleKernel(int n, int dim, const int *orig, const double *const *columns, double *out)
+// A pull's fields in one pass, so the copies out follow one launch.
+template <int D>
+__global__ void pullKernel(int n, MasterView M, Frame F, const float4 *acc, PullRows R)
 {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= n) return;
-    int o = orig[s];
-    for (int a = 0; a < dim; ++a) out[o * dim + a] = columns[a][s];
+    const size_t o = (size_t)M.orig[s];
+    if (R.x) for (int a = 0; a < D; ++a) R.x[o * D + a] = M.x[a][s];
+    if (R.v) for (int a = 0; a < D; ++a) R.v[o * D + a] = M.v[a][s];
+    if (R.rho) R.rho[o] = M.rho[s];
+    if (R.m) R.m[o] = M.m[s];
+    if (R.h) R.h[o] = M.h[s];
+    if (R.p) R.p[o] = (double)pressureOf<D>(F, s);
+    if (R.a) {
+        const float4 q = acc[s];
+        const float c[3] = {q.x, q.y, q.z};
+        for (int a = 0; a < D; ++a) R.a[o * D + a] = (double)c[a];
+    }
+    if (R.fluid) R.fluid[o] = M.fluid[s];
 }
 
 __global__ void scatterFloat4Kernel(int n, int dim, const int *orig, const float4 *values, double *out)
@@ -594,10 +607,12 @@ void launchRefreshDensity(int n, const double *rho, float *out, cudaStream_t st)
     refreshDensityKernel<<<blocksFor(n, 256), 256, 0, st>>>(n, rho, out);
 }
 
-void launchScatterDouble(int n, int dim, const int *orig, const double *const *columns, double *out, cudaStream_t st)
+void launchPull(int n, int dim, const MasterView &M, const Frame &F, const float4 *acc, const PullRows &R,
+                cudaStream_t st)
 {
     if (n == 0) return;
-    scatterDoubleKernel<<<blocksFor(n, 256), 256, 0, st>>>(n, dim, orig, columns, out);
+    if (dim == 2) pullKernel<2><<<blocksFor(n, 256), 256, 0, st>>>(n, M, F, acc, R);
+    else pullKernel<3><<<blocksFor(n, 256), 256, 0, st>>>(n, M, F, acc, R);
 }
 
 void launchScatterFloat4(int n, int dim, const int *orig, const float4 *values, double *out, cudaStream_t st)

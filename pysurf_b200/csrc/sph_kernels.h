@@ -102,7 +102,14 @@ void launchColumnSums(const double *columns, long long stride, int n, int count,
 // Each slot's kinetic, potential and elastic energy (zero on the boundary) into three columns.
 void launchFluidEnergy(const Params &P, const Frame &F, double *columns, long long stride, cudaStream_t st);
 void launchRefreshDensity(int n, const double *rho, float *out, cudaStream_t st);
-void launchScatterDouble(int n, int dim, const int *orig, const double *const *columns, double *out, cudaStream_t st);
+// The fields a pull asks for, each into its own caller-order rows (null: not asked for).
+struct PullRows {
+    double *x, *v, *rho, *m, *h, *p, *a;
+    uint8_t *fluid;
+};
+// Every asked field in one pass: slot s to caller place M.orig[s]; p from the frame, a from acc.
+void launchPull(int n, int dim, const MasterView &M, const Frame &F, const float4 *acc, const PullRows &R,
+                cudaStream_t st);
 void launchScatterFloat4(int n, int dim, const int *orig, const float4 *values, double *out, cudaStream_t st);
 void launchScatterFloat(int n, const int *orig, const float *values, double *out, cudaStream_t st);
 // Caller-order float32 positions (n x dim), float32 speeds and fluid flags of every particle.

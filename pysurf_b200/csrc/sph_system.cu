@@ -152,9 +152,8 @@ struct SphSystem {
     Control *ctl = nullptr;
     // Caller-order float64 staging on the device, kStageSlots rows of capacity doubles:
     //   inputs   0-2 vectors, 3 densities, 4 pressures (loadState: 0-2 x, 3-5 v, 6 rho, 7 m, 8 h)
-    //   outputs  5-13 (up to dim x dim per particle)
-    //   15       a small table of device pointers
-    static constexpr int kStageSlots = 16;
+    //   outputs  5-13 (up to dim x dim per particle); a pull's fields 0-12
+    static constexpr int kStageSlots = 14;
     static constexpr int kOutSlot = 5;
     double *dStage = nullptr;
     uint8_t *dStageU8 = nullptr;
@@ -184,6 +183,7 @@ struct SphSystem {
     long long beginStep = 0;
     long long enqueued = 0;
     cudaEvent_t evStart = nullptr, evStop = nullptr;
+    cudaEvent_t uploaded = nullptr;     // after a load's copies in, before the kernels that read them
     double lastAdvanceMs = 0.0;
 
     // ---- memory ------------------------------------------------------------------------------
@@ -286,7 +286,7 @@ struct SphSystem {
         TRY(deviceAlloc(&sortBuffers.slotWithin, cap));
         TRY(deviceAlloc(&sortBuffers.perm, cap));
         TRY(deviceAlloc(&sortBuffers.bucket, cap));
-        TRY(deviceAlloc(&dStage, (size_t)kStageSlots * cap + 4));    // + the pointer table of a tiny capacity
+        TRY(deviceAlloc(&dStage, (size_t)kStageSlots * cap));
         TRY(deviceAlloc(&dStageU8, cap));
         TRY(deviceAlloc(&dRank, cap));
         TRY(deviceAlloc(&ncount, cap));
@@ -680,7 +680,8 @@ int sph_create(int dimensions, double smoothing_length, const double *domain_min
     s->ownStream = true;
     if (status == SPH_OK && cudaMalloc((void **)&s->ctl, sizeof(Control)) != cudaSuccess) status = SPH_ERR_NOMEM;
     if (status == SPH_OK && cudaMallocHost((void **)&s->hCtl, sizeof(Control)) != cudaSuccess) status = SPH_ERR_NOMEM;
-    if (status == SPH_OK && (cudaEventCreate(&s->evStart) != cudaSuccess || cudaEventCreate(&s->evStop) != cudaSuccess))
+    if (status == SPH_OK && (cudaEventCreate(&s->evStart) != cudaSuccess || cudaEventCreate(&s->evStop) != cudaSuccess ||
+                             cudaEventCreateWithFlags(&s->uploaded, cudaEventDisableTiming) != cudaSuccess))
         status = SPH_ERR_CUDA;
     for (int b = 0; b < 2 && status == SPH_OK; ++b)
         for (int k = 0; k <= kStageCount && status == SPH_OK; ++k)
@@ -723,6 +724,7 @@ int sph_destroy(SphSystem *sys)
     if (sys->hCtl) cudaFreeHost(sys->hCtl);
     if (sys->evStart) cudaEventDestroy(sys->evStart);
     if (sys->evStop) cudaEventDestroy(sys->evStop);
+    if (sys->uploaded) cudaEventDestroy(sys->uploaded);
     if (sys->ownStream && sys->stream) cudaStreamDestroy(sys->stream);
     delete sys;
     return SPH_OK;
@@ -963,6 +965,7 @@ static int loadState(SphSystem *sys, int64_t count, const double *positions, con
     TRY(sys->upload(sm, masses, sizeof(double) * n));
     if (lengths) TRY(sys->upload(sh, lengths, sizeof(double) * n));
     TRY(sys->upload(sys->dStageU8, is_fluid, n));
+    CUDA_TRY(cudaEventRecord(sys->uploaded, sys->stream));
     sys->cur = 0;
     launchLoadMaster(n, dim, sx, velocities ? sv : nullptr, densities ? srho : nullptr, sm, sys->dStageU8,
                      lengths ? sh : nullptr, sys->h, sys->master[0], sys->stream);
@@ -1228,7 +1231,9 @@ int sph_push(SphSystem *sys, int64_t n, const double *positions, const double *v
     if (sys->budget && sys->energy)
         CUDA_TRY(cudaMemsetAsync(sys->energy, 0, sizeof(double) * kEnergyTerms * sys->energyCap, sys->stream));
     CUDA_TRY(cudaGetLastError());
-    CUDA_TRY(cudaStreamSynchronize(sys->stream));
+    // the caller's arrays are free once the copies in are done; the kernels after them run on
+    // behind the return, in stream order before any later call's work
+    CUDA_TRY(sys->n > 0 ? cudaEventSynchronize(sys->uploaded) : cudaStreamSynchronize(sys->stream));
     return SPH_OK;
 }
 
@@ -1264,51 +1269,35 @@ int sph_pull(SphSystem *sys, double *positions, double *velocities, double *dens
     CHECK_SYS(sys);
     int n = sys->n, dim = sys->dim;
     if (n == 0) return SPH_OK;
-    const MasterView &M = sys->master[sys->cur];
-    // each field scattered into caller order in its own staging rows (0 .. 14; 15 holds the column
-    // pointers), copied out in stream order, and one sync at the end
+    // one launch puts every asked field into caller order in its own staging rows (0 .. 12), then
+    // the copies out follow in stream order, and one sync at the end
     int slot = 0;
-    auto rows = [&](int width) { double *p = sys->stage(slot); slot += width; return p; };
-    auto scatterColumns = [&](double *const *src, int width, double *host) -> int {
-        if (!host) return SPH_OK;
-        double *out = rows(width);
-        // the column pointers go to the device through the staging's last row; stream order keeps
-        // each launch's table until it has run
-        const double *ptrs[3] = {src[0], src[1], src[2]};
-        double **dptrs = (double **)sys->stage(15);
-        CUDA_TRY(cudaMemcpyAsync(dptrs, ptrs, sizeof(ptrs), cudaMemcpyHostToDevice, sys->stream));
-        launchScatterDouble(n, width, M.orig, (const double *const *)dptrs, out, sys->stream);
-        return sys->download(host, out, sizeof(double) * n * width);
+    auto rows = [&](const void *host, int width) -> double * {
+        if (!host) return nullptr;
+        double *p = sys->stage(slot);
+        slot += width;
+        return p;
     };
-    double *xcols[3] = {M.x[0], M.x[1], M.x[2]};
-    double *vcols[3] = {M.v[0], M.v[1], M.v[2]};
-    double *rcol[3] = {M.rho, nullptr, nullptr};
-    double *mcol[3] = {M.m, nullptr, nullptr};
-    double *hcol[3] = {M.h, nullptr, nullptr};
-    TRY(scatterColumns(xcols, dim, positions));
-    TRY(scatterColumns(vcols, dim, velocities));
-    TRY(scatterColumns(rcol, 1, densities));
-    TRY(scatterColumns(mcol, 1, masses));
-    TRY(scatterColumns(hcol, 1, lengths));
-    if (pressures && sys->framed) {
-        double *out = rows(1);
-        launchScatterPressure(n, dim, M.orig, sys->frame(), out, sys->stream);
-        TRY(sys->download(pressures, out, sizeof(double) * n));
-    }
-    if (accelerations) {
-        double *out = rows(dim);
-        launchScatterFloat4(n, dim, M.orig, sys->acc, out, sys->stream);
-        TRY(sys->download(accelerations, out, sizeof(double) * n * dim));
-    }
-    if (is_fluid) {
-        // fluid flags: gather through a float scatter of 0/1
-        std::vector<uint8_t> flags(n);
-        std::vector<int> orig(n);
-        CUDA_TRY(cudaMemcpyAsync(flags.data(), M.fluid, n, cudaMemcpyDeviceToHost, sys->stream));
-        CUDA_TRY(cudaMemcpyAsync(orig.data(), M.orig, sizeof(int) * n, cudaMemcpyDeviceToHost, sys->stream));
-        CUDA_TRY(cudaStreamSynchronize(sys->stream));
-        for (int s = 0; s < n; ++s) is_fluid[orig[s]] = flags[s];
-    }
+    PullRows R{};
+    R.x = rows(positions, dim);
+    R.v = rows(velocities, dim);
+    R.rho = rows(densities, 1);
+    R.m = rows(masses, 1);
+    R.h = rows(lengths, 1);
+    R.p = sys->framed ? rows(pressures, 1) : nullptr;
+    R.a = rows(accelerations, dim);
+    R.fluid = is_fluid ? sys->dStageU8 : nullptr;
+    launchPull(n, dim, sys->master[sys->cur], sys->frame(), sys->acc, R, sys->stream);
+    CUDA_TRY(cudaGetLastError());
+    const size_t column = sizeof(double) * (size_t)n;
+    if (R.x) TRY(sys->download(positions, R.x, column * dim));
+    if (R.v) TRY(sys->download(velocities, R.v, column * dim));
+    if (R.rho) TRY(sys->download(densities, R.rho, column));
+    if (R.m) TRY(sys->download(masses, R.m, column));
+    if (R.h) TRY(sys->download(lengths, R.h, column));
+    if (R.p) TRY(sys->download(pressures, R.p, column));
+    if (R.a) TRY(sys->download(accelerations, R.a, column * dim));
+    if (R.fluid) TRY(sys->download(is_fluid, R.fluid, (size_t)n));
     CUDA_TRY(cudaStreamSynchronize(sys->stream));
     CUDA_TRY(cudaGetLastError());
     return SPH_OK;
