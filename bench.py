@@ -64,6 +64,9 @@ def parseArgs():
                    help='solve this many cases of the seeded 256-case beach sweep to their breaking points, '
                         'case by case and then batched, and report both')
     p.add_argument('--slots', type=int, default=16, help='concurrent cases in the batched sweep and the server')
+    p.add_argument('--tune', action='store_true',
+                   help='batched sweep: pick each size class\'s cells per support and threads per particle by '
+                        'timing (the autotuner, its time counted in the batched run)')
     p.add_argument('--serve', type=int, default=0,
                    help='serve this many requests arriving as a Poisson stream (see serveBench)')
     p.add_argument('--horizon-scale', type=float, default=0.1,
@@ -307,25 +310,38 @@ def sweepBench(args) -> None:
     then --slots at a time; every batched result must equal its case-by-case one."""
     import numpy as np
     from pysurf_b200 import batch
+    from pysurf_b200 import tuning
     specs = batch.drawSweep(256, seed=0)[:args.sweep]
+    tuner = tuning.Autotuner() if args.tune else None
     runs = {}
-    for name, slots in (('case_by_case', 1), ('batched', args.slots)):
+    for name, slots, tune in (('case_by_case', 1, None), ('batched', args.slots, tuner)):
         start = time.perf_counter()
-        results = batch.BatchRunner(slots=slots).run(specs)
+        results = batch.BatchRunner(slots=slots, tuner=tune).run(specs)
         runs[name] = (time.perf_counter() - start, results)
     (serial, alone), (batched, mixed) = runs['case_by_case'], runs['batched']
-    same = all(a.key() == m.key() and a.error is None and m.error is None for a, m in zip(alone, mixed))
+    ok = all(a.error is None and m.error is None for a, m in zip(alone, mixed))
+    if tuner is None:
+        check = {'results_identical_alone_and_batched': ok and all(a.key() == m.key() for a, m in zip(alone, mixed))}
+    else:
+        # tuned choices add neighbours in another order: the breaking point, not the bits, must agree
+        def within(a, m):
+            if a.breakingTime != a.breakingTime:
+                return m.breakingTime != m.breakingTime
+            return (abs(m.breakingTime - a.breakingTime) <= 0.01 * a.breakingTime
+                    and abs(m.breakingCrestX - a.breakingCrestX) <= 0.01 * a.breakingCrestX)
+        check = {'breaking_within_1pct_of_default_case_by_case': ok and all(within(a, m) for a, m in zip(alone, mixed)),
+                 'tuned_classes': {k: vars(v) for k, v in sorted(tuner.choices.items())}}
     updates = sum(r.fluidParticles * r.steps for r in mixed)
     broke = sum(1 for r in mixed if r.breakingTime == r.breakingTime)
     seconds = np.array([r.seconds for r in mixed])
     line = {'metric': 'cases/h', 'value': 3600.0 * len(specs) / batched, 'unit': 'cases/h', 'n_gpus': 1,
             'higher_is_better': True, 'data': 'synthetic',
             'config': {'workload': f'the first {len(specs)} cases of the 256-case 2D beach sweep (seed 0), each to '
-                                   f'its breaking point', 'slots': args.slots,
+                                   f'its breaking point', 'slots': args.slots, 'autotuned': bool(args.tune),
                        'fluid_particles': [r.fluidParticles for r in mixed]},
             'case_by_case_cases_per_h': 3600.0 * len(specs) / serial, 'speedup': serial / batched,
             'seconds_batched': batched, 'seconds_case_by_case': serial, 'broke': broke,
-            'results_identical_alone_and_batched': same, 'particle_updates_per_s': updates / batched,
+            **check, 'particle_updates_per_s': updates / batched,
             'case_seconds_p50': float(np.percentile(seconds, 50)),
             'case_seconds_p99': float(np.percentile(seconds, 99))}
     print(json.dumps(line), flush=True)

@@ -85,15 +85,18 @@ def estimatedBytes(particles: int, dimensions: int = 2) -> int:
     return int(particles) * (BYTES_PER_PARTICLE_2D if dimensions == 2 else BYTES_PER_PARTICLE_3D) + (64 << 20)
 
 
-def solveCase(spec: CaseSpec, device: int = 0, clock=time.perf_counter, case=None) -> CaseResult:
+def solveCase(spec: CaseSpec, device: int = 0, clock=time.perf_counter, case=None, tuning=None) -> CaseResult:
     """One case on the device from its start to its breaking point (the tracker's, read on the
-    device every 0.01 sqrt(d / g)) or to its horizon."""
+    device every 0.01 sqrt(d / g)) or to its horizon, with the autotuner's `tuning` when one is given
+    (cells per support and threads per particle; the defaults otherwise)."""
     from pysurf_b200 import breaking, cases
     result = CaseResult(spec.index, spec, started=clock())
     try:
         case = case if case is not None else buildCase(spec)
         result.fluidParticles, result.particles = case.fluidCount, case.state.nParticles
         sums = cases.pairSumsFor(case, device=device)
+        if tuning is not None:
+            tuning.apply(sums)
         state = case.state.copy()
         sums.push(state)
         sums.setBoundary(case.boundary, state)
@@ -144,13 +147,17 @@ def deviceBudget(device: int = 0, share: float = 0.8) -> int:
 @dataclass
 class BatchRunner:
     """Cases in `slots` concurrent slots on one device, each admitted when a slot is free and its
-    estimated memory fits the budget."""
+    estimated memory fits the budget.  With a `tuner`, every size class among the cases is tuned
+    before the first case starts, and each case runs with its class's choice."""
     slots: int = 16
     device: int = 0
     budget: int | None = None
+    tuner: object = None
     results: list = field(default_factory=list)
 
     def run(self, specs: list[CaseSpec], builder=buildCase) -> list[CaseResult]:
+        if self.tuner is not None:
+            self.tuner.prepare(specs, builder)
         gate = MemoryGate(self.budget if self.budget is not None else deviceBudget(self.device))
         start = time.perf_counter()
         clock = lambda: time.perf_counter() - start     # noqa: E731
@@ -158,9 +165,10 @@ class BatchRunner:
         def one(spec):
             case = builder(spec)
             need = estimatedBytes(case.state.nParticles, case.dimensions)
+            tuning = self.tuner.choose(case) if self.tuner is not None else None
             gate.acquire(need)
             try:
-                return solveCase(spec, self.device, clock, case)
+                return solveCase(spec, self.device, clock, case, tuning)
             finally:
                 gate.release(need)
 
@@ -176,11 +184,14 @@ class Request:
     builder: object = None          # builds the request's case; None for a beach from the spec
 
 
-def serve(requests: list[Request], slots: int = 16, device: int = 0, budget: int | None = None) -> dict:
+def serve(requests: list[Request], slots: int = 16, device: int = 0, budget: int | None = None,
+          tuner=None) -> dict:
     """Serve a stream of requests: each is admitted at its arrival, or later when a slot and memory
     are free, and solved beside the others in flight (continuous batching: a request that arrives
-    while others run joins them as soon as it can).  Returns the results with each request's
-    latency from arrival to result, and the stream's p50/p99 latency and throughput."""
+    while others run joins them as soon as it can).  A `tuner` supplies each request's choice from
+    the classes it was prepared for (it does not time while the stream runs).  Returns the results
+    with each request's latency from arrival to result, and the stream's p50/p99 latency and
+    throughput."""
     gate = MemoryGate(budget if budget is not None else deviceBudget(device))
     start = time.perf_counter()
     clock = lambda: time.perf_counter() - start     # noqa: E731
@@ -193,9 +204,10 @@ def serve(requests: list[Request], slots: int = 16, device: int = 0, budget: int
             time.sleep(wait)
         case = (request.builder or buildCase)(request.spec)
         need = estimatedBytes(case.state.nParticles, case.dimensions)
+        tuning = tuner.choose(case) if tuner is not None else None
         gate.acquire(need)
         try:
-            result = solveCase(request.spec, device, clock, case)
+            result = solveCase(request.spec, device, clock, case, tuning)
         finally:
             gate.release(need)
         with lock:
