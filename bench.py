@@ -75,13 +75,13 @@ def parseArgs():
                    help='split the crest zone (surface above 0.3 H) into daughters of h/2 before timing')
     p.add_argument('--options', default='',
                    help='opt-in parts of the step, comma separated: closure (delta-LES-SPH), shifting, energy '
-                        '(the energy budget)')
+                        '(the energy budget), compensated (compensated momentum and continuity sums)')
     p.add_argument('--no-e2e', action='store_true')
     p.add_argument('--no-cpu', action='store_true')
     return p.parse_args()
 
 
-OPTIONS = ('closure', 'shifting', 'energy')
+OPTIONS = ('closure', 'shifting', 'energy', 'compensated')
 
 
 def buildCase(args):
@@ -94,6 +94,7 @@ def buildCase(args):
     case.turbulenceClosure = 'deltaLes' if 'closure' in options else case.turbulenceClosure
     case.particleShifting = 'shifting' in options or case.particleShifting
     case.trackEnergy = 'energy' in options or case.trackEnergy
+    case.compensatedSums = 'compensated' in options or case.compensatedSums
     case.info['options'] = options
     return case
 
@@ -111,7 +112,9 @@ def config(case, flush: bool = True) -> dict:
         extent = {'tank_d': info['tank']}
     if info.get('options'):
         workload += ', with ' + ' and '.join({'closure': 'the delta-LES-SPH closure', 'shifting': 'particle shifting',
-                                               'energy': 'the energy budget'}[o] for o in info['options'])
+                                               'energy': 'the energy budget',
+                                               'compensated': 'compensated momentum and continuity sums'}[o]
+                                              for o in info['options'])
     return {'workload': workload, 'particles_per_depth': info['ppd'], 'fluid_particles': case.fluidCount,
             'boundary_particles': int(case.state.nParticles - case.fluidCount), 'boundary_layers': info['layers'],
             'smoothing_length_over_dx': round(case.smoothingLength / case.spacing, 6), **extent,

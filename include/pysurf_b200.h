@@ -100,6 +100,14 @@ int sph_shifting_displacement(SphSystem *sys, const double *densities, double ti
  * budget (src/pysurf/sphEnergy.py): each fluid particle's running total of every term from the last
  * sph_push, 120 bytes a particle more while it is on. */
 int sph_set_energy_budget(SphSystem *sys, int enabled);
+/* Compensated momentum and continuity sums (no method of PairSums: the reference's float32 Warp
+ * sums are plain, src/pysurf/sphGpu.py:400-414, 476-545; its float64 numpy path is the accuracy they
+ * approach).  When on, each thread's share of a particle's du/dt and drho/dt is accumulated with its
+ * running rounding error (the Dot2 scheme of Ogita, Rump and Oishi, 2005) and the threads' shares
+ * combine the same way, so the sums lose no digits to their length; the terms keep their float32
+ * arithmetic.  Off by default.  SPH_ERR_UNSUPPORTED with the energy budget on (its sweeps keep
+ * plain sums). */
+int sph_set_compensated_sums(SphSystem *sys, int enabled);
 /* PairSums.energySums (src/pysurf/sphGpu.py:1805-1825): each term's energy [J] over the device steps
  * since sph_push, summed over the particles in caller order, into sums[14], in the order pressureFluid,
  * viscosityFluid, pressureWall, viscosityWall, gravityWork, continuityFluid, continuityWall,

@@ -78,6 +78,7 @@ SIGNATURES = {
     'sph_set_shifting': [_h, _i, _d, _d, _d, _i],
     'sph_shifting_displacement': [_h, _pd, _d, _pd, _pd, _pd, _pd],
     'sph_set_energy_budget': [_h, _i],
+    'sph_set_compensated_sums': [_h, _i],
     'sph_energy_sums': [_h, _pd],
     'sph_fluid_energy': [_h, _pd],
     'sph_closure_coefficients': [_h, _pd, _pd, _pd, _pd],

@@ -60,6 +60,7 @@ class Case:
     shiftingMach: float = 0.1
     shiftingLocal: bool = False
     trackEnergy: bool = False         # the device steps keep the energy budget (src/pysurf/sphEnergy.py)
+    compensatedSums: bool = False     # the momentum and continuity sums carry their rounding error
     kinematicViscosity: float = 1.0034e-6     # src/pysurf/constants.py:35, the closure's water term
     info: dict = field(default_factory=dict)
 
@@ -416,6 +417,8 @@ def pairSumsFor(case: Case, cellsPerSupport: int | None = None, device: int = 0)
                     case.kinematicViscosity)
     sums.setShifting(case.particleShifting, case.shiftingMach, case.spacing, case.soundSpeed, case.shiftingLocal)
     sums.setEnergyBudget(case.trackEnergy)
+    if case.compensatedSums:
+        sums.setCompensatedSums(True)
     sums.setPhysics(case.referenceDensity, case.soundSpeed, case.alpha, case.boundaryViscosityFactor, case.gravity,
                     case.xsphEpsilon, case.densityFloor)
     return sums

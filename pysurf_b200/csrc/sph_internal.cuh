@@ -111,6 +111,8 @@ struct Params {
     // index, column t at t * energyStride; the momentum sweep's parts of a at q * energyStride + slot
     int budget;
     int energyStride;
+    // the momentum and continuity sums compensated (never with the budget: its sweeps keep plain sums)
+    int compensated;
 };
 
 // The float32 frame and the float64 master state, current buffers.

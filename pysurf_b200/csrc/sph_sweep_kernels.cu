@@ -608,8 +608,9 @@ gradientKernel(Params P, Frame F, const Control *ctl, int wantG, int wantL, int 
 // ------------------------------------------------------------------------------------------
 
 // BUDGET: the sum split for the energy budget too, into the pressure and the viscosity of fluid
-// and of boundary neighbours (src/pysurf/sphGpu.py:400-414).
-template <int D, int K, bool BUDGET>
+// and of boundary neighbours (src/pysurf/sphGpu.py:400-414).  COMP: the sum compensated (Dot2),
+// its running error in comp.
+template <int D, int K, bool BUDGET, bool COMP = false>
 struct MomentumVisit {
     static constexpr bool kSkipCoincident = true;
     static constexpr bool kKinetic = true;
@@ -619,6 +620,7 @@ struct MomentumVisit {
     float alphaI;                               // closure: this particle's eddy alpha
     float Gi[3][3];
     float total[3];
+    float comp[COMP ? 3 : 1];
     float parts[BUDGET ? 4 : 1][3];
     __device__ bool accept(bool) const { return true; }
     __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int, const float4 &B,
@@ -678,7 +680,11 @@ struct MomentumVisit {
         const float pressureTerm = __fadd_rn(own, ratioJ);
         float coefficient = -__fadd_rn(pressureTerm, viscosity) * massIn<D>(B);
         float f = coefficient * kernelGradient<K>(q, k);
-        for (int a = 0; a < D; ++a) total[a] = __fmaf_rn(f, d[a], total[a]);
+        if constexpr (COMP) {
+            for (int a = 0; a < D; ++a) addProduct(f, d[a], total[a], comp[a]);
+        } else {
+            for (int a = 0; a < D; ++a) total[a] = __fmaf_rn(f, d[a], total[a]);
+        }
         if constexpr (BUDGET) {
             const float grad = massIn<D>(B) * kernelGradient<K>(q, k);
             const float fp = -pressureTerm * grad, fv = -viscosity * grad;
@@ -734,7 +740,7 @@ __device__ __forceinline__ void foldMaxima(Control *ctl, double speed, double ac
 
 // maxima: fold the fluid maxima into ctl and take the time step (the device steps); 0 for the
 // host-step sums.
-template <int D, int K, int T, bool BUDGET, bool FINE>
+template <int D, int K, int T, bool BUDGET, bool FINE, bool COMP = false>
 __global__ void __launch_bounds__(kBlock, BUDGET ? budgetMinBlocks<D>() : sweepMinBlocks<D>())
 momentumKernel(Params P, Frame F, Control *ctl, int maxima)
 {
@@ -747,7 +753,7 @@ momentumKernel(Params P, Frame F, Control *ctl, int maxima)
         if (hs <= 0.0f) {
             if (G.t == 0) F.acc[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         } else {
-            MomentumVisit<D, K, BUDGET> visit{P, F, Smoothing<K, D>(P)};
+            MomentumVisit<D, K, BUDGET, COMP> visit{P, F, Smoothing<K, D>(P)};
             velocityOf<D>(F, i, visit.vi);
             visit.rhoI = densityOf<D>(F, i);
             visit.own = pressureRatioOf<D>(F, i);
@@ -755,10 +761,15 @@ momentumKernel(Params P, Frame F, Control *ctl, int maxima)
             visit.alphaI = P.closure ? F.eddy[i].x : 0.0f;
             if (P.limited) loadMatrix<D>(F.G0, F.G1, F.G2, i, visit.Gi);
             visit.total[0] = visit.total[1] = visit.total[2] = 0.0f;
+            if constexpr (COMP) for (int a = 0; a < 3; ++a) visit.comp[a] = 0.0f;
             if constexpr (BUDGET)
                 for (int q = 0; q < 4; ++q) visit.parts[q][0] = visit.parts[q][1] = visit.parts[q][2] = 0.0f;
             forEachNeighbour<D, T, FINE>(P, F, i, G.t, hs, visit);
-            for (int a = 0; a < D; ++a) visit.total[a] = groupSum<T>(visit.total[a], G.mask);
+            if constexpr (COMP) {
+                for (int a = 0; a < D; ++a) visit.total[a] = groupSumCompensated<T>(visit.total[a], visit.comp[a], G.mask);
+            } else {
+                for (int a = 0; a < D; ++a) visit.total[a] = groupSum<T>(visit.total[a], G.mask);
+            }
             if constexpr (BUDGET) {
                 for (int q = 0; q < 4; ++q) {
                     for (int a = 0; a < D; ++a) visit.parts[q][a] = groupSum<T>(visit.parts[q][a], G.mask);
@@ -877,8 +888,8 @@ __device__ __forceinline__ void driftAndEnforce(const Params &P, const Frame &F,
 
 // BUDGET: the rate split for the energy budget too: the plain sum over fluid and over boundary
 // neighbours, the corrected sum (the correction's part is its difference) and the diffusion
-// (src/pysurf/sphGpu.py:476-545).
-template <int D, int K, bool BUDGET>
+// (src/pysurf/sphGpu.py:476-545).  COMP: the sum compensated (Dot2), its running error in comp.
+template <int D, int K, bool BUDGET, bool COMP = false>
 struct ContinuityVisit {
     static constexpr bool kSkipCoincident = true;
     static constexpr bool kKinetic = true;
@@ -888,7 +899,7 @@ struct ContinuityVisit {
     bool boundaryI, diffuses, corrected;
     float vi[3], devI, Li[3][3], gi[3];
     float deltaI;           // closure: this particle's eddy delta
-    float total;
+    float total, comp;
     float plainFluid, plainWall, continuity, diffusive;     // BUDGET
     __device__ bool accept(bool fluidJ) const { return !(boundaryI && !fluidJ); }
     __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int, const float4 &B,
@@ -910,7 +921,8 @@ struct ContinuityVisit {
         }
         // explicit roundings on the sum's path (see the momentum sweep)
         const float massDot = massIn<D>(B) * dot;
-        total = __fmaf_rn(massDot, grad, total);
+        if constexpr (COMP) addProduct(massDot, grad, total, comp);
+        else total = __fmaf_rn(massDot, grad, total);
         if constexpr (BUDGET) {
             float plainDot = dot;
             if (corrected) {
@@ -945,14 +957,15 @@ struct ContinuityVisit {
             }
             const float r2 = r * r;
             const float head = factor * h * volumeIn<D>(B, X) * difference * (-grad), ratio = __fdividef(r2, r2 + k.soft);
-            total = __fmaf_rn(head, ratio, total);
+            if constexpr (COMP) addProduct(head, ratio, total, comp);
+            else total = __fmaf_rn(head, ratio, total);
             if constexpr (BUDGET) diffusive = __fmaf_rn(head, ratio, diffusive);
         }
     }
 };
 
 // mode 0: the rate only; 1: advance the density; 2: advance, drift and enforce.
-template <int D, int K, int T, bool BUDGET, bool FINE>
+template <int D, int K, int T, bool BUDGET, bool FINE, bool COMP = false>
 __global__ void __launch_bounds__(kBlock, BUDGET ? budgetMinBlocks<D>() : sweepMinBlocks<D>())
 continuityKernel(Params P, Frame F, Control *ctl, Enforcement E, int mode)
 {
@@ -961,7 +974,7 @@ continuityKernel(Params P, Frame F, Control *ctl, Enforcement E, int mode)
     const int i = G.i;
     if (i >= P.n) return;
     float hs = signedLength<D>(F, i);
-    ContinuityVisit<D, K, BUDGET> visit{P, F, Smoothing<K, D>(P)};
+    ContinuityVisit<D, K, BUDGET, COMP> visit{P, F, Smoothing<K, D>(P)};
     visit.boundaryI = hs <= 0.0f;
     visit.diffuses = P.diffusion != 0 && !visit.boundaryI;
     visit.corrected = P.corrected && !visit.boundaryI;
@@ -974,10 +987,12 @@ continuityKernel(Params P, Frame F, Control *ctl, Enforcement E, int mode)
         float4 g = F.gradRho[i];
         visit.gi[0] = g.x; visit.gi[1] = g.y; visit.gi[2] = g.z;
     }
-    visit.total = 0.0f;
+    visit.total = visit.comp = 0.0f;
     visit.plainFluid = visit.plainWall = visit.continuity = visit.diffusive = 0.0f;
     forEachNeighbour<D, T, FINE>(P, F, i, G.t, fabsf(hs), visit);
-    const float rate = groupSum<T>(visit.total, G.mask);
+    float rate;
+    if constexpr (COMP) rate = groupSumCompensated<T>(visit.total, visit.comp, G.mask);
+    else rate = groupSum<T>(visit.total, G.mask);
     float parts[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     if constexpr (BUDGET) {
         const float plainFluid = groupSum<T>(visit.plainFluid, G.mask);
@@ -1354,12 +1369,16 @@ static void launchT(const LaunchArgs &A, Stage stage)
         break;
     case Stage::Momentum:
         if (P.budget && A.maxima) momentumKernel<D, K, T, true, FINE><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.maxima);
+        else if (P.compensated)
+            momentumKernel<D, K, T, false, FINE, true><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.maxima);
         else momentumKernel<D, K, T, false, FINE><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.maxima);
         break;
     case Stage::Kick: kickKernel<D><<<pointwise, kBlock, 0, st>>>(P, F, A.ctl); break;
     case Stage::Continuity:
         // the budget's parts matter only where the step advances the density
         if (P.budget && A.flag != 0) continuityKernel<D, K, T, true, FINE><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.flag);
+        else if (P.compensated)
+            continuityKernel<D, K, T, false, FINE, true><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.flag);
         else continuityKernel<D, K, T, false, FINE><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.flag);
         break;
     case Stage::Xsph: xsphKernel<D, K, T, FINE><<<grid, kBlock, 0, st>>>(P, F, A.ctl, A.E, A.densities, A.flag); break;

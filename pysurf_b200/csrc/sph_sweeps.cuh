@@ -64,6 +64,43 @@ __device__ __forceinline__ float groupSum(float value, unsigned mask)
     return value;
 }
 
+// Compensated accumulation (Ogita, Rump and Oishi, "Accurate sum and dot product", SIAM J. Sci.
+// Comput. 26 (2005), Dot2): a running sum s with a running error c.  Each term a b enters as its
+// rounded product p and the product's exact error fma(a, b, -p); Knuth's TwoSum gives the exact
+// error of s + p.  Both errors gather in c, so s + c is the sum as if taken in twice the precision.
+// Every rounding is an explicit intrinsic, so no contraction changes a bit.
+__device__ __forceinline__ void twoSum(float a, float b, float &sum, float &error)
+{
+    sum = __fadd_rn(a, b);
+    const float bv = __fsub_rn(sum, a);
+    error = __fadd_rn(__fsub_rn(a, __fsub_rn(sum, bv)), __fsub_rn(b, bv));
+}
+
+__device__ __forceinline__ void addProduct(float a, float b, float &s, float &c)
+{
+    const float p = __fmul_rn(a, b);
+    const float productError = __fmaf_rn(a, b, -p);
+    float sum, sumError;
+    twoSum(s, p, sum, sumError);
+    s = sum;
+    c = __fadd_rn(c, __fadd_rn(productError, sumError));
+}
+
+// The group's compensated sum, the same bits on every lane: TwoSum is exact whichever operand comes
+// first, so each lane's pair of partner values combines to the same (s, c).
+template <int T>
+__device__ __forceinline__ float groupSumCompensated(float s, float c, unsigned mask)
+{
+    for (int offset = T / 2; offset > 0; offset >>= 1) {
+        const float s2 = __shfl_xor_sync(mask, s, offset, T), c2 = __shfl_xor_sync(mask, c, offset, T);
+        float sum, error;
+        twoSum(s, s2, sum, error);
+        s = sum;
+        c = __fadd_rn(__fadd_rn(c, c2), error);
+    }
+    return __fadd_rn(s, c);
+}
+
 // The coarse test's squared distance between float32 points, and a pair's separation and squared
 // distance.  Each takes its roundings from explicit intrinsics, so that the table kernel and the
 // walk, compiled apart, reach the same decision on a pair at the edge of the support.  The support

@@ -116,6 +116,7 @@ struct SphSystem {
     // the energy budget (src/pysurf/sphEnergy.py): each particle's running total of each term, by
     // caller index, and the momentum sweep's parts of a; energyCap rows, made while it is on
     int budget = 0;
+    int compensated = 0;        // compensated momentum and continuity sums
     double *energy = nullptr;
     float4 *parts = nullptr;
     int energyCap = 0;
@@ -482,6 +483,7 @@ struct SphSystem {
         P.listStride = capacity;
         P.budget = budget && energy ? 1 : 0;
         P.energyStride = energyCap;
+        P.compensated = compensated;
         return P;
     }
 
@@ -858,8 +860,20 @@ int sph_set_shifting(SphSystem *sys, int enabled, double mach, double spacing, d
 int sph_set_energy_budget(SphSystem *sys, int enabled)
 {
     CHECK_SYS(sys);
+    if (enabled && sys->compensated)
+        return fail(SPH_ERR_UNSUPPORTED, "the energy budget's sweeps keep plain sums; turn compensated sums off first");
     sys->budget = enabled ? 1 : 0;
     if (enabled) TRY(sys->reserveBudget(true));
+    sys->graphDirty = true;
+    return SPH_OK;
+}
+
+int sph_set_compensated_sums(SphSystem *sys, int enabled)
+{
+    CHECK_SYS(sys);
+    if (enabled && sys->budget)
+        return fail(SPH_ERR_UNSUPPORTED, "the energy budget's sweeps keep plain sums; turn the budget off first");
+    sys->compensated = enabled ? 1 : 0;
     sys->graphDirty = true;
     return SPH_OK;
 }

@@ -143,6 +143,7 @@ class PairSums:
         self.trackEnergy = False
         self.shiftingEnabled = False
         self.closureEnabled = False
+        self.compensatedSums = False
         self._lib = _lib.load()
         lower, upper = np.zeros(3), np.zeros(3)
         lower[:self.dimensions] = np.asarray(domainMin, dtype=float)[:self.dimensions]
@@ -200,6 +201,13 @@ class PairSums:
         particle's running total of every term in `energyTerms`, from `push` to `energySums`."""
         check(self._lib.sph_set_energy_budget(self._handle, int(bool(enabled))), 'setEnergyBudget')
         self.trackEnergy = bool(enabled)
+
+    def setCompensatedSums(self, enabled: bool) -> None:
+        """Whether the momentum and continuity sums carry their running rounding error (Dot2
+        compensation: each particle's du/dt and drho/dt as if summed in twice float32's precision;
+        the terms stay float32).  Not with the energy budget."""
+        check(self._lib.sph_set_compensated_sums(self._handle, int(bool(enabled))), 'setCompensatedSums')
+        self.compensatedSums = bool(enabled)
 
     def energySums(self) -> np.ndarray:
         """Each term's energy over the device steps since `push` [J] (per unit depth in 2D), summed
