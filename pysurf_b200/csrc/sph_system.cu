@@ -602,14 +602,9 @@ struct SphSystem {
     int upload(void *dst, const void *src, size_t bytes)
     {
         if (bytes == 0) return SPH_OK;
-        cudaPointerAttributes attr;
-        bool pinned = cudaPointerGetAttributes(&attr, src) == cudaSuccess && attr.type == cudaMemoryTypeHost;
-        cudaGetLastError();
-        if (pinned) {
-            CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
-        } else {
-            CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
-        }
+        // pinned caller memory copies by DMA behind the return; pageable memory is staged by the
+        // driver before the call returns
+        CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
         return SPH_OK;
     }
 
