@@ -1,27 +1,36 @@
-"""Benchmark: fluid particle-updates/s of the deltaSph step on the 2D solitary wave over a 1:15 beach.
+"""Benchmark: fluid particle-updates/s of the deltaSph step on the 3D solitary wave over a Gaussian ridge.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--case beach|ridge] [--ppd P]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--case ridge|beach] [--ppd P]
 
-Workload: the first-order solitary wave of H/d = 0.45 at x0 = 10 d over a 1:15 beach from
-x = 15 d, 60 d long, 64 particles per depth (pysurf_b200.cases.solitaryBeach), stepped by the
-deltaSph scheme (Wendland C2 at h = 3 dx, hydrostatic delta-SPH diffusion, the continuity
-correction, extrapolated walls, the viscosity limiter, density floor 0.9 rho0).  A step is one
-full device-resident step: cell list, wall pressure, gradients, momentum, time step, kick,
-continuity, density update, drift and bed enforcement.  --case ridge steps the 3D Gaussian-ridge
-tank instead (pysurf_b200.cases.ridgeWave3D, 24 particles per depth by default).
+Workload (the default): a first-order solitary wave of H/d = 0.5 crossing a Gaussian ridge (0.6 d
+high, sigma 3 d, its axis at 25 degrees to the crest) in a walled 40 d x 10 d tank, 32 particles
+per depth (pysurf_b200.cases.ridgeWave3D, 11.7M fluid and 4.1M boundary particles), whose crest zone
+(every column whose surface stands 0.3 H above still water) is split on the device into 8 daughters
+of h / 2 before the timing: 22.9M fluid particles.  Stepped by the deltaSph scheme (Wendland C2 at
+h = 3 dx, hydrostatic delta-SPH diffusion, the continuity correction, extrapolated walls, the
+viscosity limiter, density floor 0.9 rho0).  A step is one full device-resident step: cell list and
+neighbour table over both grid levels, wall pressure, gradients, momentum, time step, kick,
+continuity, density update, drift and height-field enforcement.  --no-refine skips the split;
+--case beach steps the 2D solitary wave of H/d = 0.45 over a 1:15 beach at 64 particles per depth
+(pysurf_b200.cases.solitaryBeach) instead.
 
 value      fluid particles x steps / device time of exactly K steps (CUDA events on the stream the
            kernels run on, an L2 flush of 256 MiB between steps outside the timed spans), max over
            ranks; with N GPUs each rank runs its own replica of the case (independent cases need
            no collective), so the value is the sum over replicas ("scaling": "weak").
 e2e        the same metric through the public API with host buffers: each step pushes the whole
-           state from pinned host memory, steps once and pulls the state back.
+           state (after the split: its lengths too) from pinned host memory, steps once and pulls
+           the state back.
 roofline   the dominant kernel (momentum) against the measured HBM copy bandwidth, with the
-           step's algorithmic bytes per fluid particle-update (53 B in 2D, 69 B in 3D) per launch.
+           step's algorithmic bytes per fluid particle-update (53 B in 2D, 69 B in 3D, 4 B more
+           with mixed smoothing lengths) per launch.
 pair_flops the three sweeps' float32 work, 150 flop a directed pair, against the nominal FP32 SIMT
            peak: the gather sweeps are bound by latency and issue, not by HBM.
---impl reference   the float64 C restatement of the reference's step (oracle/, OpenMP over every
-           host core) on the same workload, timed per step.
+cpu_baseline and --impl reference   the float64 C restatement of the reference's step (oracle/,
+           OpenMP over every host core), timed per step: on the beach over the whole case; on the
+           ridge over a sample of it, the particles of a slab of whole columns across the tank's
+           middle (y within 0.125 d of it) over the tank's full length, split by the same zone rule,
+           since a float64 step over all 27M particles takes minutes.
 """
 from __future__ import annotations
 
@@ -52,9 +61,10 @@ def parseArgs():
     p.add_argument('--steps', type=int, default=40)
     p.add_argument('--warmup', type=int, default=5)
     p.add_argument('--impl', default='b200', choices=['b200', 'reference'])
-    p.add_argument('--case', default='beach', choices=['beach', 'ridge'],
-                   help='beach: the 2D solitary wave on a 1:15 beach (the headline); ridge: the 3D Gaussian ridge')
-    p.add_argument('--ppd', type=int, default=None, help='particles per depth (64 beach, 24 ridge)')
+    p.add_argument('--case', default='ridge', choices=['ridge', 'beach'],
+                   help='ridge: the 3D Gaussian ridge, crest zone split (the headline); beach: the 2D solitary wave '
+                        'on a 1:15 beach')
+    p.add_argument('--ppd', type=int, default=None, help='particles per depth (32 ridge, 64 beach)')
     p.add_argument('--cells', type=int, default=None, help='cells per kernel support in the device cell list')
     p.add_argument('--threads', type=int, default=None, help='threads per particle in the sweeps (1, 2, 4, 8)')
     p.add_argument('--no-table', action='store_true', help='walk the cells in every sweep (no neighbour table)')
@@ -73,8 +83,9 @@ def parseArgs():
                    help='serve this many requests arriving as a Poisson stream (see serveBench)')
     p.add_argument('--horizon-scale', type=float, default=0.1,
                    help='the served requests horizons, U(2, 6) s of simulated time times this')
-    p.add_argument('--refine', action='store_true',
-                   help='split the crest zone (surface above 0.3 H) into daughters of h/2 before timing')
+    p.add_argument('--no-refine', action='store_true',
+                   help='ridge: leave the crest zone (surface above 0.3 H) whole instead of splitting it into '
+                        'daughters of h/2 before the timing')
     p.add_argument('--options', default='',
                    help='opt-in parts of the step, comma separated: closure (delta-LES-SPH), shifting, energy '
                         '(the energy budget), compensated (compensated momentum and continuity sums)')
@@ -88,7 +99,7 @@ OPTIONS = ('closure', 'shifting', 'energy', 'compensated')
 
 def buildCase(args):
     from pysurf_b200 import cases
-    case = cases.ridgeWave3D(args.ppd or 24) if args.case == 'ridge' else cases.solitaryBeach(args.ppd or 64)
+    case = cases.ridgeWave3D(args.ppd or 32) if args.case == 'ridge' else cases.solitaryBeach(args.ppd or 64)
     options = [o for o in args.options.split(',') if o]
     unknown = set(options) - set(OPTIONS)
     if unknown:
@@ -133,6 +144,60 @@ def meanNeighbours(case, sample: int = 20000) -> float:
     chosen = np.random.default_rng(0).choice(fluid, size=min(sample, fluid.size), replace=False)
     counts = cKDTree(positions).query_ball_point(positions[chosen], 2.0 * case.smoothingLength, return_length=True)
     return float(np.mean(counts) - 1.0)
+
+
+RIDGE_SAMPLE_HALF_WIDTH = 0.125    # d: the ridge's CPU sample is the columns within this of the tank's middle
+
+
+def refines(case, args) -> bool:
+    return case.dimensions == 3 and not args.no_refine
+
+
+def ridgeSample(case, refine: bool, halfWidth: float = RIDGE_SAMPLE_HALF_WIDTH) -> dict:
+    """A bounded sample of the ridge workload for the float64 CPU step: every particle (fluid, bed and
+    end walls) of the columns -- one spacing across, as the crest zone counts them -- within halfWidth d
+    of the tank's middle line in y, over the tank's full length, split by the device's zone rule
+    (oracle.crestZone, then oracle.splitParticles into 8 daughters of h / 2).  The slab's particles near
+    its y edges miss the neighbours beyond them, so a float64 step over it costs less a particle than
+    over the whole tank.  Also the mean neighbour count (r < h_i + h_j) of the slab's fluid, counted
+    among the particles of a slab two supports wider, as in the whole tank."""
+    import numpy as np
+    from scipy.spatial import cKDTree
+    from oracle import oracle
+    st, s, info = case.state, case.spacing, case.info
+    lower, upper = case.domainMin, case.domainMax
+    nx = int(math.ceil((upper[0] - lower[0]) / s))
+    ny = int(math.ceil((upper[1] - lower[1]) / s))
+    rows = int(round(halfWidth * float(info['depth']) / s))
+    margin = int(math.ceil(4.0 * case.smoothingLength / s))
+    centre = int(math.floor((0.5 * float(info['tank'][1]) - lower[1]) / s + 0.5))
+    cy = np.floor((st.positions[:, 1] - lower[1]) / s)
+    keep = (cy >= centre - rows - margin) & (cy < centre + rows + margin)
+    wide = {'positions': st.positions[keep].copy(), 'velocities': st.velocities[keep].copy(),
+            'densities': st.densities[keep].copy(), 'masses': np.broadcast_to(st.masses, keep.shape)[keep].copy(),
+            'isFluid': st.isFluid[keep].copy(), 'lengths': np.full(int(keep.sum()), case.smoothingLength)}
+    if refine:
+        depth, height = float(info['depth']), float(info['H/d']) * float(info['depth'])
+        fluidMass = float(np.max(st.masses[st.isFluid]))
+        zone = oracle.crestZone(wide, lower[0], lower[1], s, nx, ny, depth + 0.3 * height, 0.999 * fluidMass)
+        oracle.splitParticles(wide, zone, case.referenceDensity, case.smoothingLength, 0.5)
+    x, h = wide['positions'], wide['lengths']
+    column = np.floor((x[:, 1] - lower[1]) / s)
+    narrow = (column >= centre - rows) & (column < centre + rows)
+    fluid = np.flatnonzero(narrow & wide['isFluid'])
+    chosen = np.random.default_rng(0).choice(fluid, size=min(20000, fluid.size), replace=False)
+    tree, hmax = cKDTree(x), float(h.max())
+    counts = []
+    for i, near in zip(chosen, tree.query_ball_point(x[chosen], h[chosen] + hmax)):
+        near = np.asarray(near)
+        r = np.linalg.norm(x[near] - x[i], axis=1)
+        counts.append(int(np.count_nonzero(r < h[i] + h[near])) - 1)
+    sample = {k: v[narrow] for k, v in wide.items()}
+    sample['neighbours'] = float(np.mean(counts)) if counts else float('nan')
+    sample['description'] = (f'the columns within {halfWidth} d of the tank\'s middle over its full length '
+                             f'({int(sample["isFluid"].sum())} fluid and {int((~sample["isFluid"]).sum())} boundary '
+                             f'particles{", crest zone split" if refine else ""})')
+    return sample
 
 
 def oracleStepper(case):
@@ -233,12 +298,25 @@ def profiledTraffic(case) -> float | None:
     return traffic
 
 
-def cpuBaseline(case, seconds: float = 12.0) -> dict:
-    """The float64 oracle's step on the same workload, on every host core, for about `seconds`."""
+def cpuState(case, refine: bool) -> tuple:
+    """The state the float64 CPU step runs on, its fluid count and what it is: the whole beach, or the
+    ridge's sample (ridgeSample)."""
     import numpy as np
-    stepper = oracleStepper(case)
+    if case.dimensions == 3:
+        sample = ridgeSample(case, refine)
+        return sample, int(sample['isFluid'].sum()), 'one float64 step over a sample of the workload: ' + \
+            sample.pop('description')
     state = {k: np.array(getattr(case.state, k), copy=True) for k in ('positions', 'velocities', 'densities',
                                                                        'masses', 'isFluid')}
+    return state, case.fluidCount, f'full steps of the whole case ({case.state.nParticles} particles) in float64'
+
+
+def cpuBaseline(case, refine: bool, seconds: float = 12.0) -> dict:
+    """The float64 oracle's step on the same workload (the ridge: its sample), on every host core, for
+    about `seconds` after one untimed step."""
+    stepper = oracleStepper(case)
+    state, fluid, what = cpuState(case, refine)
+    state.pop('neighbours', None)
     stepper(state)                          # warm-up: page in, first neighbour list
     steps, start = 0, time.perf_counter()
     while True:
@@ -248,35 +326,35 @@ def cpuBaseline(case, seconds: float = 12.0) -> dict:
         if elapsed > seconds or steps >= 200:
             break
     cores = os.cpu_count()
-    return {'value': case.fluidCount * steps / elapsed, 'unit': METRIC, 'cores': cores, 'kind': 'port',
-            'sample': f'{steps} full steps of the same case ({case.state.nParticles} particles) in float64, '
-                      f'OpenMP over {cores} threads, {elapsed:.1f} s'}
+    return {'value': fluid * steps / elapsed, 'unit': METRIC, 'cores': cores, 'kind': 'port',
+            'sample': f'{steps} x {what}, OpenMP over {cores} threads, {elapsed:.1f} s'}
 
 
 def referenceArm(args) -> None:
-    """The reference's algorithm on the host cores: the float64 C restatement (oracle/), timed per step."""
+    """The reference's algorithm on the host cores: the float64 C restatement (oracle/), timed per step
+    (the ridge: each step over its sample)."""
     rank = int(os.environ.get('RANK', '0'))
     if rank != 0:
         return
     case = buildCase(args)
-    import numpy as np
+    refine = refines(case, args)
     stepper = oracleStepper(case)
-    state = {k: np.array(getattr(case.state, k), copy=True) for k in ('positions', 'velocities', 'densities',
-                                                                       'masses', 'isFluid')}
+    state, fluid, what = cpuState(case, refine)
+    state.pop('neighbours', None)
     for _ in range(args.warmup):
         stepper(state)
     start = time.perf_counter()
     for _ in range(args.steps):
         stepper(state)
     elapsed = time.perf_counter() - start
-    value = case.fluidCount * args.steps / elapsed
+    value = fluid * args.steps / elapsed
     cores = os.cpu_count()
     line = {'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': METRIC, 'n_gpus': args.gpus,
             'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': 1e3 * elapsed / args.steps,
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
-            'config': config(case, flush=False),
+            'config': dict(config(case, flush=False), crest_zone_split=refine),
             'cpu_baseline': {'value': value, 'unit': METRIC, 'cores': cores, 'kind': 'port',
-                             'sample': f'{args.steps} full steps of the whole case in float64 on {cores} threads'},
+                             'sample': f'{args.steps} x {what}, OpenMP over {cores} threads'},
             'e2e': {'value': value, 'unit': METRIC, 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
     print(json.dumps(line), flush=True)
 
@@ -429,14 +507,17 @@ def main() -> None:
     state = case.state.copy()
     sums.push(state)
     sums.setBoundary(case.boundary, state)
-    neighbours = meanNeighbours(case)
     h, cfl, maxdt = case.smoothingLength, case.cflNumber, case.maxTimeStep
+    refine = refines(case, args)
     refined = None
-    if args.refine:
+    if refine:
         refined = cases.refineCrestZone(sums, case)
         h = 0.5 * case.smoothingLength     # the shortest length sets the time step
-        neighbours = float('nan')           # mixed lengths: the start's count no longer stands
-        args.no_e2e = args.no_cpu = True    # the host copy no longer matches the device's count
+    # the 2D start's neighbour count from the whole case; the ridge's from its CPU sample (a tree over
+    # every one of its particles takes longer than the run), which is split as the device split
+    sample = ridgeSample(case, refine) if case.dimensions == 3 else None
+    neighbours = sample['neighbours'] if sample is not None else meanNeighbours(case)
+    del sample
     fluidCount = case.fluidCount + (refined or 0) * (2 ** case.dimensions - 1)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device='cuda')     # 256 MiB, twice the L2
 
@@ -474,7 +555,7 @@ def main() -> None:
     dominant = max((name for name in stages if name != 'cells'), key=stages.get)
     peaks = measuredPeaks()
     kernelMs = stages[dominant]
-    unitBytes = ALGORITHMIC_BYTES[case.dimensions]
+    unitBytes = ALGORITHMIC_BYTES[case.dimensions] + (4 if refine else 0)     # + h when the lengths are mixed
     achieved = unitBytes * fluidCount / (kernelMs / 1e3) / 1e9
     pairFlop = fluidCount * neighbours * FLOP_PER_PAIR
     simt = {'flop_per_pair': FLOP_PER_PAIR, 'neighbours_per_fluid_particle': neighbours,
@@ -489,18 +570,25 @@ def main() -> None:
     # end to end through the public API with host buffers: push, one step, pull, every step
     e2e = None
     if not args.no_e2e:
-        n, dim = case.state.nParticles, case.dimensions
+        # the device state as it stands (after a split: its count, masses, lengths and flags) in pinned
+        # host buffers, pushed whole every step
+        current = sums.pullState()
+        n, dim = len(current['masses']), case.dimensions
         pinned = {name: torch.empty(shape, dtype=torch.float64, pin_memory=True).numpy()
                   for name, shape in (('positions', (n, dim)), ('velocities', (n, dim)), ('densities', (n,)),
-                                      ('masses', (n,)), ('pressures', (n,)), ('accelerations', (n, dim)))}
-        sums.pull(state)
+                                      ('masses', (n,)), ('pressures', (n,)), ('accelerations', (n, dim)),
+                                      ('lengths', (n,)))}
         flags = torch.empty(n, dtype=torch.bool, pin_memory=True).numpy()
         host = type(state)(pinned['positions'], pinned['velocities'], pinned['accelerations'], pinned['densities'],
                            pinned['pressures'], pinned['masses'], flags)
         for name in ('positions', 'velocities', 'densities', 'masses', 'pressures', 'accelerations'):
-            getattr(host, name)[:] = getattr(state, name)
-        host.isFluid[:] = state.isFluid
-        bytesIn = n * (dim * 8 * 2 + 8 + 8 + 1)
+            getattr(host, name)[:] = current[name]
+        host.isFluid[:] = current['isFluid']
+        if refine:
+            pinned['lengths'][:] = current['lengths']
+            host.lengths = pinned['lengths']
+        del current
+        bytesIn = n * (dim * 8 * 2 + 8 + 8 + 1 + (8 if refine else 0))
         bytesOut = n * (dim * 8 * 2 + 8 + 8 + dim * 8)
         e2eSteps = max(5, min(args.steps, 20))
         torch.cuda.synchronize()
@@ -524,7 +612,7 @@ def main() -> None:
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpuBaseline(case)
+        cpu = cpuBaseline(case, refine)
 
     if rank == 0:
         line = {'metric': METRIC, 'value': value, 'unit': METRIC, 'n_gpus': world, 'steps': args.steps,

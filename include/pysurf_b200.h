@@ -50,6 +50,10 @@ int sph_create(int dimensions, double smoothing_length, const double *domain_min
 int sph_destroy(SphSystem *sys);
 const char *sph_last_error(void);
 int sph_version(void);
+/* The architecture the library's kernels were compiled for, as the CUDA runtime loads them on the
+ * current device (cudaFuncAttributes.binaryVersion: 100 for sm_100a).  No counterpart in the
+ * reference: a diagnostic that the loaded library carries B200 code. */
+int sph_kernel_architecture(int *version);
 
 /* The hash grid's shape the reference's sortParticles reads (PairSums.gridShape,
  * src/pysurf/sphGpu.py:1466-1478 gridDimensions). */
@@ -160,9 +164,21 @@ int sph_density_gradients(SphSystem *sys, const double *densities, double *out);
 int sph_push(SphSystem *sys, int64_t n, const double *positions, const double *velocities, const double *densities,
              const double *masses, const uint8_t *is_fluid, const double *lengths);
 /* PairSums.pull (src/pysurf/sphGpu.py:2223-2235): any output may be NULL.  masses, lengths and
- * is_fluid come back too, since a device split changes them. */
+ * is_fluid come back too, since a device split changes them.  Pressures are the frame's, the ones
+ * the last step used; after a push, split or merge with no step since, they are the Tait pressures
+ * of the densities and the accelerations are zero (no step has taken them for that state). */
 int sph_pull(SphSystem *sys, double *positions, double *velocities, double *densities, double *pressures,
              double *accelerations, double *masses, double *lengths, uint8_t *is_fluid);
+/* sph_push and sph_pull over DEVICE arrays on the handle's device (a torch tensor's data_ptr(),
+ * float64 contiguous, the same shapes), copied device to device on the handle's stream, so a
+ * caller whose state lives in device tensors never routes it through the host.  The push reads
+ * the lengths back to check them on the host (n doubles); both return once their copies are done
+ * (the handle's stream is synchronized), so the caller's tensors are free, or hold the results,
+ * whatever stream the caller works on.  Same citations as sph_push and sph_pull. */
+int sph_push_device(SphSystem *sys, int64_t n, const double *positions, const double *velocities,
+                    const double *densities, const double *masses, const uint8_t *is_fluid, const double *lengths);
+int sph_pull_device(SphSystem *sys, double *positions, double *velocities, double *densities, double *pressures,
+                    double *accelerations, double *masses, double *lengths, uint8_t *is_fluid);
 int sph_count(const SphSystem *sys, int64_t *n);
 /* FrameWriter.write's arrays from the device state (src/pysurf/sphFrames.py:60-100): every
  * particle's float32 position (n x dim) and float32 speed, the speed |v| taken in float64 as numpy

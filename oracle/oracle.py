@@ -6,6 +6,7 @@ reference's sums in gather form, citations there) and adds the two pieces of boo
 are plainer in numpy:
 
     splitParticles      src/pysurf/sphRefinement.py:136-190
+    crestZone           the device's crest zone (sph_split_crest_zone), for the CPU baseline's sample
     solitaryWaveBeach   (set-up only) see pysurf_b200.cases
 
 Every function takes and returns numpy float64 arrays shaped as the reference's array
@@ -421,6 +422,23 @@ def splitParticles(state, mask, rho0, referenceLength, lengthRatio=1.0):
     state['isFluid'] = np.concatenate([fluid, np.ones(chosen.size * (count - 1), dtype=bool)])
     state['lengths'] = np.concatenate([lengths, rep(length)])
     return int(chosen.size)
+
+
+def crestZone(state, x0, y0, width, nx, ny, threshold, minMass):
+    """The crest zone the device splits (sph_split_crest_zone; the zone of BreakingWave3D._refineCrest,
+    src/pysurf/BreakingWave3D.py:530-576, read as columns): every fluid particle of mass at least
+    minMass whose column -- floor((x - x0) / width), floor((y - y0) / width) in 3D, nx by ny of them --
+    has its highest fluid particle above threshold.  Returns the mask."""
+    x = _f64(state['positions'])
+    dim = x.shape[1]
+    fluid = np.asarray(state['isFluid'], dtype=bool)
+    cx = np.floor((x[:, 0] - x0) / width)
+    cy = np.floor((x[:, 1] - y0) / width) if dim == 3 else np.zeros(len(x))
+    inside = fluid & (cx >= 0) & (cx < nx) & (cy >= 0) & (cy < ny)
+    column = np.where(inside, cy * nx + cx, 0).astype(np.int64)
+    tops = np.full(int(nx * ny), -np.inf)
+    np.maximum.at(tops, column[inside], x[inside, dim - 1])
+    return inside & (_f64(state['masses']) >= minMass) & (tops[column] > threshold)
 
 
 def refinementLevels(masses, referenceMass, dim):

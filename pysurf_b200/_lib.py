@@ -38,6 +38,7 @@ SIGNATURES = {
     'sph_destroy': [_h],
     'sph_last_error': [],
     'sph_version': [],
+    'sph_kernel_architecture': [C.POINTER(C.c_int)],
     'sph_grid_shape': [_h, _pi64],
     'sph_set_cells_per_support': [_h, _i],
     'sph_set_stream': [_h, _vp],
@@ -60,6 +61,8 @@ SIGNATURES = {
     'sph_density_gradients': [_h, _pd, _pd],
     'sph_push': [_h, _i64, _pd, _pd, _pd, _pd, _pu8, _pd],
     'sph_pull': [_h, _pd, _pd, _pd, _pd, _pd, _pd, _pd, _pu8],
+    'sph_push_device': [_h, _i64, _vp, _vp, _vp, _vp, _vp, _vp],
+    'sph_pull_device': [_h, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp],
     'sph_count': [_h, _pi64],
     'sph_frame': [_h, _pf, _pf, _pu8],
     'sph_clear_boundary': [_h],

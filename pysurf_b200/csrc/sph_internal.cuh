@@ -10,12 +10,17 @@
 //     pb   float4  2D (m, hs, dev, V)       3D (lx, ly, lz, m)
 //     kin  float4  2D (vx, vy, rho, P2)     3D (vx, vy, vz, rho)
 //     aux  float4  3D (P2, dev, V, -)
+//     low  float4  (vlx, vly, vlz, devLo): the float32 remainders of the float64 velocity and deviation
 //     pres float   the pressure p
 //   hi + lo is each float64 coordinate split into a float32 point and its float32 remainder, so a
 //   separation (hi_i - hi_j) + (lo_i - lo_j) keeps the float64 positions' digits without float64
 //   arithmetic (src/pysurf/sphGpu.py:227-242 states the same split).  hs is +h for a fluid
 //   particle and -h for a boundary particle; dev is rho - rho0 in float32, taken in float64
 //   (src/pysurf/sphGpu.py:1031-1038), so neighbours' density differences keep their digits.
+//   The continuity sweep takes velocity and deviation differences from the float32 values and their
+//   remainders, (v_i - v_j) + (vl_i - vl_j), so they keep float64's digits: continuity sums terms
+//   that cancel (the velocity's divergence next to a wall, the hydrostatic subtraction near rest),
+//   where a float32 value's rounding would otherwise dominate the rate.
 //   V = m / rho and P2 = p / rho^2 are each particle's own, taken once per step instead of once per
 //   pair: the same float32 quotients the pair sums would take.
 #pragma once
@@ -81,11 +86,11 @@ struct Params {
     float g[3];
     double rho0, stiffness, densityFloor;  // the equation of state's rho0 and B = rho0 c0^2 / 7
     double devReference;    // the diffusion's rho0: deviations are rho - devReference
-    float rho0F;            // devReference in float32, for the hydrostatic subtraction
+    float halfInvRho0;      // 0.5 / devReference: a pair's mean deviation over rho0
     int tension;            // the fluid may carry negative pressure
     int diffusion;          // 0 none, 1 molteni, 2 hydrostatic, 3 antuono
     float diffusionFactor;  // 2 delta c0
-    float gravityOverSound; // g / c0^2, for the hydrostatic subtraction
+    float hydrostaticSlope; // rho0 g / c0^2, rounded once from float64: the hydrostatic density's slope in z
     int corrected;          // continuity takes L_i grad W
     int limited;            // viscosity limiter
     int wallExtrapolated;
@@ -118,6 +123,7 @@ struct Params {
 // The float32 frame and the float64 master state, current buffers.
 struct Frame {
     float4 *pa, *pb, *kin, *aux;
+    float4 *low;            // remainders: velocity (xyz) and deviation (w)
     float *pres;            // pressure
     int *cell;              // sorted cell index of each slot
     const int *cellStart;   // lower bound of each cell in the sorted order, numCells + 1 entries
@@ -224,6 +230,22 @@ __device__ __forceinline__ float kernelGradient(float q, const KernelAt &k)
     if (q < 1.0f) return k.gradC * (2.25f * q - 3.0f);
     float rest = 2.0f - q;
     return __fdividef(-0.75f * k.gradC * rest * rest, q);
+}
+
+// (dW/dr) / r in float64 at a pair's float64 distance r, with the pair's (float32) kernel constants:
+// the continuity sweep's wall pairs, whose terms cancel across a particle's neighbours, so each
+// term's own rounding must stay well below float32's.
+template <int K>
+__device__ __forceinline__ double kernelGradient64(double r, const KernelAt &k)
+{
+    const double q = r * (double)k.invH;
+    if (K == 1) {
+        const double rest = 1.0 - 0.5 * q;
+        return (double)k.gradC * rest * rest * rest;
+    }
+    if (q < 1.0) return (double)k.gradC * (2.25 * q - 3.0);
+    const double rest = 2.0 - q;
+    return -0.75 * (double)k.gradC * rest * rest / q;
 }
 
 __device__ __forceinline__ float sigmaAt(float unit, float h, int dim)
@@ -405,9 +427,11 @@ template <int D> __device__ __forceinline__ void velocityIn(const float4 &K, flo
 template <int D>
 __device__ __forceinline__ void storeDensity(const Frame &F, int i, float m, double rho64, double devReference, float p)
 {
-    const float rho = (float)rho64, dev = (float)(rho64 - devReference);
+    const double dev64 = rho64 - devReference;
+    const float rho = (float)rho64, dev = (float)dev64;
     const float volume = m / rho, ratio = p / (rho * rho);
     F.pres[i] = p;
+    F.low[i].w = (float)(dev64 - (double)dev);
     if (D == 2) {
         F.kin[i].z = rho; F.kin[i].w = ratio;
         F.pb[i].z = dev; F.pb[i].w = volume;
@@ -477,17 +501,17 @@ template <> __device__ __forceinline__ void storeMatrix<3>(float4 *R0, float4 *R
     R2[j] = make_float4(M[2][0], M[2][1], M[2][2], 0.0f);
 }
 
-template <int D> __device__ __forceinline__ float determinant(const float M[3][3])
+template <int D, class R> __device__ __forceinline__ R determinant(const R M[3][3])
 {
     if (D == 2) return M[0][0] * M[1][1] - M[0][1] * M[1][0];
     return M[0][0] * (M[1][1] * M[2][2] - M[1][2] * M[2][1]) - M[0][1] * (M[1][0] * M[2][2] - M[1][2] * M[2][0])
          + M[0][2] * (M[1][0] * M[2][1] - M[1][1] * M[2][0]);
 }
 
-template <int D> __device__ __forceinline__ void inverse(const float M[3][3], float out[3][3])
+template <int D, class R> __device__ __forceinline__ void inverse(const R M[3][3], R out[3][3])
 {
-    float det = determinant<D>(M);
-    float s = 1.0f / det;
+    R det = determinant<D>(M);
+    R s = R(1) / det;
     if (D == 2) {
         out[0][0] = M[1][1] * s; out[0][1] = -M[0][1] * s;
         out[1][0] = -M[1][0] * s; out[1][1] = M[0][0] * s;

@@ -197,18 +197,25 @@ __global__ void gatherKernel(Params P, int n, const int *perm, MasterView from, 
     }
     float hs = fl ? h : -h;
     float p = (float)taitPressure(P, rho, fl != 0);
-    float dev = (float)(rho - P.devReference);
+    const double dev64 = rho - P.devReference;
+    float dev = (float)dev64;
     float rhoF = (float)rho;
     float volume = m / rhoF, ratio = p / (rhoF * rhoF);
+    float vf[3], vl[3];
+    for (int a = 0; a < 3; ++a) {
+        vf[a] = (float)v[a];
+        vl[a] = (float)(v[a] - (double)vf[a]);
+    }
     F.pres[s] = p;
+    F.low[s] = make_float4(vl[0], vl[1], vl[2], (float)(dev64 - (double)dev));
     if (P.dim == 2) {
         F.pa[s] = make_float4(hi[0], hi[1], lo[0], lo[1]);
         F.pb[s] = make_float4(m, hs, dev, volume);
-        F.kin[s] = make_float4((float)v[0], (float)v[1], rhoF, ratio);
+        F.kin[s] = make_float4(vf[0], vf[1], rhoF, ratio);
     } else {
         F.pa[s] = make_float4(hi[0], hi[1], hi[2], hs);
         F.pb[s] = make_float4(lo[0], lo[1], lo[2], m);
-        F.kin[s] = make_float4((float)v[0], (float)v[1], (float)v[2], rhoF);
+        F.kin[s] = make_float4(vf[0], vf[1], vf[2], rhoF);
         F.aux[s] = make_float4(ratio, dev, volume, 0.0f);
     }
 }
@@ -223,18 +230,27 @@ __global__ void loadFieldsKernel(Params P, int n, const int *orig, const double 
     if (s >= n) return;
     int o = orig[s];
     float4 k = F.kin[s];
+    float4 low = F.low[s];
     if (velocities) {
-        k.x = (float)velocities[o * P.dim];
-        k.y = (float)velocities[o * P.dim + 1];
-        if (P.dim == 3) k.z = (float)velocities[o * P.dim + 2];
+        const double *v = velocities + (size_t)o * P.dim;
+        k.x = (float)v[0];
+        k.y = (float)v[1];
+        low.x = (float)(v[0] - (double)k.x);
+        low.y = (float)(v[1] - (double)k.y);
+        if (P.dim == 3) {
+            k.z = (float)v[2];
+            low.z = (float)(v[2] - (double)k.z);
+        }
     }
     float p = pressures ? (float)pressures[o] : F.pres[s];
     F.pres[s] = p;
     if (P.dim == 2) {
         float4 b = F.pb[s];
         if (densities) {
+            const double dev = densities[o] - deviationReference;
             k.z = (float)densities[o];
-            b.z = (float)(densities[o] - deviationReference);
+            b.z = (float)dev;
+            low.w = (float)(dev - (double)b.z);
         }
         b.w = b.x / k.z;
         k.w = p / (k.z * k.z);
@@ -242,14 +258,17 @@ __global__ void loadFieldsKernel(Params P, int n, const int *orig, const double 
     } else {
         float4 x = F.aux[s];
         if (densities) {
+            const double dev = densities[o] - deviationReference;
             k.w = (float)densities[o];
-            x.y = (float)(densities[o] - deviationReference);
+            x.y = (float)dev;
+            low.w = (float)(dev - (double)x.y);
         }
         x.z = F.pb[s].w / k.w;
         x.x = p / (k.w * k.w);
         F.aux[s] = x;
     }
     F.kin[s] = k;
+    F.low[s] = low;
 }
 
 __global__ void refreshDensityKernel(int n, const double *rho, float *out)
@@ -338,9 +357,17 @@ __global__ void pullKernel(int n, MasterView M, Frame F, const float4 *acc, Pull
     if (R.rho) R.rho[o] = M.rho[s];
     if (R.m) R.m[o] = M.m[s];
     if (R.h) R.h[o] = M.h[s];
-    if (R.p) R.p[o] = (double)pressureOf<D>(F, s);
+    if (R.p) {
+        if (R.framed) {
+            R.p[o] = (double)pressureOf<D>(F, s);
+        } else {
+            Params P{};
+            P.rho0 = R.rho0; P.stiffness = R.stiffness; P.tension = R.tension;
+            R.p[o] = (double)(float)taitPressure(P, M.rho[s], M.fluid[s] != 0);
+        }
+    }
     if (R.a) {
-        const float4 q = acc[s];
+        const float4 q = R.framed ? acc[s] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         const float c[3] = {q.x, q.y, q.z};
         for (int a = 0; a < D; ++a) R.a[o * D + a] = (double)c[a];
     }
@@ -582,6 +609,11 @@ void launchLoadMaster(int n, int dim, const double *x, const double *v, const do
 }
 
 void launchStepEnd(Control *ctl, cudaStream_t st) { stepEndKernel<<<1, 1, 0, st>>>(ctl); }
+
+cudaError_t kernelAttributes(cudaFuncAttributes *attributes)
+{
+    return cudaFuncGetAttributes(attributes, gatherKernel);
+}
 
 void launchEnforce(const Params &P, const Frame &F, const Enforcement &E, cudaStream_t st)
 {

@@ -95,6 +95,9 @@ void launchLoadFields(const Params &P, int n, const int *orig, const double *v, 
                       double deviationReference, const Frame &F, cudaStream_t st);
 void launchLoadMaster(int n, int dim, const double *x, const double *v, const double *rho, const double *m,
                       const uint8_t *fluid, const double *h, double hDefault, const MasterView &M, cudaStream_t st);
+// The attributes of one of the library's kernels as loaded on the current device (binaryVersion:
+// the architecture the kernels were compiled for, 100 for sm_100a).
+cudaError_t kernelAttributes(cudaFuncAttributes *attributes);
 void launchStepEnd(Control *ctl, cudaStream_t st);
 void launchEnforce(const Params &P, const Frame &F, const Enforcement &E, cudaStream_t st);
 // Sums `count` columns of n rows, `stride` doubles apart, each in a fixed order, into out[0 .. count).
@@ -106,6 +109,11 @@ void launchRefreshDensity(int n, const double *rho, float *out, cudaStream_t st)
 struct PullRows {
     double *x, *v, *rho, *m, *h, *p, *a;
     uint8_t *fluid;
+    // framed: the frame holds this state's pressures and a step's accelerations.  When it does not
+    // (a push, a split or a merge since the last step), p is the Tait pressure of the master density,
+    // the pressure the next frame will hold, and a is zero: no step has taken it for this state.
+    int framed, tension;
+    double rho0, stiffness;
 };
 // Every asked field in one pass: slot s to caller place M.orig[s]; p from the frame, a from acc.
 void launchPull(int n, int dim, const MasterView &M, const Frame &F, const float4 *acc, const PullRows &R,

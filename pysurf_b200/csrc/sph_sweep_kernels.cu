@@ -29,6 +29,16 @@ namespace sph {
 // accumulators need about 100 registers a thread in 2D (5 blocks of 128 threads leave 102).
 template <int D>
 constexpr int budgetMinBlocks() { return D == 2 ? 5 : 4; }
+// The gradients and continuity sweeps carry float64 sums beside their float32 ones (M; the wall pairs'
+// terms), so they take more registers a thread and fewer resident blocks.
+#ifndef SPH_PRECISE_MIN_BLOCKS
+#define SPH_PRECISE_MIN_BLOCKS 6
+#endif
+#ifndef SPH_PRECISE_MIN_BLOCKS_3D
+#define SPH_PRECISE_MIN_BLOCKS_3D 5
+#endif
+template <int D>
+constexpr int preciseMinBlocks() { return D == 2 ? SPH_PRECISE_MIN_BLOCKS : SPH_PRECISE_MIN_BLOCKS_3D; }
 
 // ------------------------------------------------------------------------------------------
 // The neighbour table
@@ -503,6 +513,12 @@ wallPressureKernel(Params P, Frame F, const Control *ctl, int writeDensity)
 // Sweep B: G, L and grad rho from one pass
 // ------------------------------------------------------------------------------------------
 
+// M (for L) is summed in float64 from float64 kernel gradients: L multiplies continuity's cancelling
+// terms (a wall's velocity jump), where an L off by float32's summation error would move the rate by
+// more than 1e-5 of its largest value against the float64 sums.  Its upper triangle, packed.
+template <int D>
+__device__ __forceinline__ constexpr int packed(int a, int b) { return a * D - a * (a - 1) / 2 + (b - a); }
+
 template <int D, int K>
 struct GradientVisit {
     static constexpr bool kSkipCoincident = true;
@@ -511,26 +527,34 @@ struct GradientVisit {
     Smoothing<K, D> kernel;
     bool wantG, wantL, wantRho;
     float vi[3], devI;
-    float S[3][3], Mf[3][3], M[3][3], gsum[3];
+    float S[3][3], Mf[D * (D + 1) / 2], gsum[3];     // Mf: its upper triangle, packed
+    double M[D * (D + 1) / 2];
     __device__ bool accept(bool) const { return true; }
     __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int, const float4 &B,
                                const float4 &Kj)
     {
         const KernelAt k = kernel.at(h);
         const float4 X = auxRow<D>(F, j);
+        if (wantL) {
+            double dd[3] = {(double)d[0], (double)d[1], (double)d[2]}, r2 = 0.0;
+            for (int a = 0; a < D; ++a) r2 = fma(dd[a], dd[a], r2);
+            const double rf = (double)r, rr = fma(fma(-rf, rf, r2), 0.5 / rf, rf);
+            const double w64 = (double)volumeIn<D>(B, X) * kernelGradient64<K>(rr, k);
+            for (int a = 0; a < D; ++a) {
+                const double wa = -w64 * dd[a];
+                for (int b = a; b < D; ++b) M[packed<D>(a, b)] = fma(wa, dd[b], M[packed<D>(a, b)]);
+            }
+        }
         float w = volumeIn<D>(B, X) * kernelGradient<K>(r * k.invH, k);
         if (wantG && fluidJ) {
             float vj[3];
             velocityIn<D>(Kj, vj);
-            for (int a = 0; a < D; ++a)
-                for (int b = 0; b < D; ++b) {
-                    S[a][b] += w * (vj[a] - vi[a]) * d[b];
-                    Mf[a][b] += -w * d[a] * d[b];
-                }
+            for (int a = 0; a < D; ++a) {
+                for (int b = 0; b < D; ++b) S[a][b] += w * (vj[a] - vi[a]) * d[b];
+                const float wa = -w * d[a];
+                for (int b = a; b < D; ++b) Mf[packed<D>(a, b)] += wa * d[b];
+            }
         }
-        if (wantL)
-            for (int a = 0; a < D; ++a)
-                for (int b = 0; b < D; ++b) M[a][b] += -w * d[a] * d[b];
         if (wantRho) {
             float t = w * (deviationIn<D>(B, X) - devI);
             for (int a = 0; a < D; ++a) gsum[a] += t * d[a];
@@ -546,7 +570,7 @@ __device__ __forceinline__ void groupSumMatrix(float M[3][3], unsigned mask)
 }
 
 template <int D, int K, int T, bool FINE>
-__global__ void __launch_bounds__(kBlock, sweepMinBlocks<D>())
+__global__ void __launch_bounds__(kBlock, preciseMinBlocks<D>())
 gradientKernel(Params P, Frame F, const Control *ctl, int wantG, int wantL, int wantRho, float floorDet)
 {
     if (ctl && !ctl->active) return;
@@ -568,19 +592,28 @@ gradientKernel(Params P, Frame F, const Control *ctl, int wantG, int wantL, int 
     visit.devI = deviationOf<D>(F, i);
     for (int a = 0; a < 3; ++a) {
         visit.gsum[a] = 0.0f;
-        for (int b = 0; b < 3; ++b) { visit.S[a][b] = 0.0f; visit.Mf[a][b] = 0.0f; visit.M[a][b] = 0.0f; }
+        for (int b = 0; b < 3; ++b) visit.S[a][b] = 0.0f;
     }
+    for (int q = 0; q < D * (D + 1) / 2; ++q) { visit.M[q] = 0.0; visit.Mf[q] = 0.0f; }
     forEachNeighbour<D, T, FINE>(P, F, i, G.t, hs, visit);
-    if (wantG) { groupSumMatrix<D, T>(visit.S, G.mask); groupSumMatrix<D, T>(visit.Mf, G.mask); }
-    if (wantL || wantRho) groupSumMatrix<D, T>(visit.M, G.mask);
+    float Mf[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    if (wantG) {
+        groupSumMatrix<D, T>(visit.S, G.mask);
+        for (int a = 0; a < D; ++a)
+            for (int b = a; b < D; ++b) Mf[a][b] = Mf[b][a] = groupSum<T>(visit.Mf[packed<D>(a, b)], G.mask);
+    }
+    double M[3][3] = {{1.0, 0.0, 0.0}, {0.0, 1.0, 0.0}, {0.0, 0.0, 1.0}};
+    if (wantL || wantRho)
+        for (int a = 0; a < D; ++a)
+            for (int b = a; b < D; ++b) M[a][b] = M[b][a] = groupSum<T>(visit.M[packed<D>(a, b)], G.mask);
     if (wantRho)
         for (int a = 0; a < D; ++a) visit.gsum[a] = groupSum<T>(visit.gsum[a], G.mask);
     if (G.t != 0) return;
     if (wantG) {
         float Gm[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
-        if (determinant<D>(visit.Mf) >= floorDet) {
+        if (determinant<D>(Mf) >= floorDet) {
             float inv[3][3];
-            inverse<D>(visit.Mf, inv);
+            inverse<D>(Mf, inv);
             for (int a = 0; a < D; ++a)
                 for (int b = 0; b < D; ++b) {
                     float t = 0.0f;
@@ -591,8 +624,14 @@ gradientKernel(Params P, Frame F, const Control *ctl, int wantG, int wantL, int 
         storeMatrix<D>(F.G0, F.G1, F.G2, i, Gm);
     }
     if (wantL || wantRho) {
+        // L = M^-1 in float64, rounded once
         float L[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
-        if (determinant<D>(visit.M) >= floorDet) inverse<D>(visit.M, L);
+        if (determinant<D>(M) >= (double)floorDet) {
+            double inv[3][3];
+            inverse<D>(M, inv);
+            for (int a = 0; a < D; ++a)
+                for (int b = 0; b < D; ++b) L[a][b] = (float)inv[a][b];
+        }
         if (wantL) storeMatrix<D>(F.L0, F.L1, F.L2, i, L);
         if (wantRho) {
             float g[3] = {0.0f, 0.0f, 0.0f};
@@ -851,10 +890,12 @@ __global__ void kickKernel(Params P, Frame F, Control *ctl)
         for (int c = 0; c < D; ++c) work += (double)P.g[c] * mean[c];
         addEnergy(P, F, i, kGravityWork, m * work * dt);
     }
-    float4 k = F.kin[i];
+    float4 k = F.kin[i], low = F.low[i];
     k.x = (float)v[0]; k.y = (float)v[1];
-    if (D == 3) k.z = (float)v[2];
+    low.x = (float)(v[0] - (double)k.x); low.y = (float)(v[1] - (double)k.y);
+    if (D == 3) { k.z = (float)v[2]; low.z = (float)(v[2] - (double)k.z); }
     F.kin[i] = k;
+    F.low[i] = low;
 }
 
 // Drift (src/pysurf/sphGpu.py:1142-1186), the periodic wrap and the enforcement of one fluid slot.
@@ -888,7 +929,15 @@ __device__ __forceinline__ void driftAndEnforce(const Params &P, const Frame &F,
 
 // BUDGET: the rate split for the energy budget too: the plain sum over fluid and over boundary
 // neighbours, the corrected sum (the correction's part is its difference) and the diffusion
-// (src/pysurf/sphGpu.py:476-545).  COMP: the sum compensated (Dot2), its running error in comp.
+// (src/pysurf/sphGpu.py:476-545).  COMP: the float32 sum compensated (Dot2), its running error in comp.
+//
+// The rate's terms cancel: next to a wall a particle's velocity jumps to the boundary's zero, and
+// sum_j m_j (v_i - v_j) . grad W_ij over a near-symmetric support is a small remainder of large
+// terms.  So each term keeps float64's digits where that matters: velocity and deviation differences
+// come from the float32 values and their remainders (the frame's low row), and the pairs of a fluid
+// and a boundary particle -- every pair of a boundary row, the wall's pairs of a fluid row -- take
+// their separation, distance, kernel gradient and term in float64, summed apart in float64 (cross).
+// Fluid pairs, whose velocity differences are small, keep float32 arithmetic.
 template <int D, int K, bool BUDGET, bool COMP = false>
 struct ContinuityVisit {
     static constexpr bool kSkipCoincident = true;
@@ -896,28 +945,76 @@ struct ContinuityVisit {
     static constexpr bool kBoundaryRows = true;         // every row
     const Params &P; const Frame &F;
     Smoothing<K, D> S;
+    int self;               // this particle's slot
     bool boundaryI, diffuses, corrected;
-    float vi[3], devI, Li[3][3], gi[3];
+    float vi[3], vlI[3], devI, devLoI, Li[3][3], gi[3];
     float deltaI;           // closure: this particle's eddy delta
     float total, comp;
+    double cross;           // the fluid-boundary pairs' terms in float64
     float plainFluid, plainWall, continuity, diffusive;     // BUDGET
     __device__ bool accept(bool fluidJ) const { return !(boundaryI && !fluidJ); }
-    __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int, const float4 &B,
+    __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int image, const float4 &B,
                                const float4 &Kj)
     {
         const KernelAt k = S.at(h);
-        const float grad = kernelGradient<K>(r * k.invH, k);    // (dW/dr) / r
         float vj[3];
         velocityIn<D>(Kj, vj);
+        const float4 lowJ = __ldg(&F.low[j]);
+        const float vlJ[3] = {lowJ.x, lowJ.y, lowJ.z};
+        if (boundaryI == fluidJ) {
+            // a fluid-boundary pair, in float64: x_i - x_j from the points and remainders, the distance
+            // by one Newton step from the float32 root, (dW/dr) / r, (v_i - v_j) . L_i (x_i - x_j)
+            const float4 A = __ldg(&F.pa[j]);
+            float pi[3], li[3], pj[3], lj[3];
+            pointOf<D>(F, self, pi);
+            remainderOf<D>(F, self, li);
+            pointIn<D>(A, pj);
+            remainderIn<D>(A, B, lj);
+            double dd[3] = {0.0, 0.0, 0.0}, r2 = 0.0;
+            for (int a = 0; a < D; ++a) {
+                dd[a] = ((double)pi[a] - (double)pj[a]) + ((double)li[a] - (double)lj[a]);
+                if (a == 1 && image) dd[a] += pi[1] < 0.5f * P.periodF ? P.period : -P.period;
+                r2 = fma(dd[a], dd[a], r2);
+            }
+            const double rf = (double)r, rr = fma(fma(-rf, rf, r2), 0.5 / rf, rf);
+            const double grad = kernelGradient64<K>(rr, k);
+            double dot = 0.0;
+            for (int a = 0; a < D; ++a) {
+                double ld = dd[a];
+                if (corrected) {
+                    ld = 0.0;
+                    for (int b = 0; b < D; ++b) ld = fma((double)Li[a][b], dd[b], ld);
+                }
+                dot = fma(((double)vi[a] + (double)vlI[a]) - ((double)vj[a] + (double)vlJ[a]), ld, dot);
+            }
+            const double term = (double)massIn<D>(B) * dot * grad;
+            cross += term;
+            if constexpr (BUDGET) {
+                double plainDot = dot;
+                if (corrected) {
+                    plainDot = 0.0;
+                    for (int a = 0; a < D; ++a)
+                        plainDot = fma(((double)vi[a] + (double)vlI[a]) - ((double)vj[a] + (double)vlJ[a]), dd[a], plainDot);
+                }
+                const float plain = (float)((double)massIn<D>(B) * plainDot * grad);
+                continuity = __fadd_rn(continuity, (float)term);
+                if (fluidJ) plainFluid += plain; else plainWall += plain;
+            }
+            return;     // a pair with a boundary member does not diffuse
+        }
+        const float grad = kernelGradient<K>(r * k.invH, k);    // (dW/dr) / r
+        float dv[3];
+        for (int a = 0; a < D; ++a)
+            dv[a] = __fadd_rn(__fsub_rn(vi[a], vj[a]), __fsub_rn(vlI[a], vlJ[a]));
         float dot = 0.0f;
         if (corrected) {
             for (int a = 0; a < D; ++a) {
                 float ld = 0.0f;
                 for (int b = 0; b < D; ++b) ld += Li[a][b] * d[b];
-                dot += (vi[a] - vj[a]) * ld;
+                dot += dv[a] * ld;
             }
         } else {
-            for (int a = 0; a < D; ++a) dot += (vi[a] - vj[a]) * d[a];
+            for (int a = 0; a < D; ++a) dot += dv[a] * d[a];
         }
         // explicit roundings on the sum's path (see the momentum sweep)
         const float massDot = massIn<D>(B) * dot;
@@ -927,7 +1024,7 @@ struct ContinuityVisit {
             float plainDot = dot;
             if (corrected) {
                 plainDot = 0.0f;
-                for (int a = 0; a < D; ++a) plainDot += (vi[a] - vj[a]) * d[a];
+                for (int a = 0; a < D; ++a) plainDot += dv[a] * d[a];
             }
             const float plain = massIn<D>(B) * plainDot * grad;
             continuity = __fmaf_rn(massDot, grad, continuity);
@@ -935,13 +1032,28 @@ struct ContinuityVisit {
         }
         if (diffuses && fluidJ) {
             const float4 X = auxRow<D>(F, j);
-            float devJ = deviationIn<D>(B, X);
-            float difference = devJ - devI;
+            const float devJ = deviationIn<D>(B, X);
+            // rho_j - rho_i from the float32 deviations and their remainders, so it keeps float64's
+            // digits (the leading difference is exact for neighbours' nearly equal deviations)
+            const float remainder = __fsub_rn(lowJ.w, devLoI);
+            float difference;
             if (P.diffusion == 2) {
-                float ratio = 1.0f + 0.5f * (devI + devJ) / P.rho0F;
-                float sq = ratio * ratio;
-                difference -= __fdividef(P.rho0F * P.gravityOverSound * d[D - 1], sq * sq * ratio);
-            } else if (P.diffusion == 3) {
+                // less the hydrostatic difference k dz (1 + e)^-5 (src/pysurf/sphSolver.py:718-735), with
+                // k = rho0 g / c0^2 and e the pair's mean deviation over rho0.  Near rest it cancels most
+                // of rho_j - rho_i, so it is taken in two parts: k dz off the leading difference in one
+                // fused rounding, then the small k dz e S / (1 + e)^5 back on, where
+                // S = 1 + (1 + e) + ... + (1 + e)^4 makes (1 + e)^5 - 1 = e S without cancelling.
+                const float e = __fmul_rn(__fadd_rn(devI, devJ), P.halfInvRho0);
+                const float ratio = __fadd_rn(1.0f, e), sq = __fmul_rn(ratio, ratio), fifth = __fmul_rn(__fmul_rn(sq, sq), ratio);
+                const float S = __fadd_rn(__fadd_rn(__fadd_rn(1.0f, ratio), __fadd_rn(sq, __fmul_rn(sq, ratio))),
+                                          __fmul_rn(sq, sq));
+                const float slope = __fmul_rn(P.hydrostaticSlope, d[D - 1]);
+                const float leading = __fmaf_rn(-P.hydrostaticSlope, d[D - 1], __fsub_rn(devJ, devI));
+                difference = __fadd_rn(__fadd_rn(leading, remainder), __fdividef(__fmul_rn(__fmul_rn(slope, e), S), fifth));
+            } else {
+                difference = __fadd_rn(__fsub_rn(devJ, devI), remainder);
+            }
+            if (P.diffusion == 3) {
                 float4 gj = __ldg(&F.gradRho[j]);
                 float gjv[3] = {gj.x, gj.y, gj.z};
                 float t = 0.0f;
@@ -966,7 +1078,7 @@ struct ContinuityVisit {
 
 // mode 0: the rate only; 1: advance the density; 2: advance, drift and enforce.
 template <int D, int K, int T, bool BUDGET, bool FINE, bool COMP = false>
-__global__ void __launch_bounds__(kBlock, BUDGET ? budgetMinBlocks<D>() : sweepMinBlocks<D>())
+__global__ void __launch_bounds__(kBlock, BUDGET ? budgetMinBlocks<D>() : preciseMinBlocks<D>())
 continuityKernel(Params P, Frame F, Control *ctl, Enforcement E, int mode)
 {
     if (ctl && !ctl->active) return;
@@ -979,6 +1091,11 @@ continuityKernel(Params P, Frame F, Control *ctl, Enforcement E, int mode)
     visit.diffuses = P.diffusion != 0 && !visit.boundaryI;
     visit.corrected = P.corrected && !visit.boundaryI;
     velocityOf<D>(F, i, visit.vi);
+    const float4 lowI = F.low[i];
+    visit.vlI[0] = lowI.x; visit.vlI[1] = lowI.y; visit.vlI[2] = lowI.z;
+    visit.devLoI = lowI.w;
+    visit.self = i;
+    visit.cross = 0.0;
     visit.devI = deviationOf<D>(F, i);
     visit.deltaI = P.closure && visit.diffuses ? F.eddy[i].y : 0.0f;
     if (visit.corrected) loadMatrix<D>(F.L0, F.L1, F.L2, i, visit.Li);
@@ -993,6 +1110,8 @@ continuityKernel(Params P, Frame F, Control *ctl, Enforcement E, int mode)
     float rate;
     if constexpr (COMP) rate = groupSumCompensated<T>(visit.total, visit.comp, G.mask);
     else rate = groupSum<T>(visit.total, G.mask);
+    // the fluid-boundary pairs' float64 sum joins before the one rounding to float32
+    rate = (float)((double)rate + groupSum<T>(visit.cross, G.mask));
     float parts[4] = {0.0f, 0.0f, 0.0f, 0.0f};
     if constexpr (BUDGET) {
         const float plainFluid = groupSum<T>(visit.plainFluid, G.mask);

@@ -64,6 +64,13 @@ __device__ __forceinline__ float groupSum(float value, unsigned mask)
     return value;
 }
 
+template <int T>
+__device__ __forceinline__ double groupSum(double value, unsigned mask)
+{
+    for (int offset = T / 2; offset > 0; offset >>= 1) value += __shfl_xor_sync(mask, value, offset, T);
+    return value;
+}
+
 // Compensated accumulation (Ogita, Rump and Oishi, "Accurate sum and dot product", SIAM J. Sci.
 // Comput. 26 (2005), Dot2): a running sum s with a running error c.  Each term a b enters as its
 // rounded product p and the product's exact error fma(a, b, -p); Knuth's TwoSum gives the exact

@@ -146,7 +146,7 @@ struct SphSystem {
     MasterView master[2]{};
     float4 *pa = nullptr, *pb = nullptr, *kin = nullptr, *G[3] = {}, *L[3] = {}, *gradRho = nullptr, *acc = nullptr,
            *vec = nullptr;
-    float4 *aux = nullptr;
+    float4 *aux = nullptr, *low = nullptr;
     float *pres = nullptr, *rate = nullptr, *scalar = nullptr;
     int *cell = nullptr, *cellStart = nullptr;
     CellSortBuffers sortBuffers = {};
@@ -197,7 +197,7 @@ struct SphSystem {
             cudaFree(M.rho); cudaFree(M.m); cudaFree(M.h); cudaFree(M.fluid); cudaFree(M.orig);
             M = MasterView{};
         }
-        void *ptrs[] = {pa, pb, kin, G[0], G[1], G[2], L[0], L[1], L[2], gradRho, acc, vec, aux, pres, rate,
+        void *ptrs[] = {pa, pb, kin, G[0], G[1], G[2], L[0], L[1], L[2], gradRho, acc, vec, aux, low, pres, rate,
                         scalar, cell, sortBuffers.slotCell, sortBuffers.slotWithin, sortBuffers.perm,
                         sortBuffers.bucket, dStage, dStageU8, dRank, nbr, ncount, eddy, shiftGrad, shiftPlain,
                         shiftRhoGrad, shiftOut, shiftDv};
@@ -210,7 +210,7 @@ struct SphSystem {
         listDirty = true;
         pa = pb = kin = gradRho = acc = vec = nullptr;
         for (int a = 0; a < 3; ++a) G[a] = L[a] = nullptr;
-        aux = nullptr; pres = rate = scalar = nullptr; cell = nullptr;
+        aux = low = nullptr; pres = rate = scalar = nullptr; cell = nullptr;
         sortBuffers.slotCell = sortBuffers.slotWithin = sortBuffers.perm = nullptr;
         sortBuffers.bucket = nullptr;
         dStage = nullptr; dStageU8 = nullptr; dRank = nullptr;
@@ -270,6 +270,7 @@ struct SphSystem {
         TRY(deviceAlloc(&pb, cap));
         TRY(deviceAlloc(&kin, cap));
         TRY(deviceAlloc(&aux, cap));
+        TRY(deviceAlloc(&low, cap));
         TRY(deviceAlloc(&pres, cap));
         for (int a = 0; a < 3; ++a) { TRY(deviceAlloc(&G[a], cap)); TRY(deviceAlloc(&L[a], cap)); }
         TRY(deviceAlloc(&gradRho, cap));
@@ -294,6 +295,7 @@ struct SphSystem {
         CUDA_TRY(cudaMemsetAsync(acc, 0, sizeof(float4) * cap, stream));
         CUDA_TRY(cudaMemsetAsync(kin, 0, sizeof(float4) * cap, stream));
         CUDA_TRY(cudaMemsetAsync(aux, 0, sizeof(float4) * cap, stream));
+        CUDA_TRY(cudaMemsetAsync(low, 0, sizeof(float4) * cap, stream));
         CUDA_TRY(cudaMemsetAsync(pres, 0, sizeof(float) * cap, stream));
         CUDA_TRY(cudaMemsetAsync(eddy, 0, sizeof(float2) * cap, stream));
         graphDirty = true;
@@ -459,11 +461,11 @@ struct SphSystem {
         P.stiffness = rho0 * c0 * c0 / 7.0;
         P.densityFloor = densityFloor;
         P.devReference = diffusionRho0;
-        P.rho0F = (float)diffusionRho0;
+        P.halfInvRho0 = (float)(0.5 / diffusionRho0);
         P.tension = tension;
         P.diffusion = diffusionMode;
         P.diffusionFactor = (float)(2.0 * diffusionDelta * diffusionC0);
-        P.gravityOverSound = (float)(diffusionG / (diffusionC0 * diffusionC0));
+        P.hydrostaticSlope = (float)(diffusionRho0 * diffusionG / (diffusionC0 * diffusionC0));
         P.corrected = corrected;
         P.limited = limited;
         P.closure = closure;
@@ -490,7 +492,7 @@ struct SphSystem {
     Frame frame() const
     {
         Frame F{};
-        F.pa = pa; F.pb = pb; F.kin = kin; F.aux = aux; F.pres = pres;
+        F.pa = pa; F.pb = pb; F.kin = kin; F.aux = aux; F.low = low; F.pres = pres;
         F.cell = cell; F.cellStart = cellStart;
         F.G0 = G[0]; F.G1 = G[1]; F.G2 = G[2];
         F.L0 = L[0]; F.L1 = L[1]; F.L2 = L[2];
@@ -599,19 +601,19 @@ struct SphSystem {
     // ---- staging -------------------------------------------------------------------------------
 
     // Copy a caller array of `count` elements of `size` bytes to device memory at `dst`.
-    int upload(void *dst, const void *src, size_t bytes)
+    int upload(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind = cudaMemcpyHostToDevice)
     {
         if (bytes == 0) return SPH_OK;
         // pinned caller memory copies by DMA behind the return; pageable memory is staged by the
-        // driver before the call returns
-        CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream));
+        // driver before the call returns; device memory (kind DeviceToDevice) copies in stream order
+        CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, kind, stream));
         return SPH_OK;
     }
 
-    int download(void *dst, const void *src, size_t bytes)
+    int download(void *dst, const void *src, size_t bytes, cudaMemcpyKind kind = cudaMemcpyDeviceToHost)
     {
         if (bytes == 0) return SPH_OK;
-        CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, stream));
+        CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, kind, stream));
         return SPH_OK;
     }
 
@@ -648,6 +650,15 @@ extern "C" {
 const char *sph_last_error(void) { return lastError.c_str(); }
 
 int sph_version(void) { return 1; }
+
+int sph_kernel_architecture(int *version)
+{
+    if (!version) return fail(SPH_ERR_INVALID, "null output");
+    cudaFuncAttributes attributes{};
+    CUDA_TRY(kernelAttributes(&attributes));
+    *version = attributes.binaryVersion;
+    return SPH_OK;
+}
 
 int sph_create(int dimensions, double smoothing_length, const double *domain_min, const double *domain_max,
                double period, int precise, int kernel_type, int device, SphSystem **out)
@@ -936,12 +947,25 @@ int sph_set_physics(SphSystem *sys, double reference_density, double sound_speed
 
 // ---- host steps -------------------------------------------------------------------------------
 
+// kind: cudaMemcpyHostToDevice for the caller's host arrays, cudaMemcpyDeviceToDevice for its
+// device arrays (the lengths, which the host checks, are then read back first).
 static int loadState(SphSystem *sys, int64_t count, const double *positions, const double *velocities,
-                     const double *densities, const double *masses, const uint8_t *is_fluid, const double *lengths)
+                     const double *densities, const double *masses, const uint8_t *is_fluid, const double *lengths,
+                     cudaMemcpyKind kind = cudaMemcpyHostToDevice)
 {
     if (count < 0 || count > (int64_t)0x3FFFFFFF) return fail(SPH_ERR_INVALID, "particle count out of range");
     if (count > 0 && (!positions || !masses || !is_fluid)) return fail(SPH_ERR_INVALID, "null state array");
     int n = (int)count;
+    const double *deviceLengths = nullptr;
+    std::vector<double> hostLengths;
+    if (kind == cudaMemcpyDeviceToDevice && lengths && n > 0) {
+        deviceLengths = lengths;
+        hostLengths.resize(n);
+        CUDA_TRY(cudaMemcpyAsync(hostLengths.data(), deviceLengths, sizeof(double) * n, cudaMemcpyDeviceToHost,
+                                 sys->stream));
+        CUDA_TRY(cudaStreamSynchronize(sys->stream));
+        lengths = hostLengths.data();
+    }
     double hMax = 0.0, hMin = sys->h;
     bool mixed = false;
     if (lengths && n > 0) {
@@ -968,12 +992,13 @@ static int loadState(SphSystem *sys, int64_t count, const double *positions, con
     if (n == 0) return SPH_OK;
     int dim = sys->dim;
     double *sx = sys->stage(0), *sv = sys->stage(3), *srho = sys->stage(6), *sm = sys->stage(7), *sh = sys->stage(8);
-    TRY(sys->upload(sx, positions, sizeof(double) * n * dim));
-    if (velocities) TRY(sys->upload(sv, velocities, sizeof(double) * n * dim));
-    if (densities) TRY(sys->upload(srho, densities, sizeof(double) * n));
-    TRY(sys->upload(sm, masses, sizeof(double) * n));
-    if (lengths) TRY(sys->upload(sh, lengths, sizeof(double) * n));
-    TRY(sys->upload(sys->dStageU8, is_fluid, n));
+    TRY(sys->upload(sx, positions, sizeof(double) * n * dim, kind));
+    if (velocities) TRY(sys->upload(sv, velocities, sizeof(double) * n * dim, kind));
+    if (densities) TRY(sys->upload(srho, densities, sizeof(double) * n, kind));
+    TRY(sys->upload(sm, masses, sizeof(double) * n, kind));
+    if (deviceLengths) TRY(sys->upload(sh, deviceLengths, sizeof(double) * n, kind));
+    else if (lengths) TRY(sys->upload(sh, lengths, sizeof(double) * n));
+    TRY(sys->upload(sys->dStageU8, is_fluid, n, kind));
     CUDA_TRY(cudaEventRecord(sys->uploaded, sys->stream));
     sys->cur = 0;
     launchLoadMaster(n, dim, sx, velocities ? sv : nullptr, densities ? srho : nullptr, sm, sys->dStageU8,
@@ -993,6 +1018,8 @@ int sph_update(SphSystem *sys, int64_t n, const double *positions, const double 
     sys->rebuild();
     if (sys->listDirty) TRY(sys->sizeList());
     CUDA_TRY(cudaGetLastError());
+    // the caller's arrays are free once the copies in are done (pinned memory copies behind the return)
+    if (sys->n > 0) CUDA_TRY(cudaEventSynchronize(sys->uploaded));
     return SPH_OK;
 }
 
@@ -1226,12 +1253,13 @@ int sph_density_gradients(SphSystem *sys, const double *densities, double *out)
 
 // ---- device-resident steps ------------------------------------------------------------------------
 
-int sph_push(SphSystem *sys, int64_t n, const double *positions, const double *velocities, const double *densities,
-             const double *masses, const uint8_t *is_fluid, const double *lengths)
+static int pushState(SphSystem *sys, int64_t n, const double *positions, const double *velocities,
+                     const double *densities, const double *masses, const uint8_t *is_fluid, const double *lengths,
+                     cudaMemcpyKind kind)
 {
     CHECK_SYS(sys);
     if (n > 0 && (!velocities || !densities)) return fail(SPH_ERR_INVALID, "null state array");
-    TRY(loadState(sys, n, positions, velocities, densities, masses, is_fluid, lengths));
+    TRY(loadState(sys, n, positions, velocities, densities, masses, is_fluid, lengths, kind));
     sys->resident = true;
     // the cell list, the frame and the table follow at the first step or host-step call; the table
     // keeps its row length unless the count changed (a particle whose row is too short walks)
@@ -1244,6 +1272,18 @@ int sph_push(SphSystem *sys, int64_t n, const double *positions, const double *v
     // behind the return, in stream order before any later call's work
     CUDA_TRY(sys->n > 0 ? cudaEventSynchronize(sys->uploaded) : cudaStreamSynchronize(sys->stream));
     return SPH_OK;
+}
+
+int sph_push(SphSystem *sys, int64_t n, const double *positions, const double *velocities, const double *densities,
+             const double *masses, const uint8_t *is_fluid, const double *lengths)
+{
+    return pushState(sys, n, positions, velocities, densities, masses, is_fluid, lengths, cudaMemcpyHostToDevice);
+}
+
+int sph_push_device(SphSystem *sys, int64_t n, const double *positions, const double *velocities,
+                    const double *densities, const double *masses, const uint8_t *is_fluid, const double *lengths)
+{
+    return pushState(sys, n, positions, velocities, densities, masses, is_fluid, lengths, cudaMemcpyDeviceToDevice);
 }
 
 int sph_frame(SphSystem *sys, float *positions, float *speeds, uint8_t *is_fluid)
@@ -1272,8 +1312,8 @@ int sph_count(const SphSystem *sys, int64_t *n)
     return SPH_OK;
 }
 
-int sph_pull(SphSystem *sys, double *positions, double *velocities, double *densities, double *pressures,
-             double *accelerations, double *masses, double *lengths, uint8_t *is_fluid)
+static int pullState(SphSystem *sys, double *positions, double *velocities, double *densities, double *pressures,
+                     double *accelerations, double *masses, double *lengths, uint8_t *is_fluid, cudaMemcpyKind kind)
 {
     CHECK_SYS(sys);
     int n = sys->n, dim = sys->dim;
@@ -1293,23 +1333,41 @@ int sph_pull(SphSystem *sys, double *positions, double *velocities, double *dens
     R.rho = rows(densities, 1);
     R.m = rows(masses, 1);
     R.h = rows(lengths, 1);
-    R.p = sys->framed ? rows(pressures, 1) : nullptr;
+    R.p = rows(pressures, 1);
     R.a = rows(accelerations, dim);
     R.fluid = is_fluid ? sys->dStageU8 : nullptr;
+    R.framed = sys->framed ? 1 : 0;
+    R.tension = sys->tension;
+    R.rho0 = sys->rho0;
+    R.stiffness = sys->rho0 * sys->c0 * sys->c0 / 7.0;
     launchPull(n, dim, sys->master[sys->cur], sys->frame(), sys->acc, R, sys->stream);
     CUDA_TRY(cudaGetLastError());
     const size_t column = sizeof(double) * (size_t)n;
-    if (R.x) TRY(sys->download(positions, R.x, column * dim));
-    if (R.v) TRY(sys->download(velocities, R.v, column * dim));
-    if (R.rho) TRY(sys->download(densities, R.rho, column));
-    if (R.m) TRY(sys->download(masses, R.m, column));
-    if (R.h) TRY(sys->download(lengths, R.h, column));
-    if (R.p) TRY(sys->download(pressures, R.p, column));
-    if (R.a) TRY(sys->download(accelerations, R.a, column * dim));
-    if (R.fluid) TRY(sys->download(is_fluid, R.fluid, (size_t)n));
+    if (R.x) TRY(sys->download(positions, R.x, column * dim, kind));
+    if (R.v) TRY(sys->download(velocities, R.v, column * dim, kind));
+    if (R.rho) TRY(sys->download(densities, R.rho, column, kind));
+    if (R.m) TRY(sys->download(masses, R.m, column, kind));
+    if (R.h) TRY(sys->download(lengths, R.h, column, kind));
+    if (R.p) TRY(sys->download(pressures, R.p, column, kind));
+    if (R.a) TRY(sys->download(accelerations, R.a, column * dim, kind));
+    if (R.fluid) TRY(sys->download(is_fluid, R.fluid, (size_t)n, kind));
     CUDA_TRY(cudaStreamSynchronize(sys->stream));
     CUDA_TRY(cudaGetLastError());
     return SPH_OK;
+}
+
+int sph_pull(SphSystem *sys, double *positions, double *velocities, double *densities, double *pressures,
+             double *accelerations, double *masses, double *lengths, uint8_t *is_fluid)
+{
+    return pullState(sys, positions, velocities, densities, pressures, accelerations, masses, lengths, is_fluid,
+                     cudaMemcpyDeviceToHost);
+}
+
+int sph_pull_device(SphSystem *sys, double *positions, double *velocities, double *densities, double *pressures,
+                    double *accelerations, double *masses, double *lengths, uint8_t *is_fluid)
+{
+    return pullState(sys, positions, velocities, densities, pressures, accelerations, masses, lengths, is_fluid,
+                     cudaMemcpyDeviceToDevice);
 }
 
 int sph_clear_boundary(SphSystem *sys)

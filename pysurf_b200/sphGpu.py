@@ -97,6 +97,19 @@ def _deviceIndex(device) -> int:
     raise ValueError(f"Device '{device}' is not a CUDA device; the B200 backend runs on CUDA only.")
 
 
+def _checkDeviceTensor(tensor, shape, dtypes, device: int) -> None:
+    """A contiguous CUDA tensor on `device` with the shape and one of the dtypes (names), or ValueError."""
+    dtypes = (dtypes,) if isinstance(dtypes, str) else dtypes
+    if not hasattr(tensor, 'data_ptr') or not getattr(tensor, 'is_cuda', False):
+        raise ValueError('expected a CUDA tensor')
+    if tensor.device.index != device:
+        raise ValueError(f'expected a tensor on cuda:{device}, got {tensor.device}')
+    if str(tensor.dtype).replace('torch.', '') not in dtypes:
+        raise ValueError(f'expected dtype {" or ".join(dtypes)}, got {tensor.dtype}')
+    if tuple(tensor.shape) != tuple(shape) or not tensor.is_contiguous():
+        raise ValueError(f'expected a contiguous tensor of shape {tuple(shape)}, got {tuple(tensor.shape)}')
+
+
 class PairSums:
 
     """
@@ -501,6 +514,51 @@ class PairSums:
             array = getattr(particles, name)
             if value is not array:
                 array[:] = value
+
+    # -- device arrays (torch CUDA tensors) in place of host arrays -- #
+
+    def pushDevice(self, positions, velocities, densities, masses, isFluid, lengths=None) -> None:
+        """`push` from device tensors on this handle's device: float64 positions and velocities (n, dim),
+        densities and masses (n,), a uint8 or bool fluid flag (n,), and optionally the lengths (n,).
+        The state is copied device to device; nothing crosses the host but the lengths' check."""
+        n, dim = int(positions.shape[0]), self.dimensions
+        shapes = ((positions, (n, dim)), (velocities, (n, dim)), (densities, (n,)), (masses, (n,)))
+        for tensor, shape in shapes + (((lengths, (n,)),) if lengths is not None else ()):
+            _checkDeviceTensor(tensor, shape, 'float64', self.device)
+        _checkDeviceTensor(isFluid, (n,), ('uint8', 'bool'), self.device)
+        if lengths is not None and n:
+            longest = float(lengths.max())
+            if longest > self.maxLength * (1.0 + 1e-9):
+                raise ValueError(f'A smoothing length of {longest} m exceeds the {self.maxLength} m the hash '
+                                 f'grid is built for.')
+            self.minLength = float(lengths.min())
+            self.uniformLengths = bool((lengths == lengths[0]).all())
+        else:
+            self.minLength, self.uniformLengths = self.smoothingLength, True
+        self.count = n
+        check(self._lib.sph_push_device(self._handle, n, positions.data_ptr(), velocities.data_ptr(),
+                                        densities.data_ptr(), masses.data_ptr(), isFluid.data_ptr(),
+                                        None if lengths is None else lengths.data_ptr()), 'pushDevice')
+
+    def pullDevice(self, positions=None, velocities=None, densities=None, pressures=None, accelerations=None,
+                   masses=None, lengths=None, isFluid=None) -> None:
+        """`pull` into device tensors on this handle's device (float64, contiguous; isFluid uint8), any of
+        them None.  Copied device to device; the tensors hold the state when this returns."""
+        n, dim = self.count, self.dimensions
+        vectors, scalars = (positions, velocities, accelerations), (densities, pressures, masses, lengths)
+        for tensor in vectors:
+            if tensor is not None:
+                _checkDeviceTensor(tensor, (n, dim), 'float64', self.device)
+        for tensor in scalars:
+            if tensor is not None:
+                _checkDeviceTensor(tensor, (n,), 'float64', self.device)
+        if isFluid is not None:
+            _checkDeviceTensor(isFluid, (n,), 'uint8', self.device)
+        if n == 0:
+            return
+        ptr = lambda t: None if t is None else t.data_ptr()
+        check(self._lib.sph_pull_device(self._handle, ptr(positions), ptr(velocities), ptr(densities), ptr(pressures),
+                                        ptr(accelerations), ptr(masses), ptr(lengths), ptr(isFluid)), 'pullDevice')
 
     # -- the breaking tracker's reads (2D), on the device -- #
 

@@ -123,11 +123,11 @@ class Autotuner:
     def prepare(self, items, builder=None) -> dict:
         """Time a middle-sized case of every size class among `items` (cases, or specs that `builder`
         turns into cases) that has no choice yet.  Returns the classes tuned now with their tables."""
+        items = list(items)     # walked twice: a generator would be spent by the first walk
         sizes = {}
         for k, item in enumerate(items):
             case = builder(item) if builder is not None else item
             sizes.setdefault(self.classOf(case), []).append((case.state.nParticles, k))
-        items = list(items)
         tuned = {}
         for key in sorted(sizes):
             if key in self.choices:

@@ -349,6 +349,59 @@ def makeRuns():
     np.savez_compressed(os.path.join(HERE, 'runs.npz'), **out)
 
 
+def ridgeWave(particlesPerDepth=6):
+    """A small 3D tank for BreakingWave3D's deltaSph scheme on the host: a solitary wave of H/d = 0.4
+    approaching a Gaussian ridge (0.3 d high, sigma 0.8 d, its axis at 25 degrees to the crest) over a
+    height-field bed, 5 d x 1.5 d, built by the reference's own facade (src/pysurf/BreakingWave3D.py:630-700)
+    without start packing, its solver on the numpy backend."""
+    from pysurf.bathymetry import HeightField
+    from pysurf.BreakingWave3D import BreakingWave3D
+    angle = math.radians(25.0)
+
+    def ridge(x, y):
+        across = (x - 3.0) * math.cos(angle) + (y - 0.75) * math.sin(angle)
+        return 0.3 * np.exp(-across ** 2 / (2.0 * 0.8 ** 2))
+
+    field = HeightField.fromFunction(ridge, (0.0, 5.0, 0.0, 1.5), 1.0 / 32.0, stillWaterLevel=1.0)
+    wave = BreakingWave3D(field, 0.4, 2.0, particlesPerDepth=particlesPerDepth, backend='numpy', startPacking=False,
+                          endTime=0.1)
+    wave.build()
+    return wave
+
+
+def heightFieldRecord(boundary):
+    field, clearance = boundary.field, 0.25 * boundary.spacing
+    startX, endX, startY, endY = field.bounds
+    return dict(kind=3, table=field.z, gridX=field.x, gridY=field.y, bounds=list(field.bounds),
+                stillWaterLevel=field.stillWaterLevel, spacing=boundary.spacing, layers=boundary.nLayers,
+                wallTop=boundary.wallTop, offshoreWall=int(bool(boundary.offshoreWall)),
+                endWall=int(bool(boundary.endWall)),
+                params=[float(field.x[0]), float(field.y[0]), float(field.x[1] - field.x[0]),
+                        float(field.y[1] - field.y[0]), clearance, startY + clearance, endY - clearance,
+                        float(bool(boundary.offshoreWall)), startX + clearance,
+                        endX - clearance if boundary.endWall else endX])
+
+
+def makeRuns3D():
+    """Host steps of the reference's float64 numpy solver in 3D: the ridge tank above under the deltaSph
+    scheme, as it starts and after its crest splits into daughters of h / 2 (WcsphSolver.refine,
+    src/pysurf/sphSolver.py:1994-2040), the runs tests/testBreakingWave3D.py:298-347 take on the GPU."""
+    out = {}
+    for tag, steps, split in (('ridge', 25, False), ('ridgeSplit', 15, True)):
+        wave = ridgeWave()
+        solver, particles = wave.solver, wave.particles
+        if split:
+            # the crest zone: fluid within a half length of the crest and above the still water level
+            x = particles.positions
+            zone = particles.isFluid & (np.abs(x[:, 0] - wave.crestX) < 0.5) & (x[:, 2] > 1.0)
+            out[f'{tag}/splitCount'] = np.array(solver.refine(zone, lengthRatio=0.5))
+        out[f'{tag}/lengths'] = np.array(particles.lengths if particles.lengths is not None
+                                         else np.full(particles.nParticles, solver.config.smoothingLength))
+        recordRun(out, tag, solver, particles, steps, heightFieldRecord(wave.boundary))
+        print(tag, particles.nParticles, 'particles', int(particles.isFluid.sum()), 'fluid', steps, 'steps')
+    np.savez_compressed(os.path.join(HERE, 'runs3d.npz'), **out)
+
+
 def makeSplit():
     """src/pysurf/sphRefinement.py:136-190 on a small 2D and 3D set, h kept and h halved."""
     from pysurf.sphParticles import ParticleSystem
@@ -767,7 +820,7 @@ def main():
     makers = {'cellkeys': makeCellKeys, 'clouds': makeClouds, 'enforce': makeEnforcement, 'split': makeSplit,
               'beach': makeBeach, 'runs': makeRuns, 'breaking': makeBreaking, 'closure': makeClosure,
               'shifting': makeShifting, 'energy': makeEnergy, 'frames': makeFrames,
-              'merge': makeMerge}
+              'merge': makeMerge, 'runs3d': makeRuns3D}
     for name in (sys.argv[2:] or list(makers)):
         makers[name]()
     for name in sorted(os.listdir(HERE)):

@@ -3,8 +3,6 @@ import os
 import re
 import subprocess
 
-import pytest
-
 from conftest import ROOT
 
 HEADER = os.path.join(ROOT, 'include', 'pysurf_b200.h')
@@ -38,8 +36,8 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_library_is_built_for_sm_100a():
-    from pysurf_b200 import _lib
-    out = subprocess.run(['cuobjdump', '--list-elf', _lib.LIBRARY], capture_output=True, text=True)
-    if out.returncode != 0:
-        pytest.skip('cuobjdump unavailable')
-    assert 'sm_100a' in out.stdout
+    # the one architecture the build passes nvcc; on a GPU, tests/test_gpu_device_arrays.py asks the
+    # CUDA runtime which architecture the loaded kernels carry
+    from pysurf_b200 import build
+    assert build.ARCH == ['-gencode', 'arch=compute_100a,code=sm_100a']
+    assert not any(flag.startswith(('-arch', '--gpu-architecture', '-gencode')) for flag in build.FLAGS)

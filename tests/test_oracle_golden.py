@@ -125,6 +125,10 @@ def stepperFor(r, **options):
         clearance, side, width, offshore, wallX, piston, endLimit = r['boundary_params']
         boundary = ('bed', oracle.bedParams(r['boundary_bedX'], r['boundary_bedZ'], clearance, bool(side), width,
                                             bool(offshore), wallX, piston, endLimit))
+    elif int(r['boundary_kind']) == 3:
+        ox, oy, sx, sy, clearance, lowY, highY, offshore, lowX, highX = r['boundary_params']
+        boundary = ('field', oracle.fieldParams(r['boundary_table'], ox, oy, sx, sy, clearance, lowY, highY,
+                                                bool(offshore), lowX, highX))
     return oracle.Stepper(int(dim), 'wendlandC2' if int(kind) == 1 else 'cubicSpline', h, rho0, c0, alpha,
                           r['gravity'], bf, xsph, floor, modes[int(mode)], delta, bool(wall), bool(tension),
                           bool(corrected), bool(limited), cfl, maxdt, period, int(interval), boundary, **options)
@@ -143,6 +147,20 @@ def test_device_step_follows_the_reference_host_steps(tag):
     fluid = r['isFluid']
     assert np.allclose(state['accelerations'][fluid], r['finalAccelerations'][fluid], rtol=0.0,
                        atol=1e-8 * np.abs(r['finalAccelerations']).max())
+
+
+@pytest.mark.parametrize('tag', goldenTags('runs3d.npz'))
+def test_device_step_follows_the_reference_host_steps_in_3d(tag):
+    # the reference's BreakingWave3D tank over a ridge (height-field bed, walls six layers deep), its
+    # numpy solver's host steps, whole and after a crest split into daughters of h / 2
+    r = golden('runs3d.npz', tag)
+    stepper = stepperFor(r)
+    state = {k: r[k].copy() for k in ('positions', 'velocities', 'densities', 'masses', 'isFluid', 'lengths')}
+    dts = [stepper(state) for _ in range(int(r['steps']))]
+    assert np.allclose(dts, r['dts'], rtol=1e-10, atol=0.0)
+    assert np.allclose(state['positions'], r['finalPositions'], rtol=0.0, atol=1e-11)
+    assert np.allclose(state['velocities'], r['finalVelocities'], rtol=0.0, atol=1e-8)
+    assert np.allclose(state['densities'], r['finalDensities'], rtol=1e-11, atol=0.0)
 
 
 def closureGolden(tag):
