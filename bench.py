@@ -83,6 +83,7 @@ def parseArgs():
                    help='serve this many requests arriving as a Poisson stream (see serveBench)')
     p.add_argument('--horizon-scale', type=float, default=0.1,
                    help='the served requests horizons, U(2, 6) s of simulated time times this')
+    p.add_argument('--rate', type=float, default=20.0, help='the served stream\'s arrivals a second')
     p.add_argument('--no-refine', action='store_true',
                    help='ridge: leave the crest zone (surface above 0.3 H) whole instead of splitting it into '
                         'daughters of h/2 before the timing')
@@ -279,36 +280,26 @@ def measuredPeaks() -> dict:
     return {'hbm_gbs': 6650.0, 'source': 'fallback'}
 
 
-def profiledTraffic(case) -> float | None:
-    """DRAM bytes per momentum launch from the committed ncu summary of this workload.  The 3D
-    workload is captured at 8 ppd (the bench's size is too large to capture); its traffic, which
-    grows with the fluid rows, is scaled to this case by the fluid count."""
-    name = 'momentum_solitaryBeach64.md' if case.dimensions == 2 else 'momentum_ridgeWave3D8.md'
+def profiledTraffic(case, kernel: str, refined: bool, fluid: int) -> float | None:
+    """DRAM bytes a launch of `kernel` (gradients, momentum, continuity) from the committed ncu summary of
+    this workload: the beach at its own size; the refined ridge captured at 12 ppd (the bench's size
+    is too large to capture), whose traffic -- the neighbour table, which grows with the particles --
+    is scaled to this run by its fluid particles after the split."""
+    if case.dimensions == 2:
+        name = 'sweeps_solitaryBeach64.md'
+    elif refined:
+        name = 'sweeps_ridgeWave3D12_refined.md'
+    else:
+        return None
     path = os.path.join(ROOT, 'profiles', name)
     if not os.path.exists(path):
         return None
     text = open(path).read()
-    match = re.search(r'traffic_bytes_per_launch:\s*([0-9.eE+]+)', text)
-    if not match:
+    match = re.search(rf'traffic_bytes_per_launch_{kernel}:\s*([0-9.eE+]+)', text)
+    captured = re.search(r'fluid_particles:\s*([0-9]+)', text)
+    if not match or not captured:
         return None
-    traffic = float(match.group(1))
-    fluid = re.search(r'fluid_particles:\s*([0-9]+)', text)
-    if case.dimensions == 3 and fluid:
-        traffic *= case.fluidCount / float(fluid.group(1))
-    return traffic
-
-
-def cpuState(case, refine: bool) -> tuple:
-    """The state the float64 CPU step runs on, its fluid count and what it is: the whole beach, or the
-    ridge's sample (ridgeSample)."""
-    import numpy as np
-    if case.dimensions == 3:
-        sample = ridgeSample(case, refine)
-        return sample, int(sample['isFluid'].sum()), 'one float64 step over a sample of the workload: ' + \
-            sample.pop('description')
-    state = {k: np.array(getattr(case.state, k), copy=True) for k in ('positions', 'velocities', 'densities',
-                                                                       'masses', 'isFluid')}
-    return state, case.fluidCount, f'full steps of the whole case ({case.state.nParticles} particles) in float64'
+    return float(match.group(1)) * fluid / float(captured.group(1))
 
 
 def cpuBaseline(case, refine: bool, seconds: float = 12.0) -> dict:
@@ -438,26 +429,37 @@ def sweepBench(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+RIDGE16_PARTICLES = 2469130     # the 40 d x 10 d ridge at 16 particles per depth
+
+
 def ridgeRequest(spec):
+    """A served 3D request: the Gaussian ridge at the spec's ppd in a tank scaled from 40 d x 10 d by
+    the spec's `scale`, the crest at a fifth and the ridge at half its length."""
     from pysurf_b200 import cases
-    return cases.ridgeWave3D(spec.ppd)
+    scale = float(spec.scale)
+    length, width = 40.0 * scale, 10.0 * scale
+    return cases.ridgeWave3D(spec.ppd, length=length, width=width, crestX=0.2 * length, ridgeX=0.5 * length)
 
 
 def serveBench(args) -> None:
-    """The served stream at a reduced size: --serve requests arriving as a Poisson stream at 20 a
-    second (seed 0), 80% 2D beaches drawn as the sweep draws them and 20% 3D ridges at 8-16 ppd (0.4M
-    to 2.4M particles), each run for U(2, 6) s of simulated time times --horizon-scale; admitted as
-    slots (--slots) and device memory free up, solved beside the requests in flight."""
+    """The served stream: --serve requests arriving as a Poisson stream at --rate a second (seed 0),
+    80% 2D beaches drawn as the sweep draws them (5k-130k fluid particles) and 20% 3D ridges at 16 ppd
+    in tanks sized for 0.5M-4M particles, each run for U(2, 6) s of simulated time times
+    --horizon-scale; admitted as slots (--slots) and device memory free up, solved beside the requests
+    in flight.  Beside p50/p99 latency the line reports the load the stream offers (its particle-updates
+    over its arrival span) against what the device cleared while busy (its particle-updates over the
+    whole run): a utilisation above 1 is a queue that grows, and its latencies are its depth."""
     import numpy as np
     from pysurf_b200 import batch
     rng = np.random.default_rng(0)
     sweep = batch.drawSweep(args.serve, seed=0)
-    arrivals = batch.poissonArrivals(args.serve, 20.0, seed=0)
+    arrivals = batch.poissonArrivals(args.serve, args.rate, seed=0)
     requests = []
     for k in range(args.serve):
         horizon = float(rng.uniform(2.0, 6.0)) * args.horizon_scale
         if rng.uniform() < 0.2:
-            spec = batch.CaseSpec(k, 0.0, 0.5, int(rng.integers(8, 17)), endTime=horizon, toBreaking=False)
+            scale = math.sqrt(float(rng.uniform(0.5e6, 4.0e6)) / RIDGE16_PARTICLES)
+            spec = batch.CaseSpec(k, 0.0, 0.5, 16, endTime=horizon, toBreaking=False, scale=scale)
             requests.append(batch.Request(float(arrivals[k]), spec, ridgeRequest))
         else:
             base = sweep[k]
@@ -465,12 +467,18 @@ def serveBench(args) -> None:
             requests.append(batch.Request(float(arrivals[k]), spec))
     out = batch.serve(requests, slots=args.slots)
     results = out['results']
+    updates = sum(r.fluidParticles * r.steps for r in results)
+    span = float(arrivals[-1] - arrivals[0]) if args.serve > 1 else float('nan')
+    offered = updates / span if span > 0 else float('nan')
     line = {'metric': 'p99 latency', 'value': out['latency_p99_s'], 'unit': 's', 'n_gpus': 1,
             'higher_is_better': False, 'data': 'synthetic',
-            'config': {'workload': f'{args.serve} requests, Poisson 20/s, 80% 2D beach 16-64 ppd, 20% 3D ridge '
-                                   f'8-16 ppd, horizons U(2, 6) s x {args.horizon_scale}', 'slots': args.slots},
+            'config': {'workload': f'{args.serve} requests, Poisson {args.rate}/s, 80% 2D beach 16-64 ppd, 20% 3D '
+                                   f'ridge 16 ppd 0.5M-4M particles, horizons U(2, 6) s x {args.horizon_scale}',
+                       'slots': args.slots},
             'latency_p50_s': out['latency_p50_s'], 'latency_p99_s': out['latency_p99_s'],
             'seconds': out['seconds'], 'particle_updates_per_s': out['particle_updates_per_s'],
+            'offered_particle_updates_per_s': offered, 'arrival_span_s': span,
+            'utilisation': offered / out['particle_updates_per_s'] if out['particle_updates_per_s'] else None,
             'failed': sum(1 for r in results if r.error), 'particles': [r.particles for r in results]}
     print(json.dumps(line), flush=True)
 
@@ -563,7 +571,8 @@ def main() -> None:
             'peak_source': 'nominal FP32 SIMT: 148 SMs x 128 lanes x 2 flop x 1965 MHz'}
     simt['frac'] = simt['achieved_tflops'] / FP32_SIMT_TFLOPS
     roofline = {'bound': 'hbm', 'kernel': dominant, 'achieved': achieved, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
-                'frac': achieved / peaks['hbm_gbs'], 'traffic': profiledTraffic(case), 'peak_source': peaks['source'],
+                'frac': achieved / peaks['hbm_gbs'], 'traffic': profiledTraffic(case, dominant, refine, fluidCount),
+                'peak_source': peaks['source'],
                 'kernel_ms': kernelMs, 'bytes_per_update': unitBytes, 'step_hbm_frac': unitBytes * fluidCount /
                 (totalMs / args.steps / 1e3) / 1e9 / peaks['hbm_gbs']}
 

@@ -277,6 +277,17 @@ int sph_face_cells(SphSystem *sys, double low_x, double high_x, double low_z, do
                    double base, double spacing, int64_t columns, int64_t bands, uint8_t *marks);
 int sph_bed_sheet(SphSystem *sys, const double *bed_x, const double *bed_z, int64_t bed_count, double wet_height,
                   double *xs, int64_t capacity, int64_t *count);
+/* The same three reads in 3D over one section of the tank (BreakingWave3D._readSections,
+ * src/pysurf/BreakingWave3D.py:461-480): the fluid whose y lies within half_width of y
+ * (|y_p - y| < half_width, the reference's section mask), read in its (x, z) plane, z the
+ * vertical; the arguments otherwise as above.  SPH_ERR_UNSUPPORTED in 2D, as the reads above are
+ * in 3D. */
+int sph_section_tops(SphSystem *sys, double y, double half_width, double x0, double width, int64_t count, double *tops);
+int sph_section_face_cells(SphSystem *sys, double y, double half_width, double low_x, double high_x, double low_z,
+                           double half, double start, double base, double spacing, int64_t columns, int64_t bands,
+                           uint8_t *marks);
+int sph_section_bed_sheet(SphSystem *sys, double y, double half_width, const double *bed_x, const double *bed_z,
+                          int64_t bed_count, double wet_height, double *xs, int64_t capacity, int64_t *count);
 
 /* The same loop in three calls, for callers that overlap their own work with the steps:
  * sph_begin_steps sets the clock and the limits on the device; sph_enqueue_steps queues `count`

@@ -89,6 +89,9 @@ SIGNATURES = {
     'sph_split_crest_zone': [_h, _d, _d, _d, _i64, _i64, _d, _d, _d, _d, _pi64],
     'sph_face_cells': [_h, _d, _d, _d, _d, _d, _d, _d, _i64, _i64, _pu8],
     'sph_bed_sheet': [_h, _pd, _pd, _i64, _d, _pd, _i64, _pi64],
+    'sph_section_tops': [_h, _d, _d, _d, _d, _i64, _pd],
+    'sph_section_face_cells': [_h, _d, _d, _d, _d, _d, _d, _d, _d, _d, _i64, _i64, _pu8],
+    'sph_section_bed_sheet': [_h, _d, _d, _pd, _pd, _i64, _d, _pd, _i64, _pi64],
     'sph_last_advance_ms': [_h, _pd],
     'sph_begin_steps': [_h, _d, _i64, _d, _d, _i64, _d, _d, _d, _i64],
     'sph_enqueue_steps': [_h, _i64],

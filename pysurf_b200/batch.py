@@ -39,6 +39,7 @@ class CaseSpec:
     ppd: int
     endTime: float = 12.0
     toBreaking: bool = True
+    scale: float = 1.0              # a 3D request's tank, scaled from 40 d x 10 d
 
 
 @dataclass

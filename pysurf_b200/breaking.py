@@ -1,4 +1,4 @@
-"""Where a 2D wave breaks on a beach: the breaking tracker of the reference's 2D facade.
+"""Where a wave breaks: the breaking tracker of the reference's 2D facade, and its 3D sections.
 
 The reference reads the wave from the fluid's positions every 0.01 sqrt(d / g) of simulated time
 (src/pysurf/BreakingWave.py:885-912) with `BreakingTracker` (src/pysurf/waveBreaking.py:709-906).
@@ -15,11 +15,19 @@ This module restates its 'cells' face measure, the one its first-order (lattice)
                     consecutive updates with the face leaning a spacing or more, with the crest past
                     `searchFromX` (waveBreaking.py:709-906, the 'cells' branch)
 
+In 3D the reference reads sections across the tank (BreakingWave3D._readSections,
+src/pysurf/BreakingWave3D.py:461-480): each section's tracker takes the fluid within half its
+width (sectionRows / 2 spacings) of its y, in the (x, z) plane, over the bed's profile along x at
+that y.  The facade reads them with the 'contour' face measure, which contours a smoothed fluid
+fraction with the third-party contourpy (not in this image); these sections read the 'cells'
+measure, the same lean, trough and waterline as the 2D tracker, over each section's fluid.
+
 `runToBreaking` steps a `PairSums` on the device to the breaking point.  At each tracker update the
 device takes the reductions an update needs (each column's highest particle, the face window's
-cells, the x of the bed's water sheet: sph_surface_tops, sph_face_cells, sph_bed_sheet) with the
-float64 arithmetic of the host's measures, and only those come back; `updateOnDevice` then reads
-them as `update` reads pulled positions, to the same values.
+cells, the x of the bed's water sheet: sph_surface_tops, sph_face_cells, sph_bed_sheet, and in 3D
+the sph_section_* reads over a section's band) with the float64 arithmetic of the host's measures,
+and only those come back; `updateOnDevice` then reads them as `update` reads pulled positions, to
+the same values.
 """
 from __future__ import annotations
 
@@ -155,6 +163,7 @@ class BreakingTracker:
     faceReach: float = 1.0
     searchFromX: float = -np.inf
     persistence: int = 3
+    section: tuple | None = None    # 3D: (y, half width), the band across the tank this tracker reads
     times: list = field(default_factory=list)
     crestX: list = field(default_factory=list)
     crestHeight: list = field(default_factory=list)
@@ -169,8 +178,16 @@ class BreakingTracker:
     def breakingFinal(self) -> bool:
         return self.breakingPoint is not None
 
+    def sectionOf(self, positions: np.ndarray) -> np.ndarray:
+        """This section's fluid in its (x, z) plane from the whole fluid's positions (N, 3)
+        (src/pysurf/BreakingWave3D.py:461-480); 2D positions as they are."""
+        if self.section is None:
+            return positions
+        y, half = self.section
+        return positions[np.abs(positions[:, 1] - y) < half][:, [0, 2]]
+
     def update(self, time: float, positions: np.ndarray) -> None:
-        """Read the wave from the fluid's positions (N, 2) at `time`."""
+        """Read the wave from the fluid's positions (N, 2) at `time` (a section's: see `sectionOf`)."""
         bed, s = self.bed, self.spacing
         centers, elevation = surfaceProfile(positions, bed.startX, bed.endX, s)
         crestX = float(centers[int(np.nanargmax(elevation))])
@@ -184,7 +201,8 @@ class BreakingTracker:
         swl = bed.stillWaterLevel
         count = max(1, int(math.ceil((bed.endX - bed.startX) / s)))
         centers = bed.startX + (np.arange(count) + 0.5) * s
-        tops = sums.surfaceTops(bed.startX, s, count)
+        band = self.section
+        tops = sums.surfaceTops(bed.startX, s, count, section=band)
         elevation = np.where(np.isfinite(tops), tops + 0.5 * s, np.nan)
         crestX = float(centers[int(np.nanargmax(elevation))])
         # faceLean's window, its cells marked on the device; the bands reach the highest particle
@@ -192,9 +210,10 @@ class BreakingTracker:
         columns = max(1, int(math.ceil((end - start) / s)))
         highest = float(np.max(tops[np.isfinite(tops)])) if np.isfinite(tops).any() else base
         bands = max(1, int(math.floor((highest - half - base) / s)) + 2)
-        marked = sums.faceCells(start - half, end + half, base - half, half, start, base, s, columns, bands)
+        marked = sums.faceCells(start - half, end + half, base - half, half, start, base, s, columns, bands,
+                                section=band)
         lean = leanOfCells(marked, start, s) if marked.any() else -np.inf
-        sheet = sums.bedSheet(bed.x, bed.z, 2.0 * s)
+        sheet = sums.bedSheet(bed.x, bed.z, 2.0 * s, section=band)
         tip = float(np.partition(sheet, sheet.size - 3)[sheet.size - 3]) if sheet.size >= 3 else float('nan')
         self.record(time, centers, elevation, lean, tip)
 
@@ -235,28 +254,61 @@ def trackerFor(case) -> BreakingTracker:
                            searchFromX=float(info['toeX']))
 
 
+def sectionTrackers(case, sections=None, sectionRows: int = 2) -> dict:
+    """The 3D facade's trackers, one a section (src/pysurf/BreakingWave3D.py:356-400, 690-694): the
+    tank's middle line by default, each reading the fluid within sectionRows / 2 spacings of its y
+    over the bed's profile along x there (cases.ridgeSection), face reach one depth, breaking looked
+    for from the wave's start on; the 'cells' face measure (see the module's notes)."""
+    from pysurf_b200 import cases
+    info, s = case.info, case.spacing
+    ridge = type(case.boundary).__name__ == 'HeightFieldBoundary'
+    width = float(info['tank'][1]) if ridge else float(info['width'])
+    ys = tuple(float(y) for y in (sections if sections is not None else (0.5 * width,)))
+    half = 0.5 * sectionRows * s
+
+    def profile(y):
+        # a height field's section; an extruded beach's profile is the same at every y
+        return cases.ridgeSection(case, y) if ridge else case.boundary.bathymetry
+
+    # the 3D facade looks for breaking from the wave's start, the 2D one from the beach's toe
+    searchFromX = float(info['crestX']) if ridge else float(info['toeX'])
+    return {y: BreakingTracker(profile(y), s, faceReach=float(info['depth']), searchFromX=searchFromX,
+                               section=(y, half)) for y in ys}
+
+
 def runToBreaking(case, sums, endTime: float, trackInterval: float = 0.01, maxSteps: int = 1 << 40,
-                  onDevice: bool = True):
-    """Step the case on the device from its start until the tracker's breaking point is final or
-    `endTime`, updating the tracker every `trackInterval` sqrt(d / g) of simulated time
-    (src/pysurf/BreakingWave.py:885-912): from the device's reductions (`onDevice`), else from the
-    pulled fluid positions.  `sums` holds the pushed state.  Returns (tracker, time, steps)."""
+                  onDevice: bool = True, trackers: dict | None = None, shortestLength: float | None = None):
+    """Step the case on the device from its start until the (first section's) breaking point is final
+    or `endTime`, updating the trackers every `trackInterval` sqrt(d / g) of simulated time
+    (src/pysurf/BreakingWave.py:885-912; src/pysurf/BreakingWave3D.py:740-770): from the device's
+    reductions (`onDevice`), else from the pulled fluid positions.  `sums` holds the pushed state; a 3D
+    case's trackers are its sections' (`sectionTrackers`, or `trackers`).  Returns (tracker, time,
+    steps), the tracker the first section's in 3D."""
     depth = float(case.info['depth'])
     interval = trackInterval * math.sqrt(depth / 9.80665)
-    tracker = trackerFor(case)
-    fluid = np.asarray(case.state.isFluid, dtype=bool)
+    if trackers is None:
+        trackers = sectionTrackers(case) if case.dimensions == 3 else {None: trackerFor(case)}
+    first = next(iter(trackers.values()))
+    shortest = case.smoothingLength if shortestLength is None else shortestLength
     positions = None
     time, step, dt = 0.0, 0, 0.0
     nextTrack = interval
-    while time < endTime and not tracker.breakingFinal and step < maxSteps:
+    while time < endTime and not first.breakingFinal and step < maxSteps:
         target = min(nextTrack, endTime)
-        time, step, dt = sums.advance(time, step, target, maxSteps, case.smoothingLength, case.cflNumber,
+        time, step, dt = sums.advance(time, step, target, maxSteps, shortest, case.cflNumber,
                                       case.maxTimeStep, case.densityFilterInterval, dt)
         if time >= nextTrack:
             if onDevice:
-                tracker.updateOnDevice(time, sums)
+                for tracker in trackers.values():
+                    tracker.updateOnDevice(time, sums)
             else:
-                positions = sums.pullPositions(positions)
-                tracker.update(time, positions[fluid])
+                state = sums.pullState() if case.dimensions == 3 else None
+                if state is not None:
+                    fluidPositions = state['positions'][state['isFluid']]
+                else:
+                    positions = sums.pullPositions(positions)
+                    fluidPositions = positions[np.asarray(case.state.isFluid, dtype=bool)]
+                for tracker in trackers.values():
+                    tracker.update(time, tracker.sectionOf(fluidPositions))
             nextTrack += interval
-    return tracker, time, step
+    return first, time, step

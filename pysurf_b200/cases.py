@@ -262,6 +262,49 @@ def solitaryBeach(particlesPerDepth: int = 64, depth: float = 1.0, height: float
                       'length': length, 'ppd': particlesPerDepth, 'layers': layers})
 
 
+def extrudedBeach(particlesPerDepth: int = 8, width: float = 1.75, depth: float = 1.0, height: float = 0.6,
+                  crestX: float = 2.5, toeX: float = 4.0, slope: float = 1.0 / 15.0, length: float = 20.0,
+                  smoothingRatio: float = 3.0) -> Case:
+    """The beach of `solitaryBeach` in 3D: its 2D start (first-order solitary wave, bed layers, offshore
+    wall) repeated across a periodic y axis `width` long, one lattice column a spacing, the bed a
+    BedBoundary over the profile with no side walls (src/pysurf/sphBoundaries.py:295-344, periodic), the
+    deltaSph scheme at h = 3 dx.  The period must exceed twice the support (4 h)."""
+    flat = solitaryBeach(particlesPerDepth, depth, height, crestX, toeX, slope, length, smoothingRatio)
+    s = flat.spacing
+    columns = int(round(width / s))
+    if columns * s <= 4.0 * flat.smoothingLength:
+        raise ValueError('the periodic width must exceed twice the kernel support (4 h)')
+    width = columns * s
+    ys = (np.arange(columns) + 0.5) * s
+
+    def extrude(points):
+        n = len(points)
+        out = np.empty((n * columns, 3))
+        out[:, 0] = np.tile(points[:, 0], columns)
+        out[:, 1] = np.repeat(ys, n)
+        out[:, 2] = np.tile(points[:, 1], columns)
+        return out
+
+    st, nf = flat.state, flat.fluidCount
+    fluid, walls = extrude(st.positions[:nf]), extrude(st.positions[nf:])
+    velocities = np.zeros((len(fluid), 3))
+    velocities[:, 0] = np.tile(st.velocities[:nf, 0], columns)
+    velocities[:, 2] = np.tile(st.velocities[:nf, 1], columns)
+    state = ParticleState.assemble(fluid, walls, s, flat.referenceDensity, velocities)
+    state.densities = np.concatenate([np.tile(st.densities[:nf], columns), np.tile(st.densities[nf:], columns)])
+    bed = flat.boundary
+    boundary = BedBoundary(bed.bathymetry, s, nLayers=bed.nLayers, wallTop=bed.wallTop, width=width,
+                           endWallTop=None, periodic=True, wallX=bed.wallX)
+    lower, upper = flat.domainMin, flat.domainMax
+    info = dict(flat.info, width=width, columns=columns)
+    return Case('extrudedBeach', state, boundary, 3, s, flat.smoothingLength, flat.kernelType,
+                np.array([lower[0], 0.0, lower[1]]), np.array([upper[0], width, upper[1]]), flat.referenceDensity,
+                flat.soundSpeed, np.array([0.0, 0.0, -GRAVITY]), alpha=flat.alpha, densityFloor=flat.densityFloor,
+                densityDiffusion=flat.densityDiffusion, wallExtrapolated=True, continuityCorrection=True,
+                viscosityLimiter=True, cflNumber=flat.cflNumber, maxTimeStep=flat.maxTimeStep, period=width,
+                info=info)
+
+
 def gaussianRidge(depth: float = 1.0, ridgeHeight: float = 0.6, ridgeWidth: float = 3.0, angle: float = 25.0,
                   length: float = 40.0, width: float = 10.0, ridgeX: float = 20.0):
     """The bed z_b(x, y) = ridgeHeight d exp(-xi^2 / (2 sigma^2)) of a Gaussian ridge whose axis crosses
@@ -380,7 +423,22 @@ def ridgeWave3D(particlesPerDepth: int = 32, depth: float = 1.0, height: float =
                 densityDiffusion='hydrostatic', wallExtrapolated=True, continuityCorrection=True,
                 viscosityLimiter=True, cflNumber=0.25, maxTimeStep=1.0,
                 info={'depth': depth, 'H/d': height / depth, 'crestX': crestX, 'ridge': [ridgeHeight, ridgeWidth, angle],
-                      'tank': [length, width], 'ppd': particlesPerDepth, 'layers': layers})
+                      'ridgeX': ridgeX, 'tank': [length, width], 'ppd': particlesPerDepth, 'layers': layers})
+
+
+def ridgeSection(case: Case, y: float) -> Profile:
+    """The ridge's bed along x at fixed y, through the height table's x positions inside the tank
+    and its two ends (HeightField.section, src/pysurf/bathymetry.py:719-731): the bed profile a
+    section's breaking tracker reads."""
+    info, table = case.info, case.boundary.field
+    ridgeHeight, ridgeWidth, angle = info['ridge']
+    length, width = info['tank']
+    elevation, _ = gaussianRidge(float(info['depth']), ridgeHeight, ridgeWidth, angle, length, width,
+                                 float(info['ridgeX']))
+    startX, endX = float(table.bounds[0]), float(table.bounds[1])
+    inside = table.x[(table.x > startX + 1e-9) & (table.x < endX - 1e-9)]
+    x = np.concatenate([[startX], inside, [endX]])
+    return Profile(x, elevation(x, np.full_like(x, float(y))), table.stillWaterLevel)
 
 
 def refineCrestZone(sums, case: Case, share: float = 0.3, lengthRatio: float = 0.5) -> int:

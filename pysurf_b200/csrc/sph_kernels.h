@@ -128,13 +128,18 @@ void launchNeighbourRows(const Params &P, const Frame &F, const int64_t *offsets
                          double radius2, cudaStream_t st);
 void launchCellOrderKey(int n, int dim, const double *positions, double width, const long long shape[3],
                         long long *keys, cudaStream_t st);
-void launchSurfaceTops(int n, const MasterView &M, int vertical, double x0, double width, long long count,
-                       unsigned long long *scratch, double *out, cudaStream_t st);
-void launchFaceCells(int n, const MasterView &M, int vertical, double lowX, double highX, double lowZ, double half,
-                     double start, double base, double spacing, long long columns, long long bands, uint8_t *marks,
-                     cudaStream_t st);
-void launchBedSheet(int n, const MasterView &M, int vertical, const double *bx, const double *bz, int m,
-                    double wetHeight, double *out, int *count, cudaStream_t st);
+// A band across the tank (3D sections): the fluid with |y - center| < half; y null for all of it.
+struct Band {
+    const double *y;
+    double center, half;
+};
+void launchSurfaceTops(int n, const MasterView &M, int vertical, const Band &band, double x0, double width,
+                       long long count, unsigned long long *scratch, double *out, cudaStream_t st);
+void launchFaceCells(int n, const MasterView &M, int vertical, const Band &band, double lowX, double highX,
+                     double lowZ, double half, double start, double base, double spacing, long long columns,
+                     long long bands, uint8_t *marks, cudaStream_t st);
+void launchBedSheet(int n, const MasterView &M, int vertical, const Band &band, const double *bx, const double *bz,
+                    int m, double wetHeight, double *out, int *count, cudaStream_t st);
 void launchCrestZone(int n, const MasterView &M, int dim, double x0, double y0, double width, long long nx,
                      long long ny, unsigned long long *tops, double threshold, double minMass, uint8_t *chosen,
                      cudaStream_t st);

@@ -1,7 +1,7 @@
 // sph_surface.cu -- the breaking tracker's reads of the fluid, and the crest zone, on the device.
 //
-// A tracker update needs three small things from the fluid's positions, not the positions
-// themselves: each column's highest particle (the free surface, src/pysurf/waveBreaking.py:129-162),
+// A tracker update needs three small things from the fluid's positions (in 3D, a section's: the
+// fluid in a band across the tank, read in its (x, z) plane), not the positions themselves: each column's highest particle (the free surface, src/pysurf/waveBreaking.py:129-162),
 // the cells a particle marks in the window ahead of the crest (the face lean, 559-634), and the x
 // of the particles on the bed's water sheet (the waterline, 636-656).  Each kernel does the
 // reference's float64 arithmetic term by term, with explicitly rounded operations where a fused
@@ -26,12 +26,19 @@ __device__ __forceinline__ double fromOrderedBits(unsigned long long o)
     return __longlong_as_double((long long)u);
 }
 
+// A section's band across the tank (3D): the fluid with |y - center| < half, the comparison the
+// reference's section mask takes in float64 (src/pysurf/BreakingWave3D.py:461-468); y null takes all.
+__device__ __forceinline__ bool inBand(const Band &B, int s)
+{
+    return !B.y || fabs(__dsub_rn(B.y[s], B.center)) < B.half;
+}
+
 // tops[c] = the largest height of a fluid particle whose column floor((x - x0) / width) is c.
-__global__ void surfaceTopKernel(int n, const double *x, const double *z, const uint8_t *fluid, double x0,
+__global__ void surfaceTopKernel(int n, const double *x, const double *z, const uint8_t *fluid, Band band, double x0,
                                  double width, long long count, unsigned long long *tops)
 {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n || !fluid[s]) return;
+    if (s >= n || !fluid[s] || !inBand(band, s)) return;
     const double c = floor((x[s] - x0) / width);
     if (!(c >= 0.0 && c < (double)count)) return;
     atomicMax(&tops[(long long)c], orderedBits(z[s]));
@@ -47,12 +54,12 @@ __global__ void surfaceTopDecodeKernel(long long count, const unsigned long long
 // The face window's cells: a fluid particle with lowX <= x < highX and z > lowZ marks the cells
 // (band0 + db, column0 + dc), db, dc in {0, 1}, column0 = floor((x - half - start) / spacing),
 // band0 = floor((z - half - base) / spacing), those inside columns x bands.
-__global__ void faceCellsKernel(int n, const double *x, const double *z, const uint8_t *fluid, double lowX,
+__global__ void faceCellsKernel(int n, const double *x, const double *z, const uint8_t *fluid, Band band, double lowX,
                                 double highX, double lowZ, double half, double start, double base, double spacing,
                                 long long columns, long long bands, uint8_t *marks)
 {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n || !fluid[s]) return;
+    if (s >= n || !fluid[s] || !inBand(band, s)) return;
     const double xv = x[s], zv = z[s];
     if (!(xv >= lowX && xv < highX && zv > lowZ)) return;
     const double c0 = floor(__dsub_rn(__dsub_rn(xv, half), start) / spacing);
@@ -83,11 +90,11 @@ __device__ __forceinline__ double bedElevation(double v, const double *bx, const
 }
 
 // The x of every fluid particle less than wetHeight above the bed, in no set order.
-__global__ void bedSheetKernel(int n, const double *x, const double *z, const uint8_t *fluid, const double *bx,
-                               const double *bz, int m, double wetHeight, double *out, int *count)
+__global__ void bedSheetKernel(int n, const double *x, const double *z, const uint8_t *fluid, Band band,
+                               const double *bx, const double *bz, int m, double wetHeight, double *out, int *count)
 {
     int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n || !fluid[s]) return;
+    if (s >= n || !fluid[s] || !inBand(band, s)) return;
     const double xv = x[s];
     if (__dsub_rn(z[s], bedElevation(xv, bx, bz, m)) < wetHeight) out[atomicAdd(count, 1)] = xv;
 }
@@ -138,33 +145,33 @@ void launchCrestZone(int n, const MasterView &M, int dim, double x0, double y0, 
                                                        chosen);
 }
 
-void launchSurfaceTops(int n, const MasterView &M, int vertical, double x0, double width, long long count,
-                       unsigned long long *scratch, double *out, cudaStream_t st)
+void launchSurfaceTops(int n, const MasterView &M, int vertical, const Band &band, double x0, double width,
+                       long long count, unsigned long long *scratch, double *out, cudaStream_t st)
 {
     cudaMemsetAsync(scratch, 0, sizeof(unsigned long long) * count, st);
     if (n > 0)
-        surfaceTopKernel<<<blocksFor(n, 256), 256, 0, st>>>(n, M.x[0], M.x[vertical], M.fluid, x0, width, count,
+        surfaceTopKernel<<<blocksFor(n, 256), 256, 0, st>>>(n, M.x[0], M.x[vertical], M.fluid, band, x0, width, count,
                                                             scratch);
     surfaceTopDecodeKernel<<<blocksFor(count, 256), 256, 0, st>>>(count, scratch, out);
 }
 
-void launchFaceCells(int n, const MasterView &M, int vertical, double lowX, double highX, double lowZ, double half,
-                     double start, double base, double spacing, long long columns, long long bands, uint8_t *marks,
-                     cudaStream_t st)
+void launchFaceCells(int n, const MasterView &M, int vertical, const Band &band, double lowX, double highX,
+                     double lowZ, double half, double start, double base, double spacing, long long columns,
+                     long long bands, uint8_t *marks, cudaStream_t st)
 {
     cudaMemsetAsync(marks, 0, (size_t)columns * (size_t)bands, st);
     if (n > 0)
-        faceCellsKernel<<<blocksFor(n, 256), 256, 0, st>>>(n, M.x[0], M.x[vertical], M.fluid, lowX, highX, lowZ,
+        faceCellsKernel<<<blocksFor(n, 256), 256, 0, st>>>(n, M.x[0], M.x[vertical], M.fluid, band, lowX, highX, lowZ,
                                                            half, start, base, spacing, columns, bands, marks);
 }
 
-void launchBedSheet(int n, const MasterView &M, int vertical, const double *bx, const double *bz, int m,
-                    double wetHeight, double *out, int *count, cudaStream_t st)
+void launchBedSheet(int n, const MasterView &M, int vertical, const Band &band, const double *bx, const double *bz,
+                    int m, double wetHeight, double *out, int *count, cudaStream_t st)
 {
     cudaMemsetAsync(count, 0, sizeof(int), st);
     if (n > 0)
-        bedSheetKernel<<<blocksFor(n, 256), 256, 0, st>>>(n, M.x[0], M.x[vertical], M.fluid, bx, bz, m, wetHeight,
-                                                          out, count);
+        bedSheetKernel<<<blocksFor(n, 256), 256, 0, st>>>(n, M.x[0], M.x[vertical], M.fluid, band, bx, bz, m,
+                                                          wetHeight, out, count);
 }
 
 }  // namespace sph

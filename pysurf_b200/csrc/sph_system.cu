@@ -1878,50 +1878,68 @@ int sph_split_crest_zone(SphSystem *sys, double x0, double y0, double width, int
     return sph_split(sys, mask.data(), reference_density, length_ratio, split);
 }
 
-int sph_surface_tops(SphSystem *sys, double x0, double width, int64_t count, double *tops)
+// The reads of the fluid a tracker update takes (sph_surface.cu), over the whole fluid in 2D or a
+// section's band across the tank in 3D; x along the tank, the vertical the last axis.
+static int readBand(SphSystem *sys, bool section, double center, double half, Band *band, int *vertical)
+{
+    if (!sys->resident) return fail(SPH_ERR_STATE, "no device state: call sph_push first");
+    if (!section && sys->dim != 2) return fail(SPH_ERR_UNSUPPORTED, "the whole-fluid surface reads are 2D");
+    if (section && sys->dim != 3) return fail(SPH_ERR_UNSUPPORTED, "the section reads are 3D");
+    if (section && !(half > 0.0)) return fail(SPH_ERR_INVALID, "a section's half width must be positive");
+    *band = Band{section ? sys->master[sys->cur].x[1] : nullptr, center, half};
+    *vertical = sys->dim - 1;
+    return SPH_OK;
+}
+
+static int readTops(SphSystem *sys, bool section, double center, double half, double x0, double width, int64_t count,
+             double *tops)
 {
     CHECK_SYS(sys);
     if (!tops || count <= 0 || count > (1ll << 28) || !(width > 0.0)) return fail(SPH_ERR_INVALID, "bad columns");
-    if (!sys->resident) return fail(SPH_ERR_STATE, "no device state: call sph_push first");
-    if (sys->dim != 2) return fail(SPH_ERR_UNSUPPORTED, "the surface reads are 2D");
+    Band band;
+    int vertical;
+    TRY(readBand(sys, section, center, half, &band, &vertical));
     void *scratch = nullptr;
     TRY(surfaceScratch(sys, sizeof(double) * 2 * (size_t)count, &scratch));
     unsigned long long *bits = (unsigned long long *)scratch;
     double *values = (double *)scratch + count;
-    launchSurfaceTops(sys->n, sys->master[sys->cur], 1, x0, width, count, bits, values, sys->stream);
+    launchSurfaceTops(sys->n, sys->master[sys->cur], vertical, band, x0, width, count, bits, values, sys->stream);
     CUDA_TRY(cudaGetLastError());
     TRY(sys->download(tops, values, sizeof(double) * count));
     CUDA_TRY(cudaStreamSynchronize(sys->stream));
     return SPH_OK;
 }
 
-int sph_face_cells(SphSystem *sys, double low_x, double high_x, double low_z, double half, double start,
-                   double base, double spacing, int64_t columns, int64_t bands, uint8_t *marks)
+static int readFaceCells(SphSystem *sys, bool section, double center, double halfBand, double low_x, double high_x,
+                  double low_z, double half, double start, double base, double spacing, int64_t columns, int64_t bands,
+                  uint8_t *marks)
 {
     CHECK_SYS(sys);
     if (!marks || columns <= 0 || bands <= 0 || columns * bands > (1ll << 30) || !(spacing > 0.0))
         return fail(SPH_ERR_INVALID, "bad window");
-    if (!sys->resident) return fail(SPH_ERR_STATE, "no device state: call sph_push first");
-    if (sys->dim != 2) return fail(SPH_ERR_UNSUPPORTED, "the surface reads are 2D");
+    Band band;
+    int vertical;
+    TRY(readBand(sys, section, center, halfBand, &band, &vertical));
     const size_t bytes = (size_t)columns * (size_t)bands;
     void *scratch = nullptr;
     TRY(surfaceScratch(sys, bytes, &scratch));
-    launchFaceCells(sys->n, sys->master[sys->cur], 1, low_x, high_x, low_z, half, start, base, spacing, columns,
-                    bands, (uint8_t *)scratch, sys->stream);
+    launchFaceCells(sys->n, sys->master[sys->cur], vertical, band, low_x, high_x, low_z, half, start, base, spacing,
+                    columns, bands, (uint8_t *)scratch, sys->stream);
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(marks, scratch, bytes, cudaMemcpyDeviceToHost, sys->stream));
     CUDA_TRY(cudaStreamSynchronize(sys->stream));
     return SPH_OK;
 }
 
-int sph_bed_sheet(SphSystem *sys, const double *bed_x, const double *bed_z, int64_t bed_count, double wet_height,
-                  double *xs, int64_t capacity, int64_t *count)
+static int readBedSheet(SphSystem *sys, bool section, double center, double half, const double *bed_x, const double *bed_z,
+                 int64_t bed_count, double wet_height, double *xs, int64_t capacity, int64_t *count)
 {
     CHECK_SYS(sys);
     if (!bed_x || !bed_z || !count || bed_count < 2 || bed_count > (1 << 24) || capacity < 0 || (capacity && !xs))
         return fail(SPH_ERR_INVALID, "bad bed or output");
-    if (!sys->resident) return fail(SPH_ERR_STATE, "no device state: call sph_push first");
-    if (sys->dim != 2) return fail(SPH_ERR_UNSUPPORTED, "the surface reads are 2D");
+    Band band;
+    int vertical;
+    TRY(readBand(sys, section, center, half, &band, &vertical));
     const int m = (int)bed_count, n = sys->n;
     void *scratch = nullptr;
     TRY(surfaceScratch(sys, sizeof(double) * (2 * (size_t)m + 1 + (size_t)n), &scratch));
@@ -1930,7 +1948,7 @@ int sph_bed_sheet(SphSystem *sys, const double *bed_x, const double *bed_z, int6
     double *out = bz + m + 1;
     CUDA_TRY(cudaMemcpyAsync(bx, bed_x, sizeof(double) * m, cudaMemcpyHostToDevice, sys->stream));
     CUDA_TRY(cudaMemcpyAsync(bz, bed_z, sizeof(double) * m, cudaMemcpyHostToDevice, sys->stream));
-    launchBedSheet(n, sys->master[sys->cur], 1, bx, bz, m, wet_height, out, dCount, sys->stream);
+    launchBedSheet(n, sys->master[sys->cur], vertical, band, bx, bz, m, wet_height, out, dCount, sys->stream);
     CUDA_TRY(cudaGetLastError());
     int found = 0;
     CUDA_TRY(cudaMemcpyAsync(&found, dCount, sizeof(int), cudaMemcpyDeviceToHost, sys->stream));
@@ -1942,6 +1960,42 @@ int sph_bed_sheet(SphSystem *sys, const double *bed_x, const double *bed_z, int6
         CUDA_TRY(cudaStreamSynchronize(sys->stream));
     }
     return SPH_OK;
+}
+
+int sph_surface_tops(SphSystem *sys, double x0, double width, int64_t count, double *tops)
+{
+    return readTops(sys, false, 0.0, 0.0, x0, width, count, tops);
+}
+
+int sph_face_cells(SphSystem *sys, double low_x, double high_x, double low_z, double half, double start,
+                   double base, double spacing, int64_t columns, int64_t bands, uint8_t *marks)
+{
+    return readFaceCells(sys, false, 0.0, 0.0, low_x, high_x, low_z, half, start, base, spacing, columns, bands, marks);
+}
+
+int sph_bed_sheet(SphSystem *sys, const double *bed_x, const double *bed_z, int64_t bed_count, double wet_height,
+                  double *xs, int64_t capacity, int64_t *count)
+{
+    return readBedSheet(sys, false, 0.0, 0.0, bed_x, bed_z, bed_count, wet_height, xs, capacity, count);
+}
+
+int sph_section_tops(SphSystem *sys, double y, double half_width, double x0, double width, int64_t count, double *tops)
+{
+    return readTops(sys, true, y, half_width, x0, width, count, tops);
+}
+
+int sph_section_face_cells(SphSystem *sys, double y, double half_width, double low_x, double high_x, double low_z,
+                           double half, double start, double base, double spacing, int64_t columns, int64_t bands,
+                           uint8_t *marks)
+{
+    return readFaceCells(sys, true, y, half_width, low_x, high_x, low_z, half, start, base, spacing, columns, bands,
+                         marks);
+}
+
+int sph_section_bed_sheet(SphSystem *sys, double y, double half_width, const double *bed_x, const double *bed_z,
+                          int64_t bed_count, double wet_height, double *xs, int64_t capacity, int64_t *count)
+{
+    return readBedSheet(sys, true, y, half_width, bed_x, bed_z, bed_count, wet_height, xs, capacity, count);
 }
 
 int sph_split(SphSystem *sys, const uint8_t *mask, double reference_density, double length_ratio, int64_t *split)

@@ -47,22 +47,37 @@ class FrameWriter:
         return self._store(time, positions, speeds, step, fields, scalars)
 
     def _store(self, time, positions, speeds, step, fields, scalars) -> Path:
-        arrays = {'positions': positions, 'speeds': speeds}
-        count = len(speeds)
-        for name, values in (fields or {}).items():
-            values = np.asarray(values)
-            if len(values) != count:
-                raise ValueError(f"Field '{name}' has {len(values)} rows for {count} fluid particles.")
-            arrays[name] = values
+        # The format: arrays positions, speeds, then the caller's fields (one row a fluid particle) in
+        # frameNNNNN.npz; an index entry {frame, time, step, count, file, scalars...}; the index
+        # {"frames": [...]} rewritten whole, one-space indent, after every frame.
+        count = int(np.shape(speeds)[0])
+        extra = {name: np.asarray(values) for name, values in (fields or {}).items()}
+        wrong = {name: len(values) for name, values in extra.items() if len(values) != count}
+        if wrong:
+            name, rows = next(iter(wrong.items()))
+            raise ValueError(f"Field '{name}' has {rows} rows for {count} fluid particles.")
         number = len(self.frames)
-        path = self.directory / f'frame{number:05d}.npz'
-        (np.savez_compressed if self.compress else np.savez)(path, **arrays)
-        entry = {'frame': number, 'time': float(time), 'step': step, 'count': count, 'file': path.name}
-        entry.update({name: float(value) for name, value in (scalars or {}).items()})
-        self.frames.append(entry)
-        with open(self.directory / INDEX, 'w', encoding='utf-8') as handle:
-            json.dump({'frames': self.frames}, handle, indent=1)
+        path = self.directory / _frameName(number)
+        save = np.savez_compressed if self.compress else np.savez
+        save(path, positions=positions, speeds=speeds, **extra)
+        self.frames.append(_indexEntry(number, time, step, count, path.name, scalars))
+        _writeIndex(self.directory, self.frames)
         return path
+
+
+def _frameName(number: int) -> str:
+    return f'frame{number:05d}.npz'
+
+
+def _indexEntry(number: int, time: float, step, count: int, file: str, scalars: dict | None) -> dict:
+    entry = dict(frame=number, time=float(time), step=step, count=count, file=file)
+    for name, value in (scalars or {}).items():
+        entry[name] = float(value)
+    return entry
+
+
+def _writeIndex(directory: Path, entries: list) -> None:
+    (directory / INDEX).write_text(json.dumps({'frames': entries}, indent=1), encoding='utf-8')
 
 
 def readIndex(directory) -> list[dict]:

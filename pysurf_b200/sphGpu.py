@@ -562,29 +562,44 @@ class PairSums:
 
     # -- the breaking tracker's reads (2D), on the device -- #
 
-    def surfaceTops(self, x0: float, width: float, count: int) -> np.ndarray:
-        """The highest fluid particle's height in each of `count` columns from x0 (-inf where empty)."""
+    def surfaceTops(self, x0: float, width: float, count: int, section=None) -> np.ndarray:
+        """The highest fluid particle's height in each of `count` columns from x0 (-inf where empty).
+        `section` (3D): (y, halfWidth), the fluid with |y_p - y| < halfWidth, its heights along z."""
         tops = np.empty(int(count))
-        check(self._lib.sph_surface_tops(self._handle, float(x0), float(width), int(count), dptr(tops)),
-              'surfaceTops')
+        if section is None:
+            check(self._lib.sph_surface_tops(self._handle, float(x0), float(width), int(count), dptr(tops)),
+                  'surfaceTops')
+        else:
+            check(self._lib.sph_section_tops(self._handle, float(section[0]), float(section[1]), float(x0),
+                                             float(width), int(count), dptr(tops)), 'surfaceTops')
         return tops
 
     def faceCells(self, lowX: float, highX: float, lowZ: float, half: float, start: float, base: float,
-                  spacing: float, columns: int, bands: int) -> np.ndarray:
-        """The face window's marked cells, (bands, columns) booleans (see sph_face_cells)."""
+                  spacing: float, columns: int, bands: int, section=None) -> np.ndarray:
+        """The face window's marked cells, (bands, columns) booleans (see sph_face_cells); `section` as
+        in `surfaceTops`."""
         marks = np.empty((int(bands), int(columns)), dtype=np.uint8)
-        check(self._lib.sph_face_cells(self._handle, float(lowX), float(highX), float(lowZ), float(half),
-                                       float(start), float(base), float(spacing), int(columns), int(bands),
-                                       marks.ctypes.data_as(_lib._pu8)), 'faceCells')
+        window = (float(lowX), float(highX), float(lowZ), float(half), float(start), float(base), float(spacing),
+                  int(columns), int(bands), marks.ctypes.data_as(_lib._pu8))
+        if section is None:
+            check(self._lib.sph_face_cells(self._handle, *window), 'faceCells')
+        else:
+            check(self._lib.sph_section_face_cells(self._handle, float(section[0]), float(section[1]), *window),
+                  'faceCells')
         return marks.astype(bool)
 
-    def bedSheet(self, bedX, bedZ, wetHeight: float) -> np.ndarray:
-        """The x of the fluid particles less than `wetHeight` above the bed profile, in no set order."""
+    def bedSheet(self, bedX, bedZ, wetHeight: float, section=None) -> np.ndarray:
+        """The x of the fluid particles less than `wetHeight` above the bed profile, in no set order;
+        `section` as in `surfaceTops`."""
         bx, bz = f64(bedX), f64(bedZ)
         xs = np.empty(max(self.count, 1))
         found = _lib.C.c_int64(0)
-        check(self._lib.sph_bed_sheet(self._handle, dptr(bx), dptr(bz), len(bx), float(wetHeight), dptr(xs),
-                                      len(xs), _lib.C.byref(found)), 'bedSheet')
+        sheet = (dptr(bx), dptr(bz), len(bx), float(wetHeight), dptr(xs), len(xs), _lib.C.byref(found))
+        if section is None:
+            check(self._lib.sph_bed_sheet(self._handle, *sheet), 'bedSheet')
+        else:
+            check(self._lib.sph_section_bed_sheet(self._handle, float(section[0]), float(section[1]), *sheet),
+                  'bedSheet')
         return xs[:found.value]
 
     def pullPositions(self, out: np.ndarray | None = None) -> np.ndarray:
