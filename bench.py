@@ -351,9 +351,10 @@ def referenceArm(args) -> None:
 
 
 def toBreaking(args) -> None:
-    """The beach from its start to the breaking point on one GPU: the device steps, with the
-    breaking tracker reading the pulled fluid positions every 0.01 sqrt(d / g) (what the reference's
-    facade does, src/pysurf/BreakingWave.py:885-912); wall time from push to the breaking point."""
+    """The case from its start to the breaking point on one GPU: the device steps, with the breaking
+    tracker (the ridge: its middle section's) reading the wave on the device every 0.01 sqrt(d / g)
+    (what the reference's facades do, src/pysurf/BreakingWave.py:885-912); wall time from push to the
+    breaking point."""
     import torch
     from pysurf_b200 import breaking, cases
     case = buildCase(args)
@@ -364,7 +365,12 @@ def toBreaking(args) -> None:
     start = time.perf_counter()
     sums.push(state)
     sums.setBoundary(case.boundary, state)
-    tracker, simulated, steps = breaking.runToBreaking(case, sums, endTime=12.0)
+    shortest = case.smoothingLength
+    if refines(case, args):
+        cases.refineCrestZone(sums, case)
+        shortest *= 0.5
+    # the ridge's sections, or the beach's tracker; the 32-ppd ridge takes hours to its breaking point
+    tracker, simulated, steps = breaking.runToBreaking(case, sums, endTime=12.0, shortestLength=shortest)
     torch.cuda.synchronize()
     wall = time.perf_counter() - start
     point = tracker.breakingPoint
@@ -447,8 +453,9 @@ def serveBench(args) -> None:
     in tanks sized for 0.5M-4M particles, each run for U(2, 6) s of simulated time times
     --horizon-scale; admitted as slots (--slots) and device memory free up, solved beside the requests
     in flight.  Beside p50/p99 latency the line reports the load the stream offers (its particle-updates
-    over its arrival span) against what the device cleared while busy (its particle-updates over the
-    whole run): a utilisation above 1 is a queue that grows, and its latencies are its depth."""
+    over its arrival span) against what the device cleared while it held a request (its particle-updates
+    over the union of the requests' solve spans): offered over cleared above 1 is a queue that grows,
+    and its latencies are its depth."""
     import numpy as np
     from pysurf_b200 import batch
     rng = np.random.default_rng(0)
@@ -470,6 +477,13 @@ def serveBench(args) -> None:
     updates = sum(r.fluidParticles * r.steps for r in results)
     span = float(arrivals[-1] - arrivals[0]) if args.serve > 1 else float('nan')
     offered = updates / span if span > 0 else float('nan')
+    # the seconds with at least one request on the device: the union of the requests' solve spans
+    busy, reach = 0.0, -math.inf
+    for begin, end in sorted((r.started, r.finished) for r in results):
+        if end > reach:
+            busy += end - max(begin, reach)
+            reach = end
+    cleared = updates / busy if busy > 0 else float('nan')
     line = {'metric': 'p99 latency', 'value': out['latency_p99_s'], 'unit': 's', 'n_gpus': 1,
             'higher_is_better': False, 'data': 'synthetic',
             'config': {'workload': f'{args.serve} requests, Poisson {args.rate}/s, 80% 2D beach 16-64 ppd, 20% 3D '
@@ -477,8 +491,9 @@ def serveBench(args) -> None:
                        'slots': args.slots},
             'latency_p50_s': out['latency_p50_s'], 'latency_p99_s': out['latency_p99_s'],
             'seconds': out['seconds'], 'particle_updates_per_s': out['particle_updates_per_s'],
-            'offered_particle_updates_per_s': offered, 'arrival_span_s': span,
-            'utilisation': offered / out['particle_updates_per_s'] if out['particle_updates_per_s'] else None,
+            'offered_particle_updates_per_s': offered, 'arrival_span_s': span, 'busy_s': busy,
+            'cleared_while_busy_particle_updates_per_s': cleared,
+            'offered_over_cleared': offered / cleared if cleared == cleared and cleared > 0 else None,
             'failed': sum(1 for r in results if r.error), 'particles': [r.particles for r in results]}
     print(json.dumps(line), flush=True)
 

@@ -657,7 +657,7 @@ struct MomentumVisit {
     Smoothing<K, D> S;
     float vi[3], rhoI, own, viscosityScale;   // viscosityScale: -alpha c0
     float alphaI;                               // closure: this particle's eddy alpha
-    float Gi[3][3];
+    float slopeI[D * (D + 1) / 2];              // r . G_i r's coefficients: G_aa, and G_ab + G_ba (a < b)
     float total[3];
     float comp[COMP ? 3 : 1];
     float parts[BUDGET ? 4 : 1][3];
@@ -674,29 +674,31 @@ struct MomentumVisit {
         const float plain = approach;           // before the limiter reconstructs it
         float viscosity = 0.0f;
         if (approach < 0.0f && P.limited && fluidJ) {
+            // the slopes r . G r along the pair, each a quadratic form in r: only G's symmetric part
+            // enters, so r's products d_a d_b (a <= b) serve both particles
             float Gj[3][3];
             loadMatrix<D>(F.G0, F.G1, F.G2, j, Gj);
-            float rampI[3] = {0, 0, 0}, rampJ[3] = {0, 0, 0};
-            float slopeI = 0.0f, slopeJ = 0.0f;
-            for (int a = 0; a < D; ++a) {
-                for (int b = 0; b < D; ++b) { rampI[a] += Gi[a][b] * d[b]; rampJ[a] += Gj[a][b] * d[b]; }
-                slopeI += d[a] * rampI[a];
-                slopeJ += d[a] * rampJ[a];
-            }
+            float slopeIJ = 0.0f, slopeJ = 0.0f;
+            for (int a = 0; a < D; ++a)
+                for (int b = a; b < D; ++b) {
+                    const float dd = d[a] * d[b], gj = a == b ? Gj[a][a] : Gj[a][b] + Gj[b][a];
+                    slopeIJ += slopeI[packed<D>(a, b)] * dd;
+                    slopeJ += gj * dd;
+                }
             float limiter = 0.0f;
-            if (slopeI * slopeJ > 0.0f) {
+            if (slopeIJ * slopeJ > 0.0f) {
                 // 4 R / (1 + R)^2 at R = slopeI / slopeJ, as 4 slopeI slopeJ / (slopeI + slopeJ)^2
-                const float sum = slopeI + slopeJ;
+                const float sum = slopeIJ + slopeJ;
                 // the fast division (2 ulp) takes 8% off the momentum sweep; its range limit (a
                 // denominator past 2^126) lies far beyond any pair's slopes
-                limiter = fminf(1.0f, __fdividef(4.0f * slopeI * slopeJ, sum * sum));
+                limiter = fminf(1.0f, __fdividef(4.0f * slopeIJ * slopeJ, sum * sum));
                 if (q < kCloseDistance) {
                     float fade = (q - kCloseDistance) * (1.0f / kFoldWidth);
                     limiter *= expf(-fade * fade);
                 }
             }
-            approach = 0.0f;
-            for (int a = 0; a < D; ++a) approach += (rel[a] - 0.5f * limiter * (rampI[a] + rampJ[a])) * d[a];
+            // (v_ij - (phi / 2) (G_i + G_j) r) . r = v_ij . r - (phi / 2) (r . G_i r + r . G_j r)
+            approach = plain - 0.5f * limiter * (slopeIJ + slopeJ);
         }
         if (approach < 0.0f) {
             // -alpha c0 h (v_ij . r_ij) / ((r^2 + 0.01 h^2) (rho_i + rho_j) / 2); the denominator is
@@ -798,7 +800,12 @@ momentumKernel(Params P, Frame F, Control *ctl, int maxima)
             visit.own = pressureRatioOf<D>(F, i);
             visit.viscosityScale = -P.alpha * P.c0;
             visit.alphaI = P.closure ? F.eddy[i].x : 0.0f;
-            if (P.limited) loadMatrix<D>(F.G0, F.G1, F.G2, i, visit.Gi);
+            if (P.limited) {
+                float Gi[3][3];
+                loadMatrix<D>(F.G0, F.G1, F.G2, i, Gi);
+                for (int a = 0; a < D; ++a)
+                    for (int b = a; b < D; ++b) visit.slopeI[packed<D>(a, b)] = a == b ? Gi[a][a] : Gi[a][b] + Gi[b][a];
+            }
             visit.total[0] = visit.total[1] = visit.total[2] = 0.0f;
             if constexpr (COMP) for (int a = 0; a < 3; ++a) visit.comp[a] = 0.0f;
             if constexpr (BUDGET)

@@ -203,6 +203,7 @@ struct Candidates {
     const int4 *column;
     int stride, count, k, step;
     int4 chunk;         // the entries still to visit of the current chunk, first in x
+    int4 ahead;         // this lane's next chunk, loaded while the current one's neighbours are summed
     // walk
     bool walking;
     int search, first, nx, ny, x0, x1, y0, y1, z1, zz, yy, j, end;
@@ -246,7 +247,12 @@ struct Candidates {
     {
         if (!walking) {
             if (k >= count) return false;
-            if ((k & 3) == 0) chunk = __ldg(column + (size_t)(k >> 2) * stride);
+            if ((k & 3) == 0) {
+                // the table streams from DRAM: the lane's next chunk is requested a chunk ahead
+                chunk = ahead;
+                const int next = (k >> 2) + step;
+                if (4 * next < count) ahead = __ldg(column + (size_t)next * stride);
+            }
             const int entry = chunk.x;
             chunk.x = chunk.y; chunk.y = chunk.z; chunk.z = chunk.w;
             // the chunk's last entry passes to this lane's next chunk
@@ -343,6 +349,7 @@ __device__ __forceinline__ void forEachNeighbour(const Params &P, const Frame &F
         C.stride = P.listStride;
         C.count = count;
         C.k = 4 * t;
+        if (C.k < count) C.ahead = __ldg(C.column + (size_t)t * C.stride);
         C.step = T;
     } else {
         O.cell = F.cell[i];
