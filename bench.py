@@ -302,6 +302,19 @@ def profiledTraffic(case, kernel: str, refined: bool, fluid: int) -> float | Non
     return float(match.group(1)) * fluid / float(captured.group(1))
 
 
+def cpuState(case, refine: bool) -> tuple:
+    """The state the float64 CPU step runs on, its fluid count and what it is: the whole beach, or the
+    ridge's sample (ridgeSample)."""
+    import numpy as np
+    if case.dimensions == 3:
+        sample = ridgeSample(case, refine)
+        return sample, int(sample['isFluid'].sum()), 'one float64 step over a sample of the workload: ' + \
+            sample.pop('description')
+    state = {k: np.array(getattr(case.state, k), copy=True) for k in ('positions', 'velocities', 'densities',
+                                                                       'masses', 'isFluid')}
+    return state, case.fluidCount, f'full steps of the whole case ({case.state.nParticles} particles) in float64'
+
+
 def cpuBaseline(case, refine: bool, seconds: float = 12.0) -> dict:
     """The float64 oracle's step on the same workload (the ridge: its sample), on every host core, for
     about `seconds` after one untimed step."""

@@ -315,6 +315,46 @@ struct BoundaryRows<V, std::void_t<decltype(V::kBoundaryRows)>> {
     static constexpr bool value = V::kBoundaryRows;
 };
 
+// Whether a sweep reading its particle's table row keeps the next neighbour's rows in flight while it
+// sums the current one (kPipelined): one more neighbour's loads in registers, the same visits in the
+// same order, so the same bits.
+template <class V, class = void>
+struct Pipelined {
+    static constexpr bool value = false;
+};
+template <class V>
+struct Pipelined<V, std::void_t<decltype(V::kPipelined)>> {
+    static constexpr bool value = V::kPipelined;
+};
+
+// One table entry's visit: the separation from the rows already loaded, the support's r, the visitor.
+template <int D, class Visitor>
+__device__ __forceinline__ void visitEntry(const Params &P, const float pi[3], const float li[3], double shift64,
+                                           float hI, int j, int image, const float4 &A, const float4 &B,
+                                           const float4 &Kj, Visitor &visit)
+{
+    const float offset = image ? (float)shift64 : 0.0f;
+    float pj[3], lj[3], d[3];
+    pointIn<D>(A, pj);
+    const float hs = signedLengthIn<D>(A, B);
+    const bool fluidJ = hs > 0.0f;
+    if (!visit.accept(fluidJ)) return;
+    remainderIn<D>(A, B, lj);
+    const float r2 = separation2<D>(P, pi, li, pj, lj, offset, image, shift64, d);
+    const float h = P.mixedH ? 0.5f * (hI + fabsf(hs)) : P.hMax;
+    const float r = __fsqrt_rn(r2);
+    if (Visitor::kSkipCoincident && r < 1.0e-12f) return;
+    visit(j, d, r, h, fluidJ, image, B, Kj);
+}
+
+template <int D, class Visitor>
+__device__ __forceinline__ void loadRows(const Frame &F, int j, float4 &A, float4 &B, float4 &Kj)
+{
+    A = __ldg(&F.pa[j]);
+    B = __ldg(&F.pb[j]);
+    Kj = Visitor::kKinetic ? __ldg(&F.kin[j]) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+}
+
 template <int D, int T, bool FINE, class Visitor>
 __device__ __forceinline__ void forEachNeighbour(const Params &P, const Frame &F, int i, int t, float hI,
                                                  Visitor &visit, bool useTable = true)
@@ -358,6 +398,23 @@ __device__ __forceinline__ void forEachNeighbour(const Params &P, const Frame &F
     }
 
     int counted = 0, j = 0, image = 0, level = 0;
+    if constexpr (Pipelined<Visitor>::value) {
+        if (!C.walking) {
+            // a software pipeline over the row: the next entry's rows load while this one is summed
+            float4 A, B, Kj;
+            bool more = C.next(P, O, pi, li, j, image, level);
+            if (more) loadRows<D, Visitor>(F, j, A, B, Kj);
+            while (more) {
+                int jn = 0, imagen = 0;
+                float4 An, Bn, Kn;
+                more = C.next(P, O, pi, li, jn, imagen, level);
+                if (more) loadRows<D, Visitor>(F, jn, An, Bn, Kn);
+                visitEntry<D>(P, pi, li, shift64, hI, j, image, A, B, Kj, visit);
+                j = jn; image = imagen; A = An; B = Bn; Kj = Kn;
+            }
+            return;
+        }
+    }
     while (C.next(P, O, pi, li, j, image, level)) {
         const float offset = image ? (float)shift64 : 0.0f;     // the search's origin: particle or image
         const float4 A = __ldg(&F.pa[j]);
