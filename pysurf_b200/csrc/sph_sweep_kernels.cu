@@ -530,19 +530,21 @@ template <int D, int K>
 struct GradientVisit {
     static constexpr bool kSkipCoincident = true;
     static constexpr bool kPipelined = true;
+    static constexpr bool kAuxRow = D == 3;
     static constexpr bool kKinetic = true;
     const Frame &F;
     Smoothing<K, D> kernel;
     bool wantG, wantL, wantRho;
     float vi[3], devI;
     float S[3][3], Mf[D * (D + 1) / 2], gsum[3];     // Mf: its upper triangle, packed
+    float4 rowX;
     double M[D * (D + 1) / 2];
     __device__ bool accept(bool) const { return true; }
     __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int, const float4 &B,
                                const float4 &Kj)
     {
         const KernelAt k = kernel.at(h);
-        const float4 X = auxRow<D>(F, j);
+        const float4 X = D == 3 ? rowX : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (wantL) {
             double dd[3] = {(double)d[0], (double)d[1], (double)d[2]}, r2 = 0.0;
             for (int a = 0; a < D; ++a) r2 = fma(dd[a], dd[a], r2);
@@ -661,6 +663,7 @@ template <int D, int K, bool BUDGET, bool COMP = false>
 struct MomentumVisit {
     static constexpr bool kSkipCoincident = true;
     static constexpr bool kPipelined = true;
+    static constexpr bool kAuxRow = D == 3;
     static constexpr bool kKinetic = true;
     const Params &P; const Frame &F;
     Smoothing<K, D> S;
@@ -670,6 +673,7 @@ struct MomentumVisit {
     float total[3];
     float comp[COMP ? 3 : 1];
     float parts[BUDGET ? 4 : 1][3];
+    float4 rowX;
     __device__ bool accept(bool) const { return true; }
     __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int, const float4 &B,
                                const float4 &Kj)
@@ -724,7 +728,7 @@ struct MomentumVisit {
             viscosity += -(P.waterTerm / h + mean) * P.c0 * h * P.closureRho0 * plain
                        / (r * r * rhoI * densityIn<D>(Kj));
         }
-        const float ratioJ = D == 2 ? Kj.w : __ldg(&F.aux[j].x);
+        const float ratioJ = D == 2 ? Kj.w : rowX.x;
         // explicit roundings on the sum's path, so the budget's extra uses of its terms cannot
         // change how the compiler fuses them: the tracked step is the plain step, bit for bit
         const float pressureTerm = __fadd_rn(own, ratioJ);
@@ -958,6 +962,8 @@ template <int D, int K, bool BUDGET, bool COMP = false>
 struct ContinuityVisit {
     static constexpr bool kSkipCoincident = true;
     static constexpr bool kPipelined = true;
+    static constexpr bool kAuxRow = D == 3;
+    static constexpr bool kLowRow = true;
     static constexpr bool kKinetic = true;
     static constexpr bool kBoundaryRows = true;         // every row
     const Params &P; const Frame &F;
@@ -969,6 +975,7 @@ struct ContinuityVisit {
     float total, comp;
     double cross;           // the fluid-boundary pairs' terms in float64
     float plainFluid, plainWall, continuity, diffusive;     // BUDGET
+    float4 rowX, rowLow;
     __device__ bool accept(bool fluidJ) const { return !(boundaryI && !fluidJ); }
     __device__ void operator()(int j, const float *d, float r, float h, bool fluidJ, int image, const float4 &B,
                                const float4 &Kj)
@@ -976,7 +983,7 @@ struct ContinuityVisit {
         const KernelAt k = S.at(h);
         float vj[3];
         velocityIn<D>(Kj, vj);
-        const float4 lowJ = __ldg(&F.low[j]);
+        const float4 lowJ = rowLow;
         const float vlJ[3] = {lowJ.x, lowJ.y, lowJ.z};
         if (boundaryI == fluidJ) {
             // a fluid-boundary pair, in float64: x_i - x_j from the points and remainders, the distance
@@ -1048,7 +1055,7 @@ struct ContinuityVisit {
             if (fluidJ) plainFluid += plain; else plainWall += plain;
         }
         if (diffuses && fluidJ) {
-            const float4 X = auxRow<D>(F, j);
+            const float4 X = D == 3 ? rowX : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
             const float devJ = deviationIn<D>(B, X);
             // rho_j - rho_i from the float32 deviations and their remainders, so it keeps float64's
             // digits (the leading difference is exact for neighbours' nearly equal deviations)

@@ -327,11 +327,38 @@ struct Pipelined<V, std::void_t<decltype(V::kPipelined)>> {
     static constexpr bool value = V::kPipelined;
 };
 
+// Whether a visitor reads a neighbour's aux row (3D: P2, deviation, V) or remainder row (kAuxRow,
+// kLowRow): the walk loads them with the others, so the pipeline keeps them in flight too, and hands
+// them to the visitor in its rowX / rowLow.
+template <class V, class = void>
+struct AuxRow {
+    static constexpr bool value = false;
+};
+template <class V>
+struct AuxRow<V, std::void_t<decltype(V::kAuxRow)>> {
+    static constexpr bool value = V::kAuxRow;
+};
+template <class V, class = void>
+struct LowRow {
+    static constexpr bool value = false;
+};
+template <class V>
+struct LowRow<V, std::void_t<decltype(V::kLowRow)>> {
+    static constexpr bool value = V::kLowRow;
+};
+
+template <int D, class Visitor>
+__device__ __forceinline__ void loadExtra(const Frame &F, int j, float4 &X, float4 &L)
+{
+    if constexpr (AuxRow<Visitor>::value) X = auxRow<D>(F, j);
+    if constexpr (LowRow<Visitor>::value) L = __ldg(&F.low[j]);
+}
+
 // One table entry's visit: the separation from the rows already loaded, the support's r, the visitor.
 template <int D, class Visitor>
 __device__ __forceinline__ void visitEntry(const Params &P, const float pi[3], const float li[3], double shift64,
                                            float hI, int j, int image, const float4 &A, const float4 &B,
-                                           const float4 &Kj, Visitor &visit)
+                                           const float4 &Kj, const float4 &X, const float4 &L, Visitor &visit)
 {
     const float offset = image ? (float)shift64 : 0.0f;
     float pj[3], lj[3], d[3];
@@ -344,6 +371,8 @@ __device__ __forceinline__ void visitEntry(const Params &P, const float pi[3], c
     const float h = P.mixedH ? 0.5f * (hI + fabsf(hs)) : P.hMax;
     const float r = __fsqrt_rn(r2);
     if (Visitor::kSkipCoincident && r < 1.0e-12f) return;
+    if constexpr (AuxRow<Visitor>::value) visit.rowX = X;
+    if constexpr (LowRow<Visitor>::value) visit.rowLow = L;
     visit(j, d, r, h, fluidJ, image, B, Kj);
 }
 
@@ -401,16 +430,16 @@ __device__ __forceinline__ void forEachNeighbour(const Params &P, const Frame &F
     if constexpr (Pipelined<Visitor>::value) {
         if (!C.walking) {
             // a software pipeline over the row: the next entry's rows load while this one is summed
-            float4 A, B, Kj;
+            float4 A, B, Kj, X, L;
             bool more = C.next(P, O, pi, li, j, image, level);
-            if (more) loadRows<D, Visitor>(F, j, A, B, Kj);
+            if (more) { loadRows<D, Visitor>(F, j, A, B, Kj); loadExtra<D, Visitor>(F, j, X, L); }
             while (more) {
                 int jn = 0, imagen = 0;
-                float4 An, Bn, Kn;
+                float4 An, Bn, Kn, Xn, Ln;
                 more = C.next(P, O, pi, li, jn, imagen, level);
-                if (more) loadRows<D, Visitor>(F, jn, An, Bn, Kn);
-                visitEntry<D>(P, pi, li, shift64, hI, j, image, A, B, Kj, visit);
-                j = jn; image = imagen; A = An; B = Bn; Kj = Kn;
+                if (more) { loadRows<D, Visitor>(F, jn, An, Bn, Kn); loadExtra<D, Visitor>(F, jn, Xn, Ln); }
+                visitEntry<D>(P, pi, li, shift64, hI, j, image, A, B, Kj, X, L, visit);
+                j = jn; image = imagen; A = An; B = Bn; Kj = Kn; X = Xn; L = Ln;
             }
             return;
         }
@@ -443,6 +472,8 @@ __device__ __forceinline__ void forEachNeighbour(const Params &P, const Frame &F
         }
         const float r = __fsqrt_rn(r2);
         if (Visitor::kSkipCoincident && r < 1.0e-12f) continue;
+        if constexpr (AuxRow<Visitor>::value) visit.rowX = auxRow<D>(F, j);
+        if constexpr (LowRow<Visitor>::value) visit.rowLow = __ldg(&F.low[j]);
         visit(j, d, r, h, fluidJ, image, B, Kj);
     }
 }
