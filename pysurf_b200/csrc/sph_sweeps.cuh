@@ -150,6 +150,15 @@ __device__ __forceinline__ float separation2(const Params &P, const float pi[3],
     return r2;
 }
 
+// A pair's distance from its squared distance: the hardware reciprocal square root (about 2 ulp)
+// times r^2, 0 for a coincident pair.  The support is decided on r^2, so r only enters the kernel's
+// value and gradient, where its rounding is of the float32 terms' own size; continuity's and the
+// correction matrix's float64 parts take one Newton step from it to float64's digits.
+__device__ __forceinline__ float pairDistance(float r2)
+{
+    return r2 > 0.0f ? r2 * rsqrtf(r2) : 0.0f;
+}
+
 // (2 h)^2, the support test's bound.
 __device__ __forceinline__ float support2(float h)
 {
@@ -369,7 +378,7 @@ __device__ __forceinline__ void visitEntry(const Params &P, const float pi[3], c
     remainderIn<D>(A, B, lj);
     const float r2 = separation2<D>(P, pi, li, pj, lj, offset, image, shift64, d);
     const float h = P.mixedH ? 0.5f * (hI + fabsf(hs)) : P.hMax;
-    const float r = __fsqrt_rn(r2);
+    const float r = pairDistance(r2);
     if (Visitor::kSkipCoincident && r < 1.0e-12f) return;
     if constexpr (AuxRow<Visitor>::value) visit.rowX = X;
     if constexpr (LowRow<Visitor>::value) visit.rowLow = L;
@@ -470,7 +479,7 @@ __device__ __forceinline__ void forEachNeighbour(const Params &P, const Frame &F
                 if (!visit.accept(fluidJ)) continue;
             }
         }
-        const float r = __fsqrt_rn(r2);
+        const float r = pairDistance(r2);
         if (Visitor::kSkipCoincident && r < 1.0e-12f) continue;
         if constexpr (AuxRow<Visitor>::value) visit.rowX = auxRow<D>(F, j);
         if constexpr (LowRow<Visitor>::value) visit.rowLow = __ldg(&F.low[j]);
