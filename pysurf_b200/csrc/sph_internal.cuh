@@ -195,15 +195,35 @@ __device__ __forceinline__ KernelAt kernelAt(float unit, float h)
 }
 
 // A pair's kernel constants at h_ij: one set a thread when every particle has the same smoothing
-// length (then h_ij = hMax), else taken per pair.
-template <int K, int D>
+// length (then h_ij = hMax), else taken per pair.  HOLD (mixed lengths): the set is held at the
+// particle's own length instead, which every pair with a neighbour of the same length has
+// (0.5 (h + h) = h exactly), so those pairs, all but the few across a refinement zone's edge, take
+// the held set and the rest take theirs per pair, with the same bits either way.  It pays where a
+// sweep has registers to spare (measured: the refined 3D ridge's gradients 10.2 -> 9.7 ms, while
+// continuity, at its register cap, went 11.5 -> 12.2).
+template <int K, int D, bool HOLD = false>
 struct Smoothing {
     KernelAt fixed;
+    float held;     // the length `fixed` is taken at
     float unit;
     bool mixed;
-    __device__ __forceinline__ explicit Smoothing(const Params &P)
-        : fixed(kernelAt<K, D>(P.sigmaUnit, P.hMax)), unit(P.sigmaUnit), mixed(P.mixedH != 0) {}
-    __device__ __forceinline__ KernelAt at(float h) const { return mixed ? kernelAt<K, D>(unit, h) : fixed; }
+    __device__ __forceinline__ static float heldLength(const Params &P, float own)
+    {
+        return HOLD && P.mixedH && own > 0.0f ? own : P.hMax;
+    }
+    // own: the particle's smoothing length (HOLD only)
+    __device__ __forceinline__ explicit Smoothing(const Params &P, float own = 0.0f)
+        : fixed(kernelAt<K, D>(P.sigmaUnit, heldLength(P, own))), held(heldLength(P, own)), unit(P.sigmaUnit),
+          mixed(P.mixedH != 0) {}
+    __device__ __forceinline__ KernelAt at(float h) const
+    {
+        if constexpr (HOLD) {
+            if (h == held) return fixed;
+            return kernelAt<K, D>(unit, h);
+        } else {
+            return mixed ? kernelAt<K, D>(unit, h) : fixed;
+        }
+    }
 };
 
 // W(q h), q < 2.

@@ -465,13 +465,13 @@ __global__ void applyShepardKernel(Params P, Frame F, const Control *ctl)
 // Sweep A: extrapolated wall pressure
 // ------------------------------------------------------------------------------------------
 
-template <int D, int K>
+template <int D, int K, bool HOLD = false>
 struct WallVisit {
     static constexpr bool kSkipCoincident = false;
     static constexpr bool kKinetic = true;
     static constexpr bool kBoundaryRows = true;         // it runs boundary rows only
     const Params &P; const Frame &F;
-    Smoothing<K, D> S;
+    Smoothing<K, D, HOLD> S;
     float weight, total;
     __device__ bool accept(bool fluidJ) const { return fluidJ; }
     __device__ void operator()(int j, const float *d, float r, float h, bool, int, const float4 &, const float4 &Kj)
@@ -496,7 +496,7 @@ wallPressureKernel(Params P, Frame F, const Control *ctl, int writeDensity)
     if (i >= P.n) return;
     float hs = signedLength<D>(F, i);
     if (hs > 0.0f) return;
-    WallVisit<D, K> visit{P, F, Smoothing<K, D>(P), 0.0f, 0.0f};
+    WallVisit<D, K, FINE> visit{P, F, Smoothing<K, D, FINE>(P, -hs), 0.0f, 0.0f};
     forEachNeighbour<D, T, FINE>(P, F, i, G.t, -hs, visit);
     float weight = groupSum<T>(visit.weight, G.mask), total = groupSum<T>(visit.total, G.mask);
     if (G.t != 0) return;
@@ -526,14 +526,14 @@ wallPressureKernel(Params P, Frame F, const Control *ctl, int writeDensity)
 template <int D>
 __device__ __forceinline__ constexpr int packed(int a, int b) { return a * D - a * (a - 1) / 2 + (b - a); }
 
-template <int D, int K>
+template <int D, int K, bool HOLD = false>
 struct GradientVisit {
     static constexpr bool kSkipCoincident = true;
     static constexpr bool kPipelined = true;
     static constexpr bool kAuxRow = D == 3;
     static constexpr bool kKinetic = true;
     const Frame &F;
-    Smoothing<K, D> kernel;
+    Smoothing<K, D, HOLD> kernel;
     bool wantG, wantL, wantRho;
     float vi[3], devI;
     float S[3][3], Mf[D * (D + 1) / 2], gsum[3];     // Mf: its upper triangle, packed
@@ -597,7 +597,7 @@ gradientKernel(Params P, Frame F, const Control *ctl, int wantG, int wantL, int 
         if (wantRho) F.gradRho[i] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         return;
     }
-    GradientVisit<D, K> visit{F, Smoothing<K, D>(P), wantG != 0, wantL != 0 || wantRho != 0, wantRho != 0};
+    GradientVisit<D, K, FINE> visit{F, Smoothing<K, D, FINE>(P, hs), wantG != 0, wantL != 0 || wantRho != 0, wantRho != 0};
     velocityOf<D>(F, i, visit.vi);
     visit.devI = deviationOf<D>(F, i);
     for (int a = 0; a < 3; ++a) {
