@@ -186,18 +186,25 @@ __global__ void __launch_bounds__(kBlock) listKernel(Params P, Frame F, const Co
 #endif
 constexpr int kBatch = SPH_LIST_BATCH;
 
-struct BatchMember {
-    double shift64;         // the periodic image's shift (0 when it is not searched)
-    float pi[3], li[3];
-    float hI, limit, fineLimit, offset;
-    float sure;             // a coarse distance under it is a neighbour (sureBound)
-    int slot, seam;
-    int fluidOnly;          // a boundary member: its row holds fluid neighbours only
-    int runA, runB;         // this row's run of candidates for the member, [runA, runB)
+// A batch member as the warp's lanes read it, in 16-byte rows so that each read is one shared load:
+// the run and flags decide whether the member takes a chunk at all, the point its coarse test, the
+// remainder only the few candidates near the edge of its support.  The set-up lane writes the
+// search's bounds into point.w and rest.w as each search starts.
+constexpr int kMemberSeam = 1;          // the member searches its periodic image too
+constexpr int kMemberFluidOnly = 2;     // a boundary member: its row holds fluid neighbours only
+struct alignas(16) BatchMember {
+    float4 point;       // the float32 point; w: this search's sure bound (0 where none applies)
+    float4 rest;        // the remainder; w: this search's coarse limit
+    int4 run;           // this row's run of candidates [x, y), the member's slot, its flags
+    float4 bounds;      // the limit on the coarse grid, on the fine grid, the sure bound, hI
+    double shift64;     // the periodic image's shift (0 when it is not searched)
+    float offset;       // the shift as float32
+    float unused;
 };
 
-// No blocks-a-multiprocessor bound: at the compiler's default the kernel keeps about 28 warps an
-// SM with a few spills, faster than 85-116 registers and no spills at 3 to 6 blocks (measured).
+// No blocks-a-multiprocessor bound: at the compiler's default the kernel keeps about 24 warps an
+// SM with a few spills, faster than 85-116 registers and no spills at 3 to 6 blocks, or 64
+// registers at 8 (measured).
 template <int D, bool PRECISE, bool MIXED>
 __global__ void __launch_bounds__(kBlock) cellListKernel(Params P, Frame F, const Control *ctl, int *maxCount)
 {
@@ -238,25 +245,18 @@ __global__ void __launch_bounds__(kBlock) cellListKernel(Params P, Frame F, cons
                 seamp = true;
                 shiftp = pip[1] < 0.5f * P.periodF ? P.period : -P.period;
             }
-            BatchMember &m = mine[lane];
-            for (int a = 0; a < 3; ++a) { m.pi[a] = pip[a]; m.li[a] = lip[a]; }
-            m.hI = hIp;
-            m.limit = kCandidateMargin * reach * reach;
-            m.sure = PRECISE ? sureBound(P, support, hIp, pip) : 0.0f;
             const float fineReach = hIp + P.fineMax;
-            m.fineLimit = kCandidateMargin * fineReach * fineReach;
+            BatchMember &m = mine[lane];
+            m.point = make_float4(pip[0], pip[1], pip[2], 0.0f);
+            m.rest = make_float4(lip[0], lip[1], lip[2], 0.0f);
+            m.run = make_int4(0, 0, i, (seamp ? kMemberSeam : 0) |
+                                           (signedLengthIn<D>(Ai, Bi) <= 0.0f ? kMemberFluidOnly : 0));
+            m.bounds = make_float4(kCandidateMargin * reach * reach, kCandidateMargin * fineReach * fineReach,
+                                   PRECISE ? sureBound(P, support, hIp, pip) : 0.0f, hIp);
             m.shift64 = shiftp;
             m.offset = (float)shiftp;
-            m.slot = i;
-            m.seam = seamp ? 1 : 0;
-            m.fluidOnly = signedLengthIn<D>(Ai, Bi) <= 0.0f ? 1 : 0;
         }
         const bool anySeam = __any_sync(0xFFFFFFFFu, seamp);
-        // the batch's boundary members, whose rows hold fluid neighbours only: a mask in a register for
-        // one smoothing length; with mixed lengths the register costs more than the shared-memory
-        // read it saves (measured), so that form reads each member's flag
-        const unsigned boundaryMembers =
-            MIXED ? 0u : __ballot_sync(0xFFFFFFFFu, lane < count && mine[lane < count ? lane : 0].fluidOnly);
         int counted[kBatch];
 #pragma unroll
         for (int p = 0; p < kBatch; ++p) counted[p] = 0;
@@ -264,26 +264,33 @@ __global__ void __launch_bounds__(kBlock) cellListKernel(Params P, Frame F, cons
         for (int search = 0; search < (MIXED ? 4 : 2); ++search) {
             const int level = MIXED ? search >> 1 : 0, image = search & 1;
             if (level >= P.levels || (image && !anySeam)) continue;
-            // lane p: its own box, its place in the centre cell, and its reach in cell widths
+            // lane p: this search's bounds for the others, its own box, its place in the centre cell,
+            // and its reach in cell widths
             const bool takes = lane < count && (!image || seamp);
             CellBox box{};
             float fx = 0.0f, fy = 0.0f, fz = 0.0f, R = 0.0f;
             bool trim = false;
-            if (takes) {
-                const double pos[3] = {(double)pip[0] + (double)lip[0],
-                                       (double)pip[1] + (double)lip[1] + (image ? shiftp : 0.0),
-                                       D == 3 ? (double)pip[2] + (double)lip[2] : 0.0};
-                box = cellBox(P, level, ownCell, pos, image != 0, D, searchCells(P, level, hIp), !MIXED);
-                const double width = level ? P.fineWidth : P.cellWidth;
-                const double *origin = level ? P.fineOrigin : P.origin;
-                const float invW = (float)(1.0 / width);
-                const float lim = level ? mine[lane].fineLimit : mine[lane].limit;
-                fx = (float)(((double)pip[0] - origin[0]) / width) - (float)box.cx;
-                fz = D == 3 ? (float)(((double)pip[2] - origin[2]) / width) - (float)box.cz : 0.5f;
-                fy = (float)(((double)pip[1] + (image ? shiftp : 0.0) - origin[1]) / width) - (float)box.cy;
-                R = (1.001f * sqrtf(lim) + 5.0e-7f * (fabsf(pip[0]) + fabsf(pip[1]) + fabsf(pip[2]))) * invW +
-                    1.0e-3f;
-                trim = SPH_LIST_TRIM && fx >= 0.0f && fx < 1.0f && fy >= 0.0f && fy < 1.0f && fz >= 0.0f && fz < 1.0f;
+            if (lane < count) {
+                const float4 bounds = mine[lane].bounds;
+                const float lim = level ? bounds.y : bounds.x;
+                mine[lane].point.w = PRECISE && !image && level == 0 ? bounds.z : 0.0f;
+                mine[lane].rest.w = lim;
+                if (takes) {
+                    const double pos[3] = {(double)pip[0] + (double)lip[0],
+                                           (double)pip[1] + (double)lip[1] + (image ? shiftp : 0.0),
+                                           D == 3 ? (double)pip[2] + (double)lip[2] : 0.0};
+                    box = cellBox(P, level, ownCell, pos, image != 0, D, searchCells(P, level, hIp), !MIXED);
+                    const double width = level ? P.fineWidth : P.cellWidth;
+                    const double *origin = level ? P.fineOrigin : P.origin;
+                    const float invW = (float)(1.0 / width);
+                    fx = (float)(((double)pip[0] - origin[0]) / width) - (float)box.cx;
+                    fz = D == 3 ? (float)(((double)pip[2] - origin[2]) / width) - (float)box.cz : 0.5f;
+                    fy = (float)(((double)pip[1] + (image ? shiftp : 0.0) - origin[1]) / width) - (float)box.cy;
+                    R = (1.001f * sqrtf(lim) + 5.0e-7f * (fabsf(pip[0]) + fabsf(pip[1]) + fabsf(pip[2]))) * invW +
+                        1.0e-3f;
+                    trim = SPH_LIST_TRIM && fx >= 0.0f && fx < 1.0f && fy >= 0.0f && fy < 1.0f && fz >= 0.0f &&
+                           fz < 1.0f;
+                }
             }
             // the grid's shape (the same for every member) and the union of the members' rows
             const int gridFirst = level ? P.fineFirst : 0;
@@ -318,7 +325,7 @@ __global__ void __launch_bounds__(kBlock) cellListKernel(Params P, Frame F, cons
                             b = __ldg(&F.cellStart[row + xb + 1]);
                         }
                     }
-                    if (lane < count) { mine[lane].runA = a; mine[lane].runB = b; }
+                    if (lane < count) { mine[lane].run.x = a; mine[lane].run.y = b; }
                     const int uA = __reduce_min_sync(0xFFFFFFFFu, a < b ? a : INT_MAX);
                     const int uB = __reduce_max_sync(0xFFFFFFFFu, a < b ? b : INT_MIN);
                     __syncwarp();
@@ -341,33 +348,39 @@ __global__ void __launch_bounds__(kBlock) cellListKernel(Params P, Frame F, cons
 #pragma unroll
                         for (int p = 0; p < kBatch; ++p) {
                             if (p >= count) continue;      // count is the warp's: the loop keeps its trip count
-                            const BatchMember &m = mine[p];
-                            const int ra = m.runA, rb = m.runB;
-                            if (ra >= rb || rb <= base || ra >= base + 32) continue;     // the whole warp
-                            if (image && !m.seam) continue;
+                            const int4 run = mine[p].run;
+                            if (run.x >= run.y || run.y <= base || run.x >= base + 32) continue;   // the whole warp
+                            if (image && !(run.w & kMemberSeam)) continue;
                             bool accepted = false;
-                            const bool boundaryMember = MIXED ? m.fluidOnly != 0 : ((boundaryMembers >> p) & 1u) != 0;
-                            if (valid && j >= ra && j < rb && j != m.slot && (fluidJ || !boundaryMember)) {
-                                const float offset = image ? m.offset : 0.0f;
-                                const float coarse = coarseDistance2<D>(m.pi, pj, offset);
-                                if (PRECISE && !image && level == 0 && coarse < m.sure) {
+                            if (valid && j >= run.x && j < run.y && j != run.z &&
+                                (fluidJ || !(run.w & kMemberFluidOnly))) {
+                                const float4 point = mine[p].point;
+                                const float mp[3] = {point.x, point.y, point.z};
+                                const float offset = image ? mine[p].offset : 0.0f;
+                                const float coarse = coarseDistance2<D>(mp, pj, offset);
+                                if (PRECISE && coarse < point.w) {
                                     accepted = true;
-                                } else if (coarse < (level ? m.fineLimit : m.limit)) {
-                                    float r2 = coarse;
-                                    if (PRECISE) {
-                                        float d[3];
-                                        r2 = separation2<D, 1>(P, m.pi, m.li, pj, lj, offset, image,
-                                                               image ? m.shift64 : 0.0, d);
+                                } else {
+                                    const float4 rest = mine[p].rest;
+                                    if (coarse < rest.w) {
+                                        float r2 = coarse;
+                                        if (PRECISE) {
+                                            const float ml[3] = {rest.x, rest.y, rest.z};
+                                            float d[3];
+                                            r2 = separation2<D, 1>(P, mp, ml, pj, lj, offset, image,
+                                                                   image ? mine[p].shift64 : 0.0, d);
+                                        }
+                                        const float bound =
+                                            MIXED ? support2(0.5f * (mine[p].bounds.w + hJ)) : support;
+                                        accepted = r2 < bound;
                                     }
-                                    const float bound = MIXED ? support2(0.5f * (m.hI + hJ)) : support;
-                                    accepted = r2 < bound;
                                 }
                             }
                             const unsigned bits = __ballot_sync(0xFFFFFFFFu, accepted);
                             if (accepted) {
                                 const int k = counted[p] + __popc(bits & lower);
                                 if (k < P.listCap) {
-                                    int *column = F.nbr + 4 * (size_t)m.slot;
+                                    int *column = F.nbr + 4 * (size_t)run.z;
                                     column[((size_t)(k >> 2) * P.listStride) * 4 + (k & 3)] =
                                         image ? (j | (int)0x80000000) : j;
                                 }
