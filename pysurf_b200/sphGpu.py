@@ -293,11 +293,13 @@ class PairSums:
         lengthArray = None
         if lengths is not None:
             lengthArray = f64(lengths, (count,))
-            if count and lengthArray.max() > self.maxLength * (1.0 + 1e-9):
-                raise ValueError(f'A smoothing length of {lengthArray.max()} m exceeds the {self.maxLength} m the hash '
+            longest = float(lengthArray.max()) if count else self.smoothingLength
+            if count and longest > self.maxLength * (1.0 + 1e-9):
+                raise ValueError(f'A smoothing length of {longest} m exceeds the {self.maxLength} m the hash '
                                  f'grid is built for.')
             self.minLength = float(lengthArray.min()) if count else self.smoothingLength
-            self.uniformLengths = bool(np.all(lengthArray == lengthArray[0])) if count else True
+            # all equal exactly when the least is the greatest (a NaN makes both NaN, unequal)
+            self.uniformLengths = self.minLength == longest if count else True
         else:
             self.minLength = self.smoothingLength
             self.uniformLengths = True
@@ -482,11 +484,16 @@ class PairSums:
         count = len(positions)
         lengths = getattr(particles, 'lengths', None)
         lengthArray = None if lengths is None else f64(lengths, (count,))
-        if lengthArray is not None and count and lengthArray.max() > self.maxLength * (1.0 + 1e-9):
-            raise ValueError(f'A smoothing length of {lengthArray.max()} m exceeds the {self.maxLength} m the hash '
+        # two passes over the lengths: all are equal exactly when the least is the greatest (a NaN
+        # makes both NaN, which compare unequal, as an elementwise test would find)
+        given = lengthArray is not None and count > 0
+        longest = float(lengthArray.max()) if given else self.smoothingLength
+        shortest = float(lengthArray.min()) if given else self.smoothingLength
+        if given and longest > self.maxLength * (1.0 + 1e-9):
+            raise ValueError(f'A smoothing length of {longest} m exceeds the {self.maxLength} m the hash '
                              f'grid is built for.')
-        self.minLength = float(lengthArray.min()) if lengthArray is not None and count else self.smoothingLength
-        self.uniformLengths = lengthArray is None or bool(np.all(lengthArray == lengthArray[0]))
+        self.minLength = shortest
+        self.uniformLengths = not given or shortest == longest
         flags, flagPtr = u8(particles.isFluid)
         self.count = count
         check(self._lib.sph_push(self._handle, count, dptr(positions), dptr(f64(particles.velocities)),
