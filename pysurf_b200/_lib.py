@@ -158,5 +158,6 @@ def f64(array, shape=None):
 
 
 def u8(array):
-    out = np.ascontiguousarray(np.asarray(array).astype(bool).view(np.uint8))
+    """A C-contiguous uint8 view of a flag array (a bool array's own memory, so pinned stays pinned)."""
+    out = np.ascontiguousarray(np.asarray(array).astype(bool, copy=False).view(np.uint8))
     return out, out.ctypes.data_as(_pu8)

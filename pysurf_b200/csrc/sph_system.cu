@@ -424,6 +424,12 @@ struct SphSystem {
         if (lengths)
             for (int i = 0; i < count; ++i)
                 if (lengths[i] < h && lengths[i] > longest) longest = lengths[i];
+        return takeFineLength(longest);
+    }
+
+    // The fine level from its longest length, found by the caller (0 for none).
+    int takeFineLength(double longest)
+    {
         if (longest == fineMax) return SPH_OK;
         fineMax = longest;
         return setupLevels();
@@ -966,16 +972,25 @@ static int loadState(SphSystem *sys, int64_t count, const double *positions, con
         CUDA_TRY(cudaStreamSynchronize(sys->stream));
         lengths = hostLengths.data();
     }
-    double hMax = 0.0, hMin = sys->h;
+    double hMax = 0.0, hMin = sys->h, fineLongest = 0.0;
     bool mixed = false;
     if (lengths && n > 0) {
-        hMax = lengths[0];
-        hMin = lengths[0];
+        // one pass, free of branches so that it vectorises: the range, how many lengths are not h,
+        // and the longest below h (the fine level's)
+        const double h = sys->h;
+        double top = lengths[0], bottom = lengths[0], below = 0.0;
+        long long others = 0;
         for (int i = 0; i < n; ++i) {
-            hMax = std::max(hMax, lengths[i]);
-            hMin = std::min(hMin, lengths[i]);
-            if (lengths[i] != sys->h) mixed = true;
+            const double l = lengths[i];
+            top = std::max(top, l);
+            bottom = std::min(bottom, l);
+            others += l != h;
+            below = std::max(below, l < h ? l : 0.0);
         }
+        hMax = top;
+        hMin = bottom;
+        mixed = others > 0;
+        fineLongest = below;
         if (hMax > sys->h * (1.0 + 1e-9))
             return fail(SPH_ERR_INVALID, "a smoothing length of " + std::to_string(hMax) + " m exceeds the " +
                                              std::to_string(sys->h) + " m the cell list is built for");
@@ -984,7 +999,7 @@ static int loadState(SphSystem *sys, int64_t count, const double *positions, con
     if (mixed && sys->shifting)
         return fail(SPH_ERR_INVALID, "particle shifting needs one smoothing length for every particle");
     TRY(sys->reserve(n, false));
-    TRY(sys->takeLevels(lengths, n));
+    TRY(sys->takeFineLength(lengths ? fineLongest : 0.0));
     if (sys->n != n) sys->graphDirty = true;
     sys->n = n;
     sys->mixedH = mixed;
