@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/pysurf_b200.h"
@@ -955,6 +956,54 @@ int sph_set_physics(SphSystem *sys, double reference_density, double sound_speed
 
 // kind: cudaMemcpyHostToDevice for the caller's host arrays, cudaMemcpyDeviceToDevice for its
 // device arrays (the lengths, which the host checks, are then read back first).
+// A push's smoothing lengths at a glance: their range, how many are not the grid's h, and the longest
+// below h (the fine level's, 0 for none).  Order-free, so the host threads that share a long array
+// give the bits one thread would.
+struct LengthRange {
+    double top, bottom, below;
+    long long others;
+};
+
+static LengthRange scanLengthSpan(const double *lengths, long long begin, long long end, double h)
+{
+    LengthRange r{lengths[begin], lengths[begin], 0.0, 0};
+    for (long long i = begin; i < end; ++i) {
+        const double l = lengths[i];
+        r.top = std::max(r.top, l);
+        r.bottom = std::min(r.bottom, l);
+        r.others += l != h;
+        r.below = std::max(r.below, l < h ? l : 0.0);
+    }
+    return r;
+}
+
+static LengthRange scanLengths(const double *lengths, int n, double h)
+{
+    const unsigned cores = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const int parts = n >= (1 << 20) ? (int)cores : 1;
+    if (parts == 1) return scanLengthSpan(lengths, 0, n, h);
+    std::vector<LengthRange> found(parts);
+    std::vector<std::thread> threads;
+    for (int t = 1; t < parts; ++t) {
+        const long long begin = (long long)n * t / parts, end = (long long)n * (t + 1) / parts;
+        try {
+            threads.emplace_back([&found, lengths, begin, end, h, t] { found[t] = scanLengthSpan(lengths, begin, end, h); });
+        } catch (...) {
+            found[t] = scanLengthSpan(lengths, begin, end, h);     // no thread to be had: scan the part here
+        }
+    }
+    found[0] = scanLengthSpan(lengths, 0, (long long)n / parts, h);
+    for (auto &thread : threads) thread.join();
+    LengthRange r = found[0];
+    for (int t = 1; t < parts; ++t) {
+        r.top = std::max(r.top, found[t].top);
+        r.bottom = std::min(r.bottom, found[t].bottom);
+        r.below = std::max(r.below, found[t].below);
+        r.others += found[t].others;
+    }
+    return r;
+}
+
 static int loadState(SphSystem *sys, int64_t count, const double *positions, const double *velocities,
                      const double *densities, const double *masses, const uint8_t *is_fluid, const double *lengths,
                      cudaMemcpyKind kind = cudaMemcpyHostToDevice)
@@ -975,22 +1024,11 @@ static int loadState(SphSystem *sys, int64_t count, const double *positions, con
     double hMax = 0.0, hMin = sys->h, fineLongest = 0.0;
     bool mixed = false;
     if (lengths && n > 0) {
-        // one pass, free of branches so that it vectorises: the range, how many lengths are not h,
-        // and the longest below h (the fine level's)
-        const double h = sys->h;
-        double top = lengths[0], bottom = lengths[0], below = 0.0;
-        long long others = 0;
-        for (int i = 0; i < n; ++i) {
-            const double l = lengths[i];
-            top = std::max(top, l);
-            bottom = std::min(bottom, l);
-            others += l != h;
-            below = std::max(below, l < h ? l : 0.0);
-        }
-        hMax = top;
-        hMin = bottom;
-        mixed = others > 0;
-        fineLongest = below;
+        const LengthRange range = scanLengths(lengths, n, sys->h);
+        hMax = range.top;
+        hMin = range.bottom;
+        mixed = range.others > 0;
+        fineLongest = range.below;
         if (hMax > sys->h * (1.0 + 1e-9))
             return fail(SPH_ERR_INVALID, "a smoothing length of " + std::to_string(hMax) + " m exceeds the " +
                                              std::to_string(sys->h) + " m the cell list is built for");
