@@ -30,22 +30,29 @@ namespace sph {
 template <int D>
 constexpr int budgetMinBlocks() { return D == 2 ? 5 : 4; }
 // The gradients and continuity sweeps carry float64 sums beside their float32 ones (M; the wall pairs'
-// terms), so they take more registers a thread and fewer resident blocks.
+// terms), so they take more registers a thread and fewer resident blocks.  Continuity also keeps the
+// next neighbour's five rows in flight: at 4 blocks in 3D (128 registers, none spilled) it runs 16-25%
+// faster than at 5 (96, spilling) on the ridges, and at 5 in 2D (102) 3.5% faster than at 6 on the
+// beach (measured).
 #ifndef SPH_PRECISE_MIN_BLOCKS
-#define SPH_PRECISE_MIN_BLOCKS 6
+#define SPH_PRECISE_MIN_BLOCKS 5
 #endif
 #ifndef SPH_PRECISE_MIN_BLOCKS_3D
-#define SPH_PRECISE_MIN_BLOCKS_3D 5
+#define SPH_PRECISE_MIN_BLOCKS_3D 4
 #endif
 template <int D>
 constexpr int preciseMinBlocks() { return D == 2 ? SPH_PRECISE_MIN_BLOCKS : SPH_PRECISE_MIN_BLOCKS_3D; }
 // The 3D gradients sweep keeps three 3 x 3 float32 sums and the float64 M: at 4 blocks (128
-// registers) it ran 7-17% faster than at 5 on the ridges (measured); in 2D the shared cap stands.
+// registers) it ran 7-17% faster than at 5 on the ridges; in 2D 6 blocks (80 registers) ran 3%
+// faster than 5 on the beach (measured).
+#ifndef SPH_GRADIENT_MIN_BLOCKS
+#define SPH_GRADIENT_MIN_BLOCKS 6
+#endif
 #ifndef SPH_GRADIENT_MIN_BLOCKS_3D
 #define SPH_GRADIENT_MIN_BLOCKS_3D 4
 #endif
 template <int D>
-constexpr int gradientMinBlocks() { return D == 2 ? SPH_PRECISE_MIN_BLOCKS : SPH_GRADIENT_MIN_BLOCKS_3D; }
+constexpr int gradientMinBlocks() { return D == 2 ? SPH_GRADIENT_MIN_BLOCKS : SPH_GRADIENT_MIN_BLOCKS_3D; }
 
 // ------------------------------------------------------------------------------------------
 // The neighbour table
